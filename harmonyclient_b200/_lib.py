@@ -1,0 +1,89 @@
+"""ctypes binding of libhy.so, the CUDA engine (C-ABI in include/hy.h).
+
+Importing this module loads the in-tree library; if it has not been built the
+import fails loudly — there is no CPU fallback for any operation.
+"""
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhy.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "hy.h")
+
+HY_OK, HY_ERR_ARG, HY_ERR_OOM, HY_ERR_CUDA, HY_ERR_TIMEOUT, HY_ERR_STATE, HY_ERR_IO, HY_ERR_UNSUPPORTED = range(8)
+HY_MAX_K = 256
+
+
+class HyError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"hy error {code}: {msg}")
+        self.code = code
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [("d", C.c_size_t), ("nlist", C.c_size_t), ("nprobe", C.c_size_t), ("metric", C.c_int),
+                ("opt_level", C.c_int), ("dim_blocks", C.c_size_t), ("ntotal", C.c_size_t),
+                ("arena_rows", C.c_size_t), ("trained", C.c_int), ("device", C.c_int)]
+
+
+class SearchStats(C.Structure):
+    _fields_ = [("nq", C.c_uint64), ("pairs", C.c_uint64), ("rows", C.c_uint64), ("tile_blocks", C.c_uint64),
+                ("tile_blocks_max", C.c_uint64), ("coarse_ms", C.c_double), ("scan_ms", C.c_double),
+                ("merge_ms", C.c_double), ("launches", C.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def declared_symbols():
+    """Names of every function include/hy.h declares."""
+    with open(HEADER) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"HY_API\s+[\w\s\*]+?\b(hy_\w+)\s*\(", txt)))
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libhy.so is not built ({LIB_PATH}); run: python -m harmonyclient_b200.build")
+    L = C.CDLL(LIB_PATH)
+    sz, vp, i = C.c_size_t, C.c_void_p, C.c_int
+    H = C.c_void_p
+    L.hy_last_error.restype = C.c_char_p
+    L.hy_version.restype = C.c_char_p
+    L.hy_index_create.argtypes = [sz, sz, sz, i, i, sz, i, C.POINTER(C.c_void_p)]
+    L.hy_index_destroy.argtypes = [H]
+    L.hy_index_info.argtypes = [H, C.POINTER(IndexInfo)]
+    L.hy_index_train.argtypes = [H, sz, vp, i]
+    L.hy_index_train_device.argtypes = [H, sz, vp, i, vp]
+    L.hy_index_set_centroids.argtypes = [H, vp]
+    L.hy_index_get_centroids.argtypes = [H, vp]
+    L.hy_index_add.argtypes = [H, sz, vp]
+    L.hy_index_add_device.argtypes = [H, sz, vp, vp]
+    L.hy_index_set_nprobe.argtypes = [H, sz]
+    L.hy_index_presearch.argtypes = [H, sz, sz]
+    L.hy_index_search.argtypes = [H, sz, vp, sz, vp, vp]
+    L.hy_index_search_device.argtypes = [H, sz, vp, sz, vp, vp, vp]
+    L.hy_index_search_preassigned.argtypes = [H, sz, vp, sz, sz, vp, vp, vp]
+    L.hy_index_probes.argtypes = [H, sz, vp, vp]
+    L.hy_index_warmup_tops.argtypes = [H, sz, vp, sz, sz, vp, sz, sz, vp]
+    L.hy_index_last_stats.argtypes = [H, C.POINTER(SearchStats)]
+    L.hy_index_list_size.argtypes = [H, sz, C.POINTER(C.c_size_t)]
+    L.hy_index_get_list.argtypes = [H, sz, vp, vp, vp]
+    L.hy_index_save.argtypes = [H, C.c_char_p]
+    L.hy_index_load.argtypes = [H, C.c_char_p]
+    L.hy_file_inspect.argtypes = [C.c_char_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != HY_OK:
+        raise HyError(rc, load().hy_last_error().decode(errors="replace"))

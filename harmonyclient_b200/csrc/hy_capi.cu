@@ -1,0 +1,982 @@
+// C-ABI of the B200 IVF engine: handle lifecycle, training, list
+// construction, search orchestration, list access and the reference's .index
+// file format.  Declarations and contracts are in include/hy.h.
+//
+// Everything on the data path runs on the GPU through the kernels in
+// hy_kernels.cu; host code here only validates arguments, sizes buffers,
+// computes the seeded sampling permutation (std::shuffle with
+// std::default_random_engine, as the reference's Clustering does) and moves
+// data between host and device.  There is no CPU search path.
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/hy.h"
+#include "hy_kernels.cuh"
+
+using hy::ArenaLayout;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+struct Status {
+    int code = HY_OK;
+    std::string msg;
+};
+
+#define HY_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? HY_ERR_OOM : HY_ERR_CUDA,                    \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+        }                                                                                              \
+    } while (0)
+
+#define HY_CHECK(cond, code, msg) \
+    do {                          \
+        if (!(cond)) return fail(code, msg); \
+    } while (0)
+
+#define HY_RET(call)              \
+    do {                          \
+        int rc_ = (call);         \
+        if (rc_ != HY_OK) return rc_; \
+    } while (0)
+
+// A grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return HY_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t want = std::max<size_t>(n, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(HY_ERR_OOM, std::string("cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e));
+        }
+        bytes = want;
+        return HY_OK;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+ArenaLayout make_layout(int d, int nb) {
+    ArenaLayout L;
+    L.d = d;
+    L.nb = nb;
+    const int cd = d / nb;
+    for (int b = 0; b < nb; ++b) L.bstart[b] = b * cd;
+    L.bstart[nb] = d;
+    L.boff[0] = 0;
+    L.max_pitch = 0;
+    for (int b = 0; b < nb; ++b) {
+        const int w = L.bstart[b + 1] - L.bstart[b];
+        L.pitch[b] = (w + hy::PITCH_ALIGN - 1) / hy::PITCH_ALIGN * hy::PITCH_ALIGN;
+        L.boff[b + 1] = L.boff[b] + L.pitch[b];
+        L.max_pitch = std::max(L.max_pitch, L.pitch[b]);
+    }
+    L.row_pitch = L.boff[nb];
+    return L;
+}
+
+}  // namespace
+
+struct hy_index {
+    std::mutex mu;
+    int device = 0;
+    size_t d = 0, nlist = 0, nprobe = 0;
+    int metric = HY_METRIC_L2;
+    int opt_level = 0;
+    size_t sub_k = 0, sub_nlist = 1, sub_nprobe = 1;
+    size_t dim_blocks = 4;
+    ArenaLayout L;
+    bool trained = false;
+    size_t ntotal = 0;
+    size_t arena_rows = 0;
+    size_t warmup_list = 0, warmup_list_size = 0;
+
+    std::vector<float> h_cent;
+    std::vector<int64_t> h_list_off;  // nlist+1, arena rows (tile aligned)
+    std::vector<int32_t> h_list_size;
+
+    DevBuf cent, list_off, list_size, ids, codes, norms;
+    // workspace
+    DevBuf w_q, w_scores, w_probes, w_thr, w_gthr, w_parts, w_D, w_I, w_f, w_counters, w_err;
+    DevBuf w_x, w_lab, w_dist, w_keys, w_keys2, w_vals, w_vals2, w_sort, w_start, w_sums, w_cnt, w_rows, w_xn;
+
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    hy_search_stats_t stats = {};
+    uint64_t launches = 0;  // kernels launched since the last stats snapshot
+};
+
+namespace {
+
+int set_device(hy_index* h) {
+    HY_CUDA(cudaSetDevice(h->device));
+    return HY_OK;
+}
+
+// Bytes of the coarse score scratch per query chunk.
+constexpr size_t SCORE_BUDGET = size_t(512) << 20;
+
+size_t query_chunk(size_t nlist, size_t n) {
+    size_t qc = SCORE_BUDGET / (nlist * sizeof(float));
+    qc = std::max<size_t>(qc, 64);
+    qc = std::min<size_t>(qc, 65536);
+    return std::min(qc, n);
+}
+
+// Nearest centroid of each of n device rows (x), chunked: labels, scores.
+int assign_rows(hy_index* h, const float* x, size_t n, int64_t* labels, float* score, cudaStream_t s) {
+    const size_t rc = query_chunk(h->nlist, n);
+    HY_RET(h->w_scores.ensure(rc * h->nlist * sizeof(float)));
+    for (size_t r0 = 0; r0 < n; r0 += rc) {
+        const size_t m = std::min(rc, n - r0);
+        HY_CUDA(hy::launch_coarse_scores(x + r0 * h->d, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d,
+                                         h->metric, h->w_scores.as<float>(), s));
+        HY_CUDA(hy::launch_argmin(h->w_scores.as<float>(), (int)m, (int)h->nlist, labels + r0, score ? score + r0 : nullptr,
+                                  s));
+    }
+    return HY_OK;
+}
+
+// k-means on a device sample xs (ns rows): centroids initialised from host
+// sample indices; FP64 sums (Clustering::update_centroids,
+// src/Clustering.cpp:93-152).
+int kmeans_device(hy_index* h, const float* xs, size_t ns, const std::vector<int64_t>& init_rows, int niter,
+                  cudaStream_t s) {
+    const size_t d = h->d, nlist = h->nlist;
+    HY_RET(h->w_rows.ensure(nlist * sizeof(int64_t)));
+    HY_CUDA(cudaMemcpyAsync(h->w_rows.p, init_rows.data(), nlist * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    HY_RET(h->cent.ensure(nlist * d * sizeof(float)));
+    HY_CUDA(hy::launch_gather_rows(xs, h->w_rows.as<int64_t>(), (int64_t)nlist, (int)d, h->cent.as<float>(), s));
+    const float* assign_src = xs;
+    if (h->metric == HY_METRIC_IP) {
+        HY_RET(h->w_xn.ensure(ns * d * sizeof(float)));
+        HY_CUDA(hy::launch_normalize_rows(xs, (int64_t)ns, (int)d, h->w_xn.as<float>(), s));
+        assign_src = h->w_xn.as<float>();
+    }
+    HY_RET(h->w_lab.ensure(ns * sizeof(int64_t)));
+    HY_RET(h->w_sums.ensure(nlist * d * sizeof(double)));
+    HY_RET(h->w_cnt.ensure(nlist * sizeof(unsigned long long)));
+    for (int it = 0; it < niter; ++it) {
+        HY_RET(assign_rows(h, assign_src, ns, h->w_lab.as<int64_t>(), nullptr, s));
+        HY_CUDA(cudaMemsetAsync(h->w_sums.p, 0, nlist * d * sizeof(double), s));
+        HY_CUDA(cudaMemsetAsync(h->w_cnt.p, 0, nlist * sizeof(unsigned long long), s));
+        HY_CUDA(hy::launch_kmeans_accumulate(xs, h->w_lab.as<int64_t>(), (int64_t)ns, (int)d, h->w_sums.as<double>(),
+                                             h->w_cnt.as<unsigned long long>(), s));
+        HY_CUDA(hy::launch_kmeans_update(h->w_sums.as<double>(), h->w_cnt.as<unsigned long long>(), (int)nlist, (int)d,
+                                         h->cent.as<float>(), s));
+    }
+    if (h->metric == HY_METRIC_IP) HY_CUDA(hy::launch_normalize_centroids(h->cent.as<float>(), (int)nlist, (int)d, s));
+    h->h_cent.resize(nlist * d);
+    HY_CUDA(cudaMemcpyAsync(h->h_cent.data(), h->cent.p, nlist * d * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    h->trained = true;
+    return HY_OK;
+}
+
+// The reference's sampling: keep everything when n <= nlist * 256, else the
+// first nlist*256 entries of a shuffle of 0..n-1 (src/Clustering.cpp:48-68);
+// initial centroids are the first nlist entries of a second shuffle of the
+// sample (src/Clustering.cpp:72-89).  Both shuffles use
+// std::default_random_engine(6666) (src/Index.cpp:392).
+void sampling_plan(size_t n, size_t nlist, std::vector<int64_t>* sample, std::vector<int64_t>* init, size_t* ns) {
+    const size_t maxs = nlist * 256;
+    const int seed = 6666;
+    sample->clear();
+    *ns = n;
+    if (n > maxs) {
+        std::vector<size_t> idx(n);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::shuffle(idx.begin(), idx.end(), std::default_random_engine(seed));
+        sample->assign(idx.begin(), idx.begin() + maxs);
+        *ns = maxs;
+    }
+    std::vector<size_t> idx2(*ns);
+    std::iota(idx2.begin(), idx2.end(), 0);
+    std::shuffle(idx2.begin(), idx2.end(), std::default_random_engine(seed));
+    init->assign(idx2.begin(), idx2.begin() + nlist);
+}
+
+int train_impl(hy_index* h, size_t n, const float* x, bool x_on_device, int lite, cudaStream_t s) {
+    HY_CHECK(n >= h->nlist, HY_ERR_ARG, "train: need at least nlist training rows");
+    std::vector<int64_t> sample, init;
+    size_t ns = 0;
+    sampling_plan(n, h->nlist, &sample, &init, &ns);
+    const size_t d = h->d;
+    HY_RET(h->w_x.ensure(ns * d * sizeof(float)));
+    float* xs = h->w_x.as<float>();
+    if (x_on_device) {
+        if (sample.empty()) {
+            HY_CUDA(cudaMemcpyAsync(xs, x, ns * d * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        } else {
+            HY_RET(h->w_keys.ensure(ns * sizeof(int64_t)));
+            HY_CUDA(cudaMemcpyAsync(h->w_keys.p, sample.data(), ns * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+            HY_CUDA(hy::launch_gather_rows(x, h->w_keys.as<int64_t>(), (int64_t)ns, (int)d, xs, s));
+        }
+    } else {
+        if (sample.empty()) {
+            HY_CUDA(cudaMemcpyAsync(xs, x, ns * d * sizeof(float), cudaMemcpyHostToDevice, s));
+        } else {
+            std::vector<float> hs(ns * d);
+            for (size_t i = 0; i < ns; ++i) std::memcpy(&hs[i * d], x + sample[i] * d, d * sizeof(float));
+            HY_CUDA(cudaMemcpyAsync(xs, hs.data(), ns * d * sizeof(float), cudaMemcpyHostToDevice, s));
+            HY_CUDA(cudaStreamSynchronize(s));
+        }
+    }
+    return kmeans_device(h, xs, ns, init, lite ? 2 : 20, s);
+}
+
+// Build the arena from n device rows x that are already grouped: `order` (an
+// array of n row indices, device) lists rows list by list; labels[i] is row
+// i's list.  sizes = rows per list.
+int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, const int64_t* labels,
+                const std::vector<int32_t>& sizes, cudaStream_t s) {
+    const size_t nlist = h->nlist;
+    h->h_list_size = sizes;
+    h->h_list_off.assign(nlist + 1, 0);
+    std::vector<int64_t> start(nlist + 1, 0);
+    for (size_t l = 0; l < nlist; ++l) {
+        start[l + 1] = start[l] + sizes[l];
+        h->h_list_off[l + 1] = h->h_list_off[l] + (sizes[l] + 31) / 32 * 32;
+    }
+    h->arena_rows = (size_t)h->h_list_off[nlist];
+    const size_t rows_alloc = std::max<size_t>(h->arena_rows, 32);
+    HY_RET(h->codes.ensure(rows_alloc * h->L.row_pitch * sizeof(float)));
+    HY_RET(h->ids.ensure(rows_alloc * sizeof(int64_t)));
+    HY_RET(h->norms.ensure(rows_alloc * sizeof(float)));
+    HY_RET(h->list_off.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_RET(h->list_size.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->w_start.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_CUDA(cudaMemsetAsync(h->codes.p, 0, rows_alloc * h->L.row_pitch * sizeof(float), s));
+    HY_CUDA(cudaMemsetAsync(h->norms.p, 0, rows_alloc * sizeof(float), s));
+    HY_CUDA(hy::launch_fill_i64(h->ids.as<int64_t>(), (int64_t)rows_alloc, -1, s));
+    HY_CUDA(cudaMemcpyAsync(h->list_off.p, h->h_list_off.data(), (nlist + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->list_size.p, sizes.data(), nlist * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_start.p, start.data(), (nlist + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    if (n > 0)
+        HY_CUDA(hy::launch_scatter(h->L, x, (int64_t)n, order, labels, h->w_start.as<int64_t>(),
+                                   h->list_off.as<int64_t>(), h->codes.as<float>(), h->ids.as<int64_t>(),
+                                   h->norms.as<float>(), s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    h->ntotal = n;
+    return HY_OK;
+}
+
+int add_impl(hy_index* h, size_t n, const float* x, bool x_on_device, cudaStream_t s) {
+    HY_CHECK(h->trained, HY_ERR_STATE, "add: index is not trained (no centroids)");
+    HY_CHECK(n < (size_t(1) << 31), HY_ERR_ARG, "add: at most 2^31-1 rows per call");
+    const size_t d = h->d, nlist = h->nlist;
+    if (n == 0) {
+        // The reference returns without touching the lists (src/Index.cpp:583-590).
+        return HY_OK;
+    }
+    const float* xd = x;
+    if (!x_on_device) {
+        HY_RET(h->w_x.ensure(n * d * sizeof(float)));
+        HY_CUDA(cudaMemcpyAsync(h->w_x.p, x, n * d * sizeof(float), cudaMemcpyHostToDevice, s));
+        xd = h->w_x.as<float>();
+    }
+    HY_RET(h->w_lab.ensure(n * sizeof(int64_t)));
+    HY_RET(h->w_dist.ensure(n * sizeof(float)));
+    HY_RET(assign_rows(h, xd, n, h->w_lab.as<int64_t>(), h->w_dist.as<float>(), s));
+    // list sizes
+    HY_RET(h->w_cnt.ensure(nlist * sizeof(int32_t)));
+    HY_CUDA(cudaMemsetAsync(h->w_cnt.p, 0, nlist * sizeof(int32_t), s));
+    HY_CUDA(hy::launch_histogram(h->w_lab.as<int64_t>(), (int64_t)n, h->w_cnt.as<int32_t>(), s));
+    std::vector<int32_t> sizes(nlist);
+    HY_CUDA(cudaMemcpyAsync(sizes.data(), h->w_cnt.p, nlist * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    // order rows by (list, score to centroid), stable in row id
+    HY_RET(h->w_keys.ensure(n * sizeof(uint64_t)));
+    HY_RET(h->w_keys2.ensure(n * sizeof(uint64_t)));
+    HY_RET(h->w_vals.ensure(n * sizeof(int32_t)));
+    HY_RET(h->w_vals2.ensure(n * sizeof(int32_t)));
+    HY_CUDA(hy::launch_make_sort_keys(h->w_lab.as<int64_t>(), h->w_dist.as<float>(), (int64_t)n,
+                                      h->w_keys.as<uint64_t>(), h->w_vals.as<int32_t>(), s));
+    int lbits = 1;
+    while ((size_t(1) << lbits) < nlist) ++lbits;
+    size_t tmp = 0;
+    HY_CUDA(hy::radix_sort_pairs(nullptr, &tmp, h->w_keys.as<uint64_t>(), h->w_keys2.as<uint64_t>(),
+                                 h->w_vals.as<int32_t>(), h->w_vals2.as<int32_t>(), (int64_t)n, 32 + lbits, s));
+    HY_RET(h->w_sort.ensure(tmp));
+    tmp = h->w_sort.bytes;
+    HY_CUDA(hy::radix_sort_pairs(h->w_sort.p, &tmp, h->w_keys.as<uint64_t>(), h->w_keys2.as<uint64_t>(),
+                                 h->w_vals.as<int32_t>(), h->w_vals2.as<int32_t>(), (int64_t)n, 32 + lbits, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    return build_arena(h, xd, n, h->w_vals2.as<int32_t>(), h->w_lab.as<int64_t>(), sizes, s);
+}
+
+int check_search_args(hy_index* h, size_t n, size_t k) {
+    HY_CHECK(k >= 1 && k <= HY_MAX_K, HY_ERR_ARG, "search: k must be in [1, " + std::to_string(HY_MAX_K) + "]");
+    HY_CHECK(h->trained, HY_ERR_STATE, "search: index is not trained (no centroids)");
+    HY_CHECK(n < (size_t(1) << 31) / 1, HY_ERR_ARG, "search: too many queries");
+    return HY_OK;
+}
+
+// Search n device queries with device probe lists (nprobe per query) into
+// device D/I.  Runs on stream s; does not synchronise.
+int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe, const int64_t* dprobes,
+                   const uint32_t* init_thr, float* dD, int64_t* dI, cudaStream_t s, bool timed) {
+    const int kp = k <= 32 ? 32 : k <= 64 ? 64 : k <= 128 ? 128 : 256;
+    int nsplit = 1;
+    const size_t target_ctas = 2 * 148;
+    if (n < target_ctas) nsplit = (int)std::min<size_t>((target_ctas + n - 1) / n, std::max<size_t>(nprobe, 1));
+    while ((nprobe + nsplit - 1) / nsplit > 2048) ++nsplit;
+    HY_RET(h->w_parts.ensure(n * nsplit * kp * sizeof(uint64_t)));
+    uint32_t* gthr = nullptr;
+    if (nsplit > 1) {
+        HY_RET(h->w_gthr.ensure(n * sizeof(uint32_t)));
+        gthr = h->w_gthr.as<uint32_t>();
+        if (init_thr)
+            HY_CUDA(cudaMemcpyAsync(gthr, init_thr, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        else
+            HY_CUDA(cudaMemsetAsync(gthr, 0xff, n * sizeof(uint32_t), s));
+    }
+    hy::ScanParams p;
+    p.L = h->L;
+    p.codes = h->codes.as<float>();
+    p.list_off = h->list_off.as<int64_t>();
+    p.list_size = h->list_size.as<int32_t>();
+    p.q = dq;
+    p.probes = dprobes;
+    p.init_thr = init_thr;
+    p.g_thr = gthr;
+    p.out = h->w_parts.as<uint64_t>();
+    p.counters = h->w_counters.as<unsigned long long>();
+    p.err = h->w_err.as<int>();
+    p.nq = (int)n;
+    p.nprobe = (int)nprobe;
+    p.nsplit = nsplit;
+    p.k = (int)k;
+    p.metric = h->metric;
+    p.prune = 1;
+    if (timed) HY_CUDA(cudaEventRecord(h->ev[2], s));
+    h->launches += 2 + (nsplit > 1 ? 1 : 0);
+    int smem = 0;
+    cudaError_t e = hy::launch_scan_plain(p, &smem, s);
+    if (e != cudaSuccess)
+        return fail(HY_ERR_CUDA, std::string("scan launch (") + std::to_string(smem) + " B shared): " + cudaGetErrorString(e));
+    if (timed) HY_CUDA(cudaEventRecord(h->ev[3], s));
+    HY_CUDA(hy::launch_merge(h->w_parts.as<uint64_t>(), (int)n, nsplit, kp, (int)k, h->metric, h->ids.as<int64_t>(),
+                             dD, dI, s));
+    if (timed) HY_CUDA(cudaEventRecord(h->ev[4], s));
+    return HY_OK;
+}
+
+int ensure_common(hy_index* h) {
+    HY_RET(h->w_counters.ensure(2 * sizeof(unsigned long long)));
+    HY_RET(h->w_err.ensure(sizeof(int)));
+    return HY_OK;
+}
+
+// Full device search: coarse quantisation, optional warm-up thresholds, scan,
+// merge, in query chunks.
+int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
+                       bool timed) {
+    const size_t nprobe = std::min(h->nprobe, h->nlist);
+    HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search: nprobe must be >= 1");
+    HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "search: nlist above 40000 is not supported by the coarse selector");
+    HY_RET(ensure_common(h));
+    const size_t qc = query_chunk(h->nlist, n);
+    HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
+    HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
+    const bool warm = h->warmup_list > 0 && h->metric == HY_METRIC_L2;
+    if (warm) HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
+    for (size_t q0 = 0; q0 < n; q0 += qc) {
+        const size_t m = std::min(qc, n - q0);
+        const float* qq = dq + q0 * h->d;
+        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[0], s));
+        HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d, h->metric,
+                                         h->w_scores.as<float>(), s));
+        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
+                                  h->w_probes.as<int64_t>(), nullptr, s));
+        h->launches += 2;
+        const uint32_t* thr = nullptr;
+        if (warm) {
+            h->launches += 1;
+            const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
+            HY_CHECK(std::min(h->warmup_list, nprobe) * wls <= 32768, HY_ERR_ARG,
+                     "presearch: warmup_list * warmup_list_size above 32768");
+            HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
+                                      qq, (int)m, h->w_probes.as<int64_t>(), (int)nprobe, (int)k, (int)h->warmup_list,
+                                      (int)wls, 1, h->w_thr.as<uint32_t>(), nullptr, h->w_err.as<int>(), s));
+            thr = h->w_thr.as<uint32_t>();
+        }
+        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[1], s));
+        HY_RET(scan_and_merge(h, m, qq, k, nprobe, h->w_probes.as<int64_t>(), thr, dD + q0 * k, dI + q0 * k, s,
+                              timed && q0 + qc >= n));
+    }
+    return HY_OK;
+}
+
+int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t nprobe) {
+    HY_CUDA(cudaStreamSynchronize(s));
+    int err = 0;
+    HY_CUDA(cudaMemcpy(&err, h->w_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err != 0) {
+        cudaMemset(h->w_err.p, 0, sizeof(int));
+        return fail(err == HY_ERR_TIMEOUT ? HY_ERR_TIMEOUT : HY_ERR_CUDA, "device reported an error in the scan kernel");
+    }
+    unsigned long long c[2] = {0, 0};
+    HY_CUDA(cudaMemcpy(c, h->w_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+    h->stats.nq = n;
+    h->stats.pairs = n * nprobe;
+    h->stats.tile_blocks = c[0];
+    h->stats.tile_blocks_max = c[1];
+    h->stats.launches = h->launches;
+    h->launches = 0;
+    if (timed) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+        h->stats.coarse_ms = ms;
+        cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+        h->stats.scan_ms = ms;
+        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+        h->stats.merge_ms = ms;
+    }
+    return HY_OK;
+}
+
+int reset_counters(hy_index* h, cudaStream_t s) {
+    HY_RET(ensure_common(h));
+    h->launches = 0;
+    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 2 * sizeof(unsigned long long), s));
+    return HY_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* hy_last_error(void) { return g_err.c_str(); }
+
+const char* hy_version(void) { return "hy 0.1 (sm_100a)"; }
+
+int hy_index_create(size_t d, size_t nlist, size_t nprobe, int metric, int opt_level, size_t dim_blocks, int device,
+                    hy_index** out) {
+    HY_CHECK(out != nullptr, HY_ERR_ARG, "create: out is NULL");
+    *out = nullptr;
+    HY_CHECK(d >= 1 && d <= 4096, HY_ERR_ARG, "create: d must be in [1, 4096]");
+    HY_CHECK(nlist >= 1 && nlist <= (size_t(1) << 24), HY_ERR_ARG, "create: nlist must be in [1, 2^24]");
+    HY_CHECK(metric == HY_METRIC_L2 || metric == HY_METRIC_IP, HY_ERR_ARG, "create: metric must be 0 (IP) or 1 (L2)");
+    HY_CHECK(opt_level >= 0 && opt_level <= 7, HY_ERR_ARG, "create: invalid opt_level");
+    if (dim_blocks == 0) dim_blocks = 4;
+    HY_CHECK(dim_blocks <= HY_MAX_DIM_BLOCKS, HY_ERR_ARG, "create: dim_blocks above HY_MAX_DIM_BLOCKS");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(HY_ERR_CUDA, std::string("create: no CUDA device available (") + cudaGetErrorString(e) + ")");
+    HY_CHECK(device >= 0 && device < ndev, HY_ERR_ARG, "create: device ordinal out of range");
+    auto* h = new (std::nothrow) hy_index();
+    HY_CHECK(h != nullptr, HY_ERR_OOM, "create: out of host memory");
+    h->device = device;
+    h->d = d;
+    h->nlist = nlist;
+    h->nprobe = nprobe;
+    h->metric = metric;
+    h->opt_level = opt_level;
+    h->dim_blocks = std::min(dim_blocks, d);
+    h->L = make_layout((int)d, (int)h->dim_blocks);
+    int rc = set_device(h);
+    if (rc == HY_OK) {
+        e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        for (int i = 0; e == cudaSuccess && i < 6; ++i) e = cudaEventCreate(&h->ev[i]);
+        if (e != cudaSuccess) rc = fail(HY_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
+    }
+    if (rc == HY_OK) rc = ensure_common(h);
+    if (rc == HY_OK) {
+        cudaMemset(h->w_err.p, 0, sizeof(int));
+    }
+    if (rc != HY_OK) {
+        hy_index_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return HY_OK;
+}
+
+int hy_index_destroy(hy_index* h) {
+    if (!h) return HY_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    DevBuf* bufs[] = {&h->cent,   &h->list_off, &h->list_size, &h->ids,    &h->codes,   &h->norms,  &h->w_q,
+                      &h->w_scores, &h->w_probes, &h->w_thr,   &h->w_gthr, &h->w_parts, &h->w_D,    &h->w_I,
+                      &h->w_f,    &h->w_counters, &h->w_err,   &h->w_x,    &h->w_lab,   &h->w_dist, &h->w_keys,
+                      &h->w_keys2, &h->w_vals,  &h->w_vals2,   &h->w_sort, &h->w_start, &h->w_sums, &h->w_cnt,
+                      &h->w_rows, &h->w_xn};
+    for (DevBuf* b : bufs) b->release();
+    for (auto& ev : h->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return HY_OK;
+}
+
+int hy_index_info(const hy_index* h, hy_index_info_t* out) {
+    HY_CHECK(h && out, HY_ERR_ARG, "info: NULL argument");
+    out->d = h->d;
+    out->nlist = h->nlist;
+    out->nprobe = h->nprobe;
+    out->metric = h->metric;
+    out->opt_level = h->opt_level;
+    out->dim_blocks = h->dim_blocks;
+    out->ntotal = h->ntotal;
+    out->arena_rows = h->arena_rows;
+    out->trained = h->trained ? 1 : 0;
+    out->device = h->device;
+    return HY_OK;
+}
+
+int hy_index_train(hy_index* h, size_t n, const float* x, int lite) {
+    HY_CHECK(h && (x || n == 0), HY_ERR_ARG, "train: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    return train_impl(h, n, x, false, lite, h->stream);
+}
+
+int hy_index_train_device(hy_index* h, size_t n, const float* dx, int lite, void* stream) {
+    HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "train: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    return train_impl(h, n, dx, true, lite, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+}
+
+int hy_index_set_centroids(hy_index* h, const float* c) {
+    HY_CHECK(h && c, HY_ERR_ARG, "set_centroids: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    const size_t bytes = h->nlist * h->d * sizeof(float);
+    HY_RET(h->cent.ensure(bytes));
+    h->h_cent.assign(c, c + h->nlist * h->d);
+    HY_CUDA(cudaMemcpy(h->cent.p, c, bytes, cudaMemcpyHostToDevice));
+    h->trained = true;
+    return HY_OK;
+}
+
+int hy_index_get_centroids(const hy_index* h, float* c) {
+    HY_CHECK(h && c, HY_ERR_ARG, "get_centroids: NULL argument");
+    HY_CHECK(h->trained, HY_ERR_STATE, "get_centroids: index is not trained");
+    std::memcpy(c, h->h_cent.data(), h->nlist * h->d * sizeof(float));
+    return HY_OK;
+}
+
+int hy_index_add(hy_index* h, size_t n, const float* x) {
+    HY_CHECK(h && (x || n == 0), HY_ERR_ARG, "add: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    return add_impl(h, n, x, false, h->stream);
+}
+
+int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream) {
+    HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "add: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    return add_impl(h, n, dx, true, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+}
+
+int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
+    HY_CHECK(h, HY_ERR_ARG, "set_nprobe: NULL handle");
+    HY_CHECK(nprobe >= 1, HY_ERR_ARG, "set_nprobe: nprobe must be >= 1");
+    h->nprobe = nprobe;
+    return HY_OK;
+}
+
+int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_list_size) {
+    HY_CHECK(h, HY_ERR_ARG, "presearch: NULL handle");
+    h->warmup_list = warmup_list;
+    h->warmup_list_size = warmup_list_size;
+    return HY_OK;
+}
+
+int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, void* stream) {
+    HY_CHECK(h && (n == 0 || (dq && dD && dI)), HY_ERR_ARG, "search: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    HY_RET(set_device(h));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    return search_device_impl(h, n, dq, k, dD, dI, s, false);
+}
+
+int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
+    HY_CHECK(h && (n == 0 || (q && D && I)), HY_ERR_ARG, "search: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
+    HY_RET(h->w_D.ensure(n * k * sizeof(float)));
+    HY_RET(h->w_I.ensure(n * k * sizeof(int64_t)));
+    HY_RET(reset_counters(h, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_RET(search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true));
+    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    return finish_host_call(h, s, true, n, std::min(h->nprobe, h->nlist));
+}
+
+int hy_index_search_preassigned(hy_index* h, size_t n, const float* q, size_t k, size_t nprobe, const int64_t* probes,
+                                float* D, int64_t* I) {
+    HY_CHECK(h && (n == 0 || (q && probes && D && I)), HY_ERR_ARG, "search_preassigned: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search_preassigned: nprobe must be >= 1");
+    for (size_t i = 0; i < n * nprobe; ++i)
+        HY_CHECK(probes[i] >= -1 && probes[i] < (int64_t)h->nlist, HY_ERR_ARG, "search_preassigned: list id out of range");
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
+    HY_RET(h->w_probes.ensure(n * nprobe * sizeof(int64_t)));
+    HY_RET(h->w_D.ensure(n * k * sizeof(float)));
+    HY_RET(h->w_I.ensure(n * k * sizeof(int64_t)));
+    HY_RET(reset_counters(h, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_probes.p, probes, n * nprobe * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const uint32_t* thr = nullptr;
+    if (h->warmup_list > 0 && h->metric == HY_METRIC_L2) {
+        const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
+        HY_CHECK(std::min(h->warmup_list, nprobe) * wls <= 32768, HY_ERR_ARG,
+                 "presearch: warmup_list * warmup_list_size above 32768");
+        HY_RET(h->w_thr.ensure(n * sizeof(uint32_t)));
+        HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
+                                  h->w_q.as<float>(), (int)n, h->w_probes.as<int64_t>(), (int)nprobe, (int)k,
+                                  (int)h->warmup_list, (int)wls, 1, h->w_thr.as<uint32_t>(), nullptr,
+                                  h->w_err.as<int>(), s));
+        thr = h->w_thr.as<uint32_t>();
+    }
+    HY_CUDA(cudaEventRecord(h->ev[0], s));
+    HY_CUDA(cudaEventRecord(h->ev[1], s));
+    HY_RET(scan_and_merge(h, n, h->w_q.as<float>(), k, nprobe, h->w_probes.as<int64_t>(), thr, h->w_D.as<float>(),
+                          h->w_I.as<int64_t>(), s, true));
+    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    return finish_host_call(h, s, true, n, nprobe);
+}
+
+int hy_index_probes(hy_index* h, size_t n, const float* q, int64_t* probes) {
+    HY_CHECK(h && (n == 0 || (q && probes)), HY_ERR_ARG, "probes: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_CHECK(h->trained, HY_ERR_STATE, "probes: index is not trained");
+    HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "probes: nlist above 40000 is not supported by the coarse selector");
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    const size_t nprobe = std::min(h->nprobe, h->nlist);
+    const size_t qc = query_chunk(h->nlist, n);
+    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
+    HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
+    HY_RET(h->w_probes.ensure(n * nprobe * sizeof(int64_t)));
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    for (size_t q0 = 0; q0 < n; q0 += qc) {
+        const size_t m = std::min(qc, n - q0);
+        HY_CUDA(hy::launch_coarse_scores(h->w_q.as<float>() + q0 * h->d, (int)m, h->cent.as<float>(), (int)h->nlist,
+                                         (int)h->d, h->metric, h->w_scores.as<float>(), s));
+        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
+                                  h->w_probes.as<int64_t>() + q0 * nprobe, nullptr, s));
+    }
+    HY_CUDA(cudaMemcpyAsync(probes, h->w_probes.p, n * nprobe * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    return HY_OK;
+}
+
+int hy_index_warmup_tops(hy_index* h, size_t n, const float* q, size_t k, size_t nprobe, const int64_t* probes,
+                         size_t warmup_list, size_t warmup_list_size, float* tops) {
+    HY_CHECK(h && (n == 0 || (q && probes && tops)), HY_ERR_ARG, "warmup_tops: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_CHECK(k >= 1, HY_ERR_ARG, "warmup_tops: k must be >= 1");
+    HY_CHECK(nprobe >= 1 && warmup_list >= 1, HY_ERR_ARG, "warmup_tops: nprobe and warmup_list must be >= 1");
+    if (warmup_list_size == 0) warmup_list_size = k;
+    HY_CHECK(std::min(warmup_list, nprobe) * warmup_list_size <= 32768, HY_ERR_ARG,
+             "warmup_tops: warmup_list * warmup_list_size above 32768");
+    for (size_t i = 0; i < n * nprobe; ++i)
+        HY_CHECK(probes[i] >= -1 && probes[i] < (int64_t)h->nlist, HY_ERR_ARG, "warmup_tops: list id out of range");
+    HY_CHECK(h->ntotal > 0 || h->arena_rows == 0, HY_ERR_STATE, "warmup_tops: no lists");
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    HY_RET(ensure_common(h));
+    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
+    HY_RET(h->w_probes.ensure(n * nprobe * sizeof(int64_t)));
+    HY_RET(h->w_thr.ensure(n * sizeof(uint32_t)));
+    HY_RET(h->w_f.ensure(n * sizeof(float)));
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_probes.p, probes, n * nprobe * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    if (h->arena_rows == 0) {
+        std::vector<float> mx(n, FLT_MAX);
+        std::memcpy(tops, mx.data(), n * sizeof(float));
+        return HY_OK;
+    }
+    HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
+                              h->w_q.as<float>(), (int)n, h->w_probes.as<int64_t>(), (int)nprobe, (int)k,
+                              (int)warmup_list, (int)warmup_list_size, 0, h->w_thr.as<uint32_t>(), h->w_f.as<float>(),
+                              h->w_err.as<int>(), s));
+    HY_CUDA(cudaMemcpyAsync(tops, h->w_f.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    return HY_OK;
+}
+
+int hy_index_last_stats(const hy_index* h, hy_search_stats_t* out) {
+    HY_CHECK(h && out, HY_ERR_ARG, "last_stats: NULL argument");
+    *out = h->stats;
+    return HY_OK;
+}
+
+int hy_index_list_size(const hy_index* h, size_t list, size_t* size) {
+    HY_CHECK(h && size, HY_ERR_ARG, "list_size: NULL argument");
+    HY_CHECK(list < h->nlist, HY_ERR_ARG, "list_size: list id out of range");
+    *size = h->h_list_size.empty() ? 0 : (size_t)h->h_list_size[list];
+    return HY_OK;
+}
+
+int hy_index_get_list(const hy_index* hc, size_t list, int64_t* ids, float* codes, float* norms) {
+    HY_CHECK(hc, HY_ERR_ARG, "get_list: NULL handle");
+    HY_CHECK(list < hc->nlist, HY_ERR_ARG, "get_list: list id out of range");
+    hy_index* h = const_cast<hy_index*>(hc);
+    std::lock_guard<std::mutex> g(h->mu);
+    if (h->h_list_size.empty() || h->h_list_size[list] == 0) return HY_OK;
+    HY_RET(set_device(h));
+    const int n = h->h_list_size[list];
+    const int64_t r0 = h->h_list_off[list];
+    cudaStream_t s = h->stream;
+    if (ids) HY_CUDA(cudaMemcpyAsync(ids, h->ids.as<int64_t>() + r0, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (norms) HY_CUDA(cudaMemcpyAsync(norms, h->norms.as<float>() + r0, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (codes) {
+        HY_RET(h->w_f.ensure((size_t)n * h->d * sizeof(float)));
+        HY_CUDA(hy::launch_unpack_list(h->L, h->codes.as<float>(), r0, n, h->w_f.as<float>(), s));
+        HY_CUDA(cudaMemcpyAsync(codes, h->w_f.p, (size_t)n * h->d * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    HY_CUDA(cudaStreamSynchronize(s));
+    return HY_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's .index format (src/Index.cpp:1708-1770, src/IVF.cpp:76-134):
+//   size_t d, size_t nlist, int32 metric, int32 opt_level, size_t sub_k,
+//   size_t sub_nlist, size_t sub_nprobe, float centroids[nlist*d], then for
+//   each non-empty list: size_t list_id, size_t list_size, size_t d,
+//   size_t sub_k, int32 opt_level, size_t ids[list_size],
+//   float codes[list_size*d], float norms[list_size], and the optional
+//   arrays its opt_level carries (skipped on load, never written).
+namespace {
+
+struct FileList {
+    size_t id = 0;
+    std::vector<int64_t> ids;
+    std::vector<float> codes;
+};
+
+struct FileIndex {
+    size_t d = 0, nlist = 0, sub_k = 0, sub_nlist = 1, sub_nprobe = 1;
+    int32_t metric = 1, opt_level = 0;
+    std::vector<float> cent;
+    std::vector<FileList> lists;
+};
+
+template <class T>
+bool rd(std::ifstream& in, T* v, size_t n = 1) {
+    in.read(reinterpret_cast<char*>(v), static_cast<std::streamsize>(sizeof(T) * n));
+    return static_cast<bool>(in);
+}
+
+int read_index_file(const char* path, FileIndex* f, bool with_data) {
+    std::ifstream in(path, std::ios::binary);
+    HY_CHECK(in.is_open(), HY_ERR_IO, std::string("cannot open file ") + path);
+    HY_CHECK(rd(in, &f->d) && rd(in, &f->nlist) && rd(in, &f->metric) && rd(in, &f->opt_level) && rd(in, &f->sub_k) &&
+                 rd(in, &f->sub_nlist) && rd(in, &f->sub_nprobe),
+             HY_ERR_IO, "truncated .index header");
+    HY_CHECK(f->d >= 1 && f->d <= 4096 && f->nlist >= 1 && f->nlist <= (size_t(1) << 24), HY_ERR_IO,
+             "corrupt .index header (d or nlist out of range)");
+    HY_CHECK(f->metric == 0 || f->metric == 1, HY_ERR_IO, "corrupt .index header (metric)");
+    f->cent.resize(f->nlist * f->d);
+    HY_CHECK(rd(in, f->cent.data(), f->cent.size()), HY_ERR_IO, "truncated .index centroids");
+    for (;;) {
+        size_t lid;
+        in.read(reinterpret_cast<char*>(&lid), sizeof(lid));
+        if (in.eof() && in.gcount() == 0) break;
+        HY_CHECK(in.gcount() == sizeof(lid), HY_ERR_IO, "truncated .index list header");
+        HY_CHECK(lid < f->nlist, HY_ERR_IO, "corrupt .index list id");
+        size_t n, d, subk;
+        int32_t opt;
+        HY_CHECK(rd(in, &n) && rd(in, &d) && rd(in, &subk) && rd(in, &opt), HY_ERR_IO, "truncated .index list header");
+        HY_CHECK(d == f->d && n < (size_t(1) << 31), HY_ERR_IO, "corrupt .index list (dimension or size)");
+        FileList L;
+        L.id = lid;
+        std::vector<uint64_t> ids(n);
+        HY_CHECK(rd(in, ids.data(), n), HY_ERR_IO, "truncated .index list ids");
+        std::vector<float> codes;
+        if (with_data) {
+            codes.resize(n * d);
+            HY_CHECK(rd(in, codes.data(), n * d), HY_ERR_IO, "truncated .index list codes");
+        } else {
+            in.seekg(static_cast<std::streamoff>(n * d * sizeof(float)), std::ios::cur);
+        }
+        size_t skip = n * sizeof(float);  // norms (recomputed on load)
+        if ((opt & 1) || (opt & 4)) skip += 2 * n * sizeof(float);
+        if (opt & 2) skip += n * subk * (sizeof(int64_t) + sizeof(float));
+        if (opt & 4) skip += 2 * n * subk * (sizeof(int64_t) + sizeof(float));
+        in.seekg(static_cast<std::streamoff>(skip), std::ios::cur);
+        HY_CHECK(static_cast<bool>(in), HY_ERR_IO, "truncated .index list payload");
+        L.ids.assign(ids.begin(), ids.end());
+        L.codes = std::move(codes);
+        f->lists.push_back(std::move(L));
+    }
+    return HY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metric, int* opt_level, size_t* nonempty_lists,
+                    size_t* ntotal) {
+    HY_CHECK(path, HY_ERR_ARG, "file_inspect: NULL path");
+    FileIndex f;
+    HY_RET(read_index_file(path, &f, false));
+    size_t tot = 0;
+    for (auto& l : f.lists) tot += l.ids.size();
+    if (d) *d = f.d;
+    if (nlist) *nlist = f.nlist;
+    if (metric) *metric = f.metric;
+    if (opt_level) *opt_level = f.opt_level;
+    if (nonempty_lists) *nonempty_lists = f.lists.size();
+    if (ntotal) *ntotal = tot;
+    return HY_OK;
+}
+
+int hy_index_save(const hy_index* hc, const char* path) {
+    HY_CHECK(hc && path, HY_ERR_ARG, "save: NULL argument");
+    HY_CHECK(hc->trained, HY_ERR_STATE, "save: index is not trained");
+    hy_index* h = const_cast<hy_index*>(hc);
+    std::ofstream out(path, std::ios::binary);
+    HY_CHECK(out.is_open(), HY_ERR_IO, std::string("Cannot open file ") + path);
+    auto wr = [&](const void* p, size_t bytes) { out.write(static_cast<const char*>(p), static_cast<std::streamsize>(bytes)); };
+    const int32_t metric = h->metric, opt = 0;
+    wr(&h->d, sizeof(size_t));
+    wr(&h->nlist, sizeof(size_t));
+    wr(&metric, 4);
+    wr(&opt, 4);
+    wr(&h->sub_k, sizeof(size_t));
+    wr(&h->sub_nlist, sizeof(size_t));
+    wr(&h->sub_nprobe, sizeof(size_t));
+    wr(h->h_cent.data(), h->nlist * h->d * sizeof(float));
+    for (size_t l = 0; l < h->nlist && !h->h_list_size.empty(); ++l) {
+        const size_t n = (size_t)h->h_list_size[l];
+        if (n == 0) continue;
+        std::vector<int64_t> ids(n);
+        std::vector<float> codes(n * h->d), norms(n);
+        HY_RET(hy_index_get_list(h, l, ids.data(), codes.data(), norms.data()));
+        // The reference fills candidate_norms only for L2 (src/Index.cpp:689-696).
+        if (h->metric != HY_METRIC_L2) std::fill(norms.begin(), norms.end(), 0.0f);
+        const size_t subk = 0;
+        std::vector<uint64_t> uids(ids.begin(), ids.end());
+        wr(&l, sizeof(size_t));
+        wr(&n, sizeof(size_t));
+        wr(&h->d, sizeof(size_t));
+        wr(&subk, sizeof(size_t));
+        wr(&opt, 4);
+        wr(uids.data(), n * sizeof(uint64_t));
+        wr(codes.data(), n * h->d * sizeof(float));
+        wr(norms.data(), n * sizeof(float));
+    }
+    HY_CHECK(static_cast<bool>(out), HY_ERR_IO, std::string("write failed: ") + path);
+    return HY_OK;
+}
+
+int hy_index_load(hy_index* h, const char* path) {
+    HY_CHECK(h && path, HY_ERR_ARG, "load: NULL argument");
+    FileIndex f;
+    HY_RET(read_index_file(path, &f, true));
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    h->d = f.d;
+    h->nlist = f.nlist;
+    h->metric = f.metric;
+    h->sub_k = f.sub_k;
+    h->sub_nlist = f.sub_nlist;
+    h->sub_nprobe = f.sub_nprobe;
+    h->opt_level = 0;  // load_index resets opt_level (src/Index.cpp:1746)
+    h->dim_blocks = std::min<size_t>(h->dim_blocks ? h->dim_blocks : 4, h->d);
+    h->L = make_layout((int)h->d, (int)h->dim_blocks);
+    HY_RET(h->cent.ensure(h->nlist * h->d * sizeof(float)));
+    h->h_cent = f.cent;
+    HY_CUDA(cudaMemcpyAsync(h->cent.p, h->h_cent.data(), h->nlist * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    h->trained = true;
+    // Rows list by list in file order; a later record of the same list
+    // replaces an earlier one, as load_IVF does.
+    std::vector<const FileList*> byid(h->nlist, nullptr);
+    for (auto& l : f.lists) byid[l.id] = &l;
+    std::vector<int32_t> sizes(h->nlist, 0);
+    size_t n = 0;
+    for (size_t l = 0; l < h->nlist; ++l)
+        if (byid[l]) {
+            sizes[l] = (int32_t)byid[l]->ids.size();
+            n += byid[l]->ids.size();
+        }
+    std::vector<float> rows(std::max<size_t>(n, 1) * h->d);
+    std::vector<int64_t> labels(std::max<size_t>(n, 1)), srcid(std::max<size_t>(n, 1));
+    std::vector<int32_t> order(std::max<size_t>(n, 1));
+    size_t p = 0;
+    for (size_t l = 0; l < h->nlist; ++l) {
+        if (!byid[l]) continue;
+        const FileList& L = *byid[l];
+        std::memcpy(&rows[p * h->d], L.codes.data(), L.codes.size() * sizeof(float));
+        for (size_t i = 0; i < L.ids.size(); ++i) {
+            labels[p + i] = (int64_t)l;
+            srcid[p + i] = L.ids[i];
+            order[p + i] = (int32_t)(p + i);
+        }
+        p += L.ids.size();
+    }
+    HY_RET(h->w_x.ensure(rows.size() * sizeof(float)));
+    HY_RET(h->w_lab.ensure(labels.size() * sizeof(int64_t)));
+    HY_RET(h->w_vals2.ensure(order.size() * sizeof(int32_t)));
+    HY_CUDA(cudaMemcpyAsync(h->w_x.p, rows.data(), rows.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_lab.p, labels.data(), labels.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->w_vals2.p, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    HY_RET(build_arena(h, h->w_x.as<float>(), n, h->w_vals2.as<int32_t>(), h->w_lab.as<int64_t>(), sizes, s));
+    // build_arena stored the row position as the id; restore the file's ids.
+    std::vector<int64_t> arena_ids(std::max<size_t>(h->arena_rows, 32), -1);
+    p = 0;
+    for (size_t l = 0; l < h->nlist; ++l) {
+        for (int32_t i = 0; i < sizes[l]; ++i) arena_ids[h->h_list_off[l] + i] = srcid[p + i];
+        p += sizes[l];
+    }
+    HY_CUDA(cudaMemcpy(h->ids.p, arena_ids.data(), arena_ids.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    return HY_OK;
+}
+
+}  // extern "C"

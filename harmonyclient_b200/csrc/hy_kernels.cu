@@ -1,0 +1,970 @@
+// IVF kernels for B200 (sm_100a): coarse quantisation, selection, warm-up
+// thresholds, the plain FP32 list scan with dimension-block pruning, the final
+// top-k merge, and the index-construction kernels (k-means, add).
+//
+// Arithmetic note: every distance is accumulated dimension by dimension in
+// increasing order with separately rounded multiply and add (__fmul_rn /
+// __fadd_rn, no FMA contraction), so each float result is bit-identical to the
+// project's sequential CPU restatement of the reference (the oracle).  The
+// plain scan accumulates each dimension block from zero and adds the block
+// sums in order, which is the order of the reference's 4-chunk pruning loop
+// (src/node.cpp:640-656).
+#include <cfloat>
+#include <cub/device/device_radix_sort.cuh>
+
+#include "hy_kernels.cuh"
+
+namespace hy {
+
+namespace {
+
+constexpr int METRIC_IP = 0;
+constexpr int METRIC_L2 = 1;
+
+__device__ inline float sq_add(float acc, float a, float b) {
+    const float t = __fsub_rn(a, b);
+    return __fadd_rn(acc, __fmul_rn(t, t));
+}
+__device__ inline float ip_add(float acc, float a, float b) { return __fadd_rn(acc, __fmul_rn(a, b)); }
+
+// ---------------------------------------------------------------------------
+// Coarse scores: out[i][c] = ||q_i - c||^2 (L2) or -<q_i, c> (IP), so that
+// smaller is better for both metrics.  64 queries x 64 centroids per CTA,
+// 4 x 4 outputs per thread, dimensions staged 32 at a time in shared memory.
+// (The reference computes these with IVFScan::lite_scan_codes over all
+// centroids, src/IVFScan.hpp:108-138, src/Index.cpp:985-990.)
+template <int METRIC>
+__global__ void __launch_bounds__(256) coarse_scores_kernel(const float* __restrict__ q, int nq,
+                                                            const float* __restrict__ c, int nlist, int d,
+                                                            float* __restrict__ out) {
+    __shared__ __align__(16) float Qs[32][68];
+    __shared__ __align__(16) float Cs[32][68];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int q0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+
+    for (int d0 = 0; d0 < d; d0 += 32) {
+        for (int i = threadIdx.x; i < 64 * 32; i += 256) {
+            const int r = i >> 5, j = i & 31;
+            const int gj = d0 + j;
+            const int gq = q0 + r, gc = c0 + r;
+            Qs[j][r] = (gq < nq && gj < d) ? q[static_cast<size_t>(gq) * d + gj] : 0.0f;
+            Cs[j][r] = (gc < nlist && gj < d) ? c[static_cast<size_t>(gc) * d + gj] : 0.0f;
+        }
+        __syncthreads();
+        const int jn = min(32, d - d0);
+        for (int j = 0; j < jn; ++j) {
+            const float4 a = *reinterpret_cast<const float4*>(&Qs[j][ty * 4]);
+            const float4 b = *reinterpret_cast<const float4*>(&Cs[j][tx * 4]);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v)
+                    acc[u][v] = METRIC == METRIC_L2 ? sq_add(acc[u][v], av[u], bv[v]) : ip_add(acc[u][v], av[u], bv[v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int gq = q0 + ty * 4 + u;
+        if (gq >= nq) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int gc = c0 + tx * 4 + v;
+            if (gc < nlist) out[static_cast<size_t>(gq) * nlist + gc] = METRIC == METRIC_L2 ? acc[u][v] : -acc[u][v];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CTA-wide radix selection over n ordered uint32 values in shared memory:
+// returns v*, the m-th smallest value (1 <= m <= n), and through *need the
+// number of elements equal to v* that belong to the m smallest.
+__device__ uint32_t cta_radix_select(const uint32_t* vals, int n, int m, int* need, int* hist /*256*/,
+                                     uint32_t* sh /*2*/) {
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        sh[0] = 0;                        // prefix
+        sh[1] = static_cast<uint32_t>(m);  // remaining
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+        for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const uint32_t prefix = sh[0];
+        for (int i = tid; i < n; i += blockDim.x) {
+            const uint32_t v = vals[i];
+            if (pass == 0 || (v >> (shift + 8)) == (prefix >> (shift + 8))) atomicAdd(&hist[(v >> shift) & 255], 1);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            const int lane = tid;
+            int loc[8];
+            int sum = 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                loc[u] = hist[lane * 8 + u];
+                sum += loc[u];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - sum;
+            const int rem = static_cast<int>(sh[1]);
+            const bool mine = excl < rem && incl >= rem;
+            const unsigned who = __ballot_sync(FULL, mine);
+            if (mine) {
+                int cum = excl;
+                int digit = lane * 8 + 7;
+                int before = excl;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (cum + loc[u] >= rem) {
+                        digit = lane * 8 + u;
+                        before = cum;
+                        break;
+                    }
+                    cum += loc[u];
+                }
+                sh[0] = prefix | (static_cast<uint32_t>(digit) << shift);
+                sh[1] = static_cast<uint32_t>(rem - before);
+            }
+            (void)who;
+        }
+        __syncthreads();
+    }
+    const uint32_t v = sh[0];
+    *need = static_cast<int>(sh[1]);
+    __syncthreads();
+    return v;
+}
+
+// Collect the m smallest (value, index) pairs of vals[0..n) as 64-bit keys
+// (value << 32 | index) into sel[0..m): everything below v*, then the `need`
+// lowest-index elements equal to v*.  Order inside sel is unspecified.
+__device__ void cta_collect(const uint32_t* vals, int n, int m, uint32_t vstar, int need, uint64_t* sel,
+                            int* scratch /*34*/) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    int* cnt_lt = scratch;      // [0]
+    int* taken = scratch + 1;   // [1]
+    int* wcnt = scratch + 2;    // [2..33]
+    if (tid == 0) {
+        *cnt_lt = 0;
+        *taken = 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+        const uint32_t v = vals[i];
+        if (v < vstar) {
+            const int pos = atomicAdd(cnt_lt, 1);
+            sel[pos] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(i);
+        }
+    }
+    const int base_eq = m - need;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + tid;
+        const bool f = i < n && vals[i] == vstar;
+        const unsigned b = __ballot_sync(FULL, f);
+        if (lane == 0) wcnt[warp] = __popc(b);
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int c = wcnt[w];
+            if (w < warp) pre += c;
+            tot += c;
+        }
+        const int r = *taken + pre + __popc(b & ((1u << lane) - 1u));
+        if (f && r < need) sel[base_eq + r] = (static_cast<uint64_t>(vstar) << 32) | static_cast<uint32_t>(i);
+        __syncthreads();
+        if (tid == 0) *taken += tot;
+        __syncthreads();
+        if (*taken >= need) break;
+    }
+    __syncthreads();
+}
+
+// In-place ascending bitonic sort of P (power of two) keys in shared memory.
+__device__ void cta_bitonic_sort(uint64_t* a, int P) {
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < P / 2; i += blockDim.x) {
+                const int lo = 2 * i - (i & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint64_t x = a[lo], y = a[hi];
+                if ((x > y) == up) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__host__ __device__ inline int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// Per row of `scores` (n values, smaller is better): the m best, best first,
+// ties broken by lower column.  One CTA per row.
+__global__ void __launch_bounds__(256) select_kernel(const float* __restrict__ scores, int n, int m,
+                                                     int64_t* __restrict__ out_idx, float* __restrict__ out_score) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int P = next_pow2(m);
+    uint64_t* sel = reinterpret_cast<uint64_t*>(sm);
+    uint32_t* vals = reinterpret_cast<uint32_t*>(sel + P);
+    __shared__ int hist[256];
+    __shared__ uint32_t sh[2];
+    __shared__ int scratch[34];
+    const size_t row = blockIdx.x;
+    const float* src = scores + row * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) vals[i] = f2o(src[i]);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) sel[i] = KEY_MAX;
+    __syncthreads();
+    int need;
+    const uint32_t vstar = cta_radix_select(vals, n, m, &need, hist, sh);
+    cta_collect(vals, n, m, vstar, need, sel, scratch);
+    cta_bitonic_sort(sel, P);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const uint64_t key = sel[i];
+        out_idx[row * m + i] = static_cast<int64_t>(key & 0xffffffffu);
+        if (out_score) out_score[row * m + i] = o2f(static_cast<uint32_t>(key >> 32));
+    }
+}
+
+// Per row: the first minimum (lowest column among equal minima), one warp per
+// row — the reference's nearest-centroid rule (strict < in column order,
+// src/IVFScan.hpp:131, src/Clustering.cpp:107).
+__global__ void argmin_kernel(const float* __restrict__ scores, int nrows, int n, int64_t* __restrict__ out_idx,
+                              float* __restrict__ out_score) {
+    const int lane = threadIdx.x & 31;
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (row >= nrows) return;
+    const float* src = scores + row * n;
+    float best = INFINITY;
+    int bi = n;
+    for (int i = lane; i < n; i += 32) {
+        const float v = src[i];
+        if (v < best) {
+            best = v;
+            bi = i;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(FULL, best, o);
+        const int oi = __shfl_xor_sync(FULL, bi, o);
+        if (ob < best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    if (lane == 0) {
+        out_idx[row] = bi < n ? bi : 0;
+        if (out_score) out_score[row] = best;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Copy query `qi` into shared memory in the arena's block-padded layout
+// (block b at boff[b], zero padding up to its pitch).
+__device__ inline void stage_query(const ArenaLayout& L, const float* __restrict__ q, float* qs) {
+    for (int i = threadIdx.x; i < L.row_pitch; i += blockDim.x) {
+        int b = 0;
+        while (b + 1 < L.nb && i >= L.boff[b + 1]) ++b;
+        const int j = i - L.boff[b];
+        const int w = L.bstart[b + 1] - L.bstart[b];
+        qs[i] = j < w ? q[L.bstart[b] + j] : 0.0f;
+    }
+}
+
+// Squared L2 of one arena row against the staged query, read straight from
+// global memory; blockwise = sum each dimension block from zero and add the
+// block sums (the scan's order), else one running sum over all dimensions
+// (the reference's lite_scan_codes order, src/utils.h:480-487).
+__device__ inline float row_l2_global(const ArenaLayout& L, const float* __restrict__ codes, int64_t r,
+                                      const float* qs, bool blockwise) {
+    float total = 0.0f;
+    const int lr = static_cast<int>(r & 31);
+    const float* tile = codes + static_cast<size_t>(r >> 5) * 32 * L.row_pitch;
+    for (int b = 0; b < L.nb; ++b) {
+        const float* rowp = tile + static_cast<size_t>(L.boff[b]) * 32 + static_cast<size_t>(lr) * L.pitch[b];
+        const float* qb = qs + L.boff[b];
+        const int w = L.bstart[b + 1] - L.bstart[b];
+        float s = blockwise ? 0.0f : total;
+        for (int c = 0; c * 4 < w; ++c) {
+            const int pc = (c & ~7) | ((c ^ lr) & 7);
+            const float4 x = __ldg(reinterpret_cast<const float4*>(rowp + pc * 4));
+            const float4 y = *reinterpret_cast<const float4*>(qb + c * 4);
+            const int j = c * 4;
+            s = sq_add(s, y.x, x.x);
+            if (j + 1 < w) s = sq_add(s, y.y, x.y);
+            if (j + 2 < w) s = sq_add(s, y.z, x.z);
+            if (j + 3 < w) s = sq_add(s, y.w, x.w);
+        }
+        total = blockwise ? (b == 0 ? s : __fadd_rn(total, s)) : s;
+    }
+    return total;
+}
+
+// Warm-up thresholds (Index::warmUpSearch, src/Index.cpp:999-1051, and the
+// heapTops read at src/Index.cpp:1300-1303): per query, the k-th smallest L2
+// distance over the first min(wls, |l|) rows of its first min(wl, nprobe)
+// probed lists; FLT_MAX when fewer than k rows were seen.  One CTA per query;
+// distances are collected in shared memory and the k-th found by radix
+// selection.
+__global__ void __launch_bounds__(256) warmup_kernel(ArenaLayout L, const float* __restrict__ codes,
+                                                     const int64_t* __restrict__ list_off,
+                                                     const int32_t* __restrict__ list_size,
+                                                     const float* __restrict__ q, const int64_t* __restrict__ probes,
+                                                     int nprobe, int k, int wl, int wls, int blockwise,
+                                                     uint32_t* __restrict__ out_thr, float* __restrict__ out_f) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    float* qs = reinterpret_cast<float*>(sm);
+    int* rbase = reinterpret_cast<int*>(qs + L.row_pitch);  // [wl+1] prefix of rows
+    int64_t* r0 = reinterpret_cast<int64_t*>(rbase + ((wl + 2) & ~1));
+    uint32_t* vals = reinterpret_cast<uint32_t*>(r0 + wl);
+    __shared__ int hist[256];
+    __shared__ uint32_t sh[2];
+    const int qi = blockIdx.x;
+    const int wle = min(wl, nprobe);
+    stage_query(L, q + static_cast<size_t>(qi) * L.d, qs);
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int j = 0; j < wle; ++j) {
+            const int64_t l = probes[static_cast<size_t>(qi) * nprobe + j];
+            rbase[j] = acc;
+            r0[j] = l >= 0 ? list_off[l] : 0;
+            acc += l >= 0 ? min(wls, static_cast<int>(list_size[l])) : 0;
+        }
+        rbase[wle] = acc;
+    }
+    __syncthreads();
+    const int total = rbase[wle];
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        int j = 0;
+        while (rbase[j + 1] <= i) ++j;
+        const int64_t r = r0[j] + (i - rbase[j]);
+        vals[i] = f2o(row_l2_global(L, codes, r, qs, blockwise != 0));
+    }
+    __syncthreads();
+    float thr = FLT_MAX;
+    if (total >= k) {
+        int need;
+        const uint32_t v = cta_radix_select(vals, total, k, &need, hist, sh);
+        thr = o2f(v);
+    }
+    if (threadIdx.x == 0) {
+        out_thr[qi] = f2o(thr);
+        if (out_f) out_f[qi] = thr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The plain FP32 list scan.
+//
+// Grid: one CTA per (query, split); split s handles probes j = s, s+nsplit, ...
+// (the reference's vector partition across teams becomes a partition of the
+// probe list across CTAs).  Each CTA enumerates the 32-row tiles of its lists
+// and its warps take tiles from a shared counter.  A warp runs S independent
+// tile slots: each slot loads one dimension block of its tile with a bulk
+// copy, accumulates the block into every lane's partial distance (lane = row),
+// prunes rows whose partial exceeds the query's running threshold, and loads
+// the next block only if some row of the tile is still alive — so pruned
+// tiles stop costing HBM bytes (the reference's DIVIDE_DIM / in-rank 4-chunk
+// prune, src/node.cpp:634-657 and 1055-1114, moved inside one kernel).
+// Survivors enter a per-warp candidate buffer; when it fills, the warp merges
+// it into its sorted top-K' (K' = 32*KR >= k) with register bitonic networks
+// and lowers the CTA threshold to its k-th key.  At the end warp 0 merges the
+// warps' lists and writes the CTA's K' best keys.
+//
+// Threshold = min(warm-up threshold, k-th best seen by any warp of this CTA,
+// k-th best published by other splits of the query).  Each is an upper bound
+// on the query's final k-th distance, so pruning (partial > threshold) and
+// admission (distance <= threshold) never drop a row of the exact top-k.
+template <int KR, int S>
+__global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constant__ ScanParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int KP = KR * 32;
+    constexpr int CAP = 2 * KP;
+    const ArenaLayout& L = p.L;
+    const int W = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x / p.nsplit, split = blockIdx.x % p.nsplit;
+    const int npc = (p.nprobe - split + p.nsplit - 1) / p.nsplit;  // probes of this CTA
+    const int npa = ((p.nprobe + p.nsplit - 1) / p.nsplit + 3) & ~3;  // table entries, padded for alignment
+    const size_t slot_floats = static_cast<size_t>(32) * L.max_pitch;
+
+    float* bufs = reinterpret_cast<float*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(bufs + static_cast<size_t>(W) * S * slot_floats);
+    uint64_t* cand = bars + W * S;
+    int64_t* s_row0 = reinterpret_cast<int64_t*>(cand + W * CAP);
+    float* qs = reinterpret_cast<float*>(s_row0 + npa);
+    int* s_size = reinterpret_cast<int*>(qs + L.row_pitch);
+    int* s_pref = s_size + npa;
+    __shared__ unsigned int s_thr;
+    __shared__ int s_next, s_ntiles;
+
+    // --- CTA setup: query, probe table (tile prefix), threshold, barriers.
+    stage_query(L, p.q + static_cast<size_t>(qi) * L.d, qs);
+    if (warp == 0) {
+        int carry = 0;
+        for (int base = 0; base < npc; base += 32) {
+            const int m = base + lane;
+            int tiles = 0;
+            if (m < npc) {
+                const int64_t l = p.probes[static_cast<size_t>(qi) * p.nprobe + split + static_cast<size_t>(m) * p.nsplit];
+                int sz = 0;
+                int64_t r0 = 0;
+                if (l >= 0) {
+                    sz = p.list_size[l];
+                    r0 = p.list_off[l];
+                }
+                s_size[m] = sz;
+                s_row0[m] = r0;
+                tiles = (sz + 31) >> 5;
+            }
+            int incl = tiles;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (m < npc) s_pref[m] = carry + incl;
+            carry += __shfl_sync(FULL, incl, 31);
+        }
+        if (lane == 0) {
+            s_ntiles = carry;
+            s_next = 0;
+            s_thr = p.init_thr ? p.init_thr[qi] : 0xffffffffu;
+        }
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < W * S; ++i) mbar_init(&bars[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int ntiles = s_ntiles;
+    float* wb = bufs + static_cast<size_t>(warp) * S * slot_floats;
+    uint64_t* wbar = bars + warp * S;
+    uint64_t* wc = cand + warp * CAP;
+    const bool l2 = p.metric == METRIC_L2;
+    const bool prune = p.prune && l2;
+
+    uint64_t t[KR];
+#pragma unroll
+    for (int r = 0; r < KR; ++r) t[r] = KEY_MAX;
+    int ccount = 0;
+    unsigned long long loaded = 0, possible = 0;
+    uint32_t gcache = p.g_thr ? p.g_thr[qi] : 0xffffffffu;
+
+    int64_t srow[S];
+    int sblk[S];
+    float spart[S];
+    bool salive[S];
+    uint32_t sphase[S];
+    bool sact[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        srow[s] = 0;
+        sblk[s] = 0;
+        spart[s] = 0.0f;
+        salive[s] = false;
+        sphase[s] = 0;
+        sact[s] = false;
+    }
+
+    auto read_thr = [&]() -> float {
+        const uint32_t a = *reinterpret_cast<volatile unsigned int*>(&s_thr);
+        const uint32_t key = a < gcache ? a : gcache;
+        return key == 0xffffffffu ? INFINITY : o2f(key);
+    };
+
+    auto issue = [&](int s) {
+        const int b = sblk[s];
+        const uint32_t bytes = static_cast<uint32_t>(32 * L.pitch[b] * sizeof(float));
+        const float* src = p.codes + static_cast<size_t>(srow[s] >> 5) * 32 * L.row_pitch + static_cast<size_t>(L.boff[b]) * 32;
+        if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(&wbar[s], bytes);
+            bulk_g2s(wb + static_cast<size_t>(s) * slot_floats, src, bytes, &wbar[s]);
+        }
+        ++loaded;
+    };
+
+    auto grab = [&](int s) -> bool {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(&s_next, 1);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= ntiles) return false;
+        int lo = 0, hi = npc - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_pref[mid] > g)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        const int tprev = lo ? s_pref[lo - 1] : 0;
+        const int tt = g - tprev;
+        srow[s] = s_row0[lo] + 32 * static_cast<int64_t>(tt);
+        const int nvalid = min(32, s_size[lo] - 32 * tt);
+        sblk[s] = 0;
+        spart[s] = 0.0f;
+        salive[s] = lane < nvalid;
+        possible += L.nb;
+        if (p.g_thr) gcache = *reinterpret_cast<volatile unsigned int*>(&p.g_thr[qi]);
+        issue(s);
+        return true;
+    };
+
+    auto flush = [&]() {
+        __syncwarp();
+        for (int base = 0; base < ccount; base += KP) {
+            uint64_t c[KR];
+#pragma unroll
+            for (int r = 0; r < KR; ++r) {
+                const int idx = base + r * 32 + lane;
+                c[r] = idx < ccount ? wc[idx] : KEY_MAX;
+            }
+            warp_sort<KR>(c, lane);
+            warp_merge<KR>(t, c, lane);
+        }
+        __syncwarp();
+        ccount = 0;
+        const uint64_t kth = warp_get<KR>(t, p.k - 1);
+        if (kth != KEY_MAX && lane == 0) {
+            const uint32_t key = static_cast<uint32_t>(kth >> 32);
+            atomicMin(&s_thr, key);
+            if (p.g_thr) atomicMin(&p.g_thr[qi], key);
+        }
+        __syncwarp();
+    };
+
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        sphase[s] = 0;
+        sact[s] = grab(s);
+    }
+
+    for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (!sact[s]) continue;
+            any = true;
+            if (!mbar_wait_bounded(&wbar[s], sphase[s], p.err)) {
+                sact[s] = false;
+                continue;
+            }
+            sphase[s] ^= 1u;
+            const int b = sblk[s];
+            const int P = L.pitch[b];
+            const float* rowp = wb + static_cast<size_t>(s) * slot_floats + lane * P;
+            const float* qb = qs + L.boff[b];
+            float acc = 0.0f;
+            for (int c8 = 0; c8 < (P >> 2); c8 += 8) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const float4 x = *reinterpret_cast<const float4*>(rowp + 4 * (c8 + (u ^ (lane & 7))));
+                    const float4 y = *reinterpret_cast<const float4*>(qb + 4 * (c8 + u));
+                    if (l2) {
+                        acc = sq_add(acc, y.x, x.x);
+                        acc = sq_add(acc, y.y, x.y);
+                        acc = sq_add(acc, y.z, x.z);
+                        acc = sq_add(acc, y.w, x.w);
+                    } else {
+                        acc = ip_add(acc, y.x, x.x);
+                        acc = ip_add(acc, y.y, x.y);
+                        acc = ip_add(acc, y.z, x.z);
+                        acc = ip_add(acc, y.w, x.w);
+                    }
+                }
+            }
+            __syncwarp();
+            spart[s] = b == 0 ? acc : __fadd_rn(spart[s], acc);
+            const float thr = read_thr();
+            if (b + 1 < L.nb) {
+                if (prune) salive[s] = salive[s] && !(spart[s] > thr);
+                if (__any_sync(FULL, salive[s])) {
+                    sblk[s] = b + 1;
+                    issue(s);
+                    continue;
+                }
+            } else {
+                const float score = l2 ? spart[s] : -spart[s];
+                const bool isc = salive[s] && score <= thr;
+                const unsigned bal = __ballot_sync(FULL, isc);
+                if (bal) {
+                    const int nc = __popc(bal);
+                    if (ccount + nc > CAP) flush();
+                    if (isc) {
+                        const int pos = ccount + __popc(bal & ((1u << lane) - 1u));
+                        wc[pos] = (static_cast<uint64_t>(f2o(score)) << 32) |
+                                  static_cast<uint32_t>(srow[s] + lane);
+                    }
+                    ccount += nc;
+                }
+            }
+            sact[s] = grab(s);
+        }
+        if (!any) break;
+    }
+    flush();
+
+    // --- CTA merge of the warps' lists.
+#pragma unroll
+    for (int r = 0; r < KR; ++r) wc[r * 32 + lane] = t[r];
+    if (lane == 0 && p.counters) {
+        atomicAdd(&p.counters[0], loaded);
+        atomicAdd(&p.counters[1], possible);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int w = 1; w < W; ++w) {
+            uint64_t c[KR];
+#pragma unroll
+            for (int r = 0; r < KR; ++r) c[r] = cand[w * CAP + r * 32 + lane];
+            warp_merge<KR>(t, c, lane);
+        }
+        uint64_t* dst = p.out + (static_cast<size_t>(qi) * p.nsplit + split) * KP;
+#pragma unroll
+        for (int r = 0; r < KR; ++r) dst[r * 32 + lane] = t[r];
+    }
+}
+
+// Final merge: per query, the k best of nparts sorted lists of kp keys, then
+// keys -> (distance, id).  Unfilled entries get the reference's heap_init
+// values (FLT_MAX / -FLT_MAX, id -1; src/heap.hpp:13-25).
+__global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__ parts, int nparts, int kp, int k,
+                                                    int metric, const int64_t* __restrict__ ids,
+                                                    float* __restrict__ D, int64_t* __restrict__ I) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    uint64_t* a = reinterpret_cast<uint64_t*>(sm);
+    const size_t qi = blockIdx.x;
+    const int n = nparts * kp;
+    const uint64_t* src = parts + qi * n;
+    const uint64_t* best = src;
+    if (nparts > 1) {
+        const int P = next_pow2(n);
+        for (int i = threadIdx.x; i < P; i += blockDim.x) a[i] = i < n ? src[i] : KEY_MAX;
+        __syncthreads();
+        cta_bitonic_sort(a, P);
+        best = a;
+    }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const uint64_t key = i < n ? best[i] : KEY_MAX;
+        float dv;
+        int64_t iv;
+        if (key == KEY_MAX) {
+            dv = metric == METRIC_L2 ? FLT_MAX : -FLT_MAX;
+            iv = -1;
+        } else {
+            const float sc = o2f(static_cast<uint32_t>(key >> 32));
+            dv = metric == METRIC_L2 ? sc : -sc;
+            iv = ids[key & 0xffffffffu];
+        }
+        D[qi * k + i] = dv;
+        I[qi * k + i] = iv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Index construction kernels.
+__global__ void histogram_kernel(const int64_t* __restrict__ labels, int64_t n, int32_t* __restrict__ counts) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        atomicAdd(&counts[labels[i]], 1);
+}
+
+// Sort key: list id, then the row's score against its centroid (L2 distance,
+// or -IP), so each list is ordered by ascending L2 / descending IP distance to
+// the centroid as Index::add orders it (src/Index.cpp:643-651).
+__global__ void sort_keys_kernel(const int64_t* __restrict__ labels, const float* __restrict__ score, int64_t n,
+                                 uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float s = score[i];
+        keys[i] = (static_cast<uint64_t>(labels[i]) << 32) | f2o(s);
+        vals[i] = static_cast<int32_t>(i);
+    }
+}
+
+// Place sorted row p into its list slot; write id and squared norm (the
+// reference's candidate_norms, src/Index.cpp:689-696, sequential float sum).
+__global__ void scatter_kernel(ArenaLayout L, const float* __restrict__ x, int64_t n, const int32_t* __restrict__ order,
+                               const int64_t* __restrict__ labels, const int64_t* __restrict__ list_start,
+                               const int64_t* __restrict__ list_off, float* __restrict__ codes,
+                               int64_t* __restrict__ ids, float* __restrict__ norms) {
+    const int lane = threadIdx.x & 31;
+    const int64_t p = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (p >= n) return;
+    const int64_t src = order[p];
+    const int64_t l = labels[src];
+    const int64_t r = list_off[l] + (p - list_start[l]);
+    const float* xr = x + src * L.d;
+    for (int b = 0; b < L.nb; ++b) {
+        const int w = L.bstart[b + 1] - L.bstart[b];
+        for (int j = lane; j < w; j += 32) codes[arena_offset(L, r, b, j)] = xr[L.bstart[b] + j];
+    }
+    if (lane == 0) {
+        float s = 0.0f;
+        for (int j = 0; j < L.d; ++j) s = __fadd_rn(s, __fmul_rn(xr[j], xr[j]));
+        ids[r] = src;
+        norms[r] = s;
+    }
+}
+
+__global__ void fill_i64_kernel(int64_t* p, int64_t n, int64_t v) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ x, const int64_t* __restrict__ rows, int64_t n, int d,
+                                   float* __restrict__ out) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n * d;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t r = i / d, j = i % d;
+        out[i] = x[rows[r] * d + j];
+    }
+}
+
+// Rows divided by their L2 norm (sequential float sum), zero rows unchanged
+// (Eigen's colwise().normalized(), src/Clustering.cpp:122).
+__global__ void normalize_rows_kernel(const float* __restrict__ x, int64_t n, int d, float* __restrict__ out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const float* xr = x + i * d;
+    float s = 0.0f;
+    for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(xr[j], xr[j]));
+    const float nr = sqrtf(s);
+    for (int j = 0; j < d; ++j) out[i * d + j] = nr > 0.0f ? __fdiv_rn(xr[j], nr) : xr[j];
+}
+
+// FP64 accumulation of each row into its centroid's sum (one warp per row).
+__global__ void kmeans_accumulate_kernel(const float* __restrict__ x, const int64_t* __restrict__ labels, int64_t n,
+                                         int d, double* __restrict__ sums, unsigned long long* __restrict__ counts) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const int64_t l = labels[i];
+    for (int j = lane; j < d; j += 32) atomicAdd(&sums[l * d + j], static_cast<double>(x[i * d + j]));
+    if (lane == 0) atomicAdd(&counts[l], 1ull);
+}
+
+// Non-empty centroids become the mean of their rows; empty ones keep their
+// previous value (src/Clustering.cpp:146-150).
+__global__ void kmeans_update_kernel(const double* __restrict__ sums, const unsigned long long* __restrict__ counts,
+                                     int nlist, int d, float* __restrict__ cent) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= static_cast<int64_t>(nlist) * d) return;
+    const unsigned long long c = counts[i / d];
+    if (c > 0) cent[i] = static_cast<float>(sums[i] / static_cast<double>(c));
+}
+
+// IP centroids are L2-normalised after training (src/Index.cpp:408-419).
+__global__ void normalize_centroids_kernel(float* cent, int nlist, int d) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nlist) return;
+    float* v = cent + static_cast<size_t>(c) * d;
+    float s = 0.0f;
+    for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(v[j], v[j]));
+    if (s != 0.0f) {
+        const float r = sqrtf(s);
+        for (int j = 0; j < d; ++j) v[j] = __fdiv_rn(v[j], r);
+    }
+}
+
+__global__ void unpack_list_kernel(ArenaLayout L, const float* __restrict__ codes, int64_t row0, int n,
+                                   float* __restrict__ out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= static_cast<int64_t>(n) * L.d) return;
+    const int64_t r = i / L.d;
+    const int j = static_cast<int>(i % L.d);
+    int b = 0;
+    while (b + 1 < L.nb && j >= L.bstart[b + 1]) ++b;
+    out[i] = codes[arena_offset(L, row0 + r, b, j - L.bstart[b])];
+}
+
+inline int grid_for(int64_t n, int threads) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g > (1 << 30)) g = 1 << 30;
+    return static_cast<int>(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+cudaError_t launch_coarse_scores(const float* q, int nq, const float* cent, int nlist, int d, int metric, float* out,
+                                 cudaStream_t s) {
+    dim3 grid((nlist + 63) / 64, (nq + 63) / 64);
+    if (metric == METRIC_L2)
+        coarse_scores_kernel<METRIC_L2><<<grid, 256, 0, s>>>(q, nq, cent, nlist, d, out);
+    else
+        coarse_scores_kernel<METRIC_IP><<<grid, 256, 0, s>>>(q, nq, cent, nlist, d, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select(const float* scores, int nq, int n, int m, int64_t* out_idx, float* out_score,
+                          cudaStream_t s) {
+    const size_t smem = static_cast<size_t>(next_pow2(m)) * 8 + static_cast<size_t>(n) * 4;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    select_kernel<<<nq, 256, smem, s>>>(scores, n, m, out_idx, out_score);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_argmin(const float* scores, int nrows, int n, int64_t* out_idx, float* out_score,
+                          cudaStream_t s) {
+    argmin_kernel<<<grid_for(static_cast<int64_t>(nrows) * 32, 256), 256, 0, s>>>(scores, nrows, n, out_idx,
+                                                                                  out_score);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_t* list_off,
+                          const int32_t* list_size, const float* q, int nq, const int64_t* probes, int nprobe, int k,
+                          int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s) {
+    (void)err;
+    const int wle = wl < nprobe ? wl : nprobe;
+    const size_t smem = static_cast<size_t>(L.row_pitch) * 4 + static_cast<size_t>((wl + 2) & ~1) * 4 +
+                        static_cast<size_t>(wl) * 8 + static_cast<size_t>(wle) * wls * 4;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(warmup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    warmup_kernel<<<nq, 256, smem, s>>>(L, codes, list_off, list_size, q, probes, nprobe, k, wl, wls, blockwise,
+                                        out_thr, out_f);
+    return cudaGetLastError();
+}
+
+template <int KR, int S>
+static cudaError_t launch_scan_t(const ScanParams& p, int W, int* smem_out, cudaStream_t s) {
+    const int npa = ((p.nprobe + p.nsplit - 1) / p.nsplit + 3) & ~3;
+    const size_t smem = static_cast<size_t>(W) * S * 32 * p.L.max_pitch * 4 + static_cast<size_t>(W) * S * 8 +
+                        static_cast<size_t>(W) * 2 * KR * 32 * 8 + static_cast<size_t>(npa) * 8 +
+                        static_cast<size_t>(p.L.row_pitch) * 4 + static_cast<size_t>(npa) * 8;
+    if (smem_out) *smem_out = static_cast<int>(smem);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(scan_plain_kernel<KR, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    scan_plain_kernel<KR, S><<<p.nq * p.nsplit, W * 32, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+// Warps, slots and K' are chosen so that one CTA's shared memory fits: 8 warps
+// with 4 slots for pitches up to 32 floats per block (d <= 128 with 4 blocks),
+// fewer for wider blocks.
+cudaError_t launch_scan_plain(const ScanParams& p, int* smem_out, cudaStream_t s) {
+    const int kr = p.k <= 32 ? 1 : p.k <= 64 ? 2 : p.k <= 128 ? 4 : 8;
+    const int slot_kb = p.L.max_pitch / 8;  // 32 rows x pitch floats, in KiB
+    const int W = slot_kb * 4 * 8 <= 160 ? 8 : 4;
+    const bool four = slot_kb * 4 * W <= 160;
+#define HY_SCAN_CASE(KR)                                                                     \
+    case KR:                                                                                 \
+        return four ? launch_scan_t<KR, 4>(p, W, smem_out, s) : launch_scan_t<KR, 2>(p, W, smem_out, s);
+    switch (kr) {
+        HY_SCAN_CASE(1)
+        HY_SCAN_CASE(2)
+        HY_SCAN_CASE(4)
+        HY_SCAN_CASE(8)
+        default:
+            return cudaErrorInvalidValue;
+    }
+#undef HY_SCAN_CASE
+}
+
+cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int k, int metric, const int64_t* ids,
+                         float* D, int64_t* I, cudaStream_t s) {
+    const size_t smem = nparts > 1 ? static_cast<size_t>(next_pow2(nparts * kp)) * 8 : 0;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_histogram(const int64_t* labels, int64_t n, int32_t* counts, cudaStream_t s) {
+    histogram_kernel<<<grid_for(n, 256), 256, 0, s>>>(labels, n, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_make_sort_keys(const int64_t* labels, const float* score, int64_t n, uint64_t* keys,
+                                  int32_t* vals, cudaStream_t s) {
+    sort_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(labels, score, n, keys, vals);
+    return cudaGetLastError();
+}
+
+cudaError_t radix_sort_pairs(void* tmp, size_t* tmp_bytes, const uint64_t* kin, uint64_t* kout, const int32_t* vin,
+                             int32_t* vout, int64_t n, int end_bit, cudaStream_t s) {
+    return cub::DeviceRadixSort::SortPairs(tmp, *tmp_bytes, kin, kout, vin, vout, static_cast<int>(n), 0, end_bit, s);
+}
+
+cudaError_t launch_scatter(const ArenaLayout& L, const float* x, int64_t n, const int32_t* order,
+                           const int64_t* labels, const int64_t* list_start, const int64_t* list_off, float* codes,
+                           int64_t* ids, float* norms, cudaStream_t s) {
+    scatter_kernel<<<grid_for(n * 32, 256), 256, 0, s>>>(L, x, n, order, labels, list_start, list_off, codes, ids,
+                                                         norms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_i64(int64_t* p, int64_t n, int64_t v, cudaStream_t s) {
+    fill_i64_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const float* x, const int64_t* rows, int64_t n, int d, float* out, cudaStream_t s) {
+    gather_rows_kernel<<<grid_for(n * d, 256), 256, 0, s>>>(x, rows, n, d, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize_rows(const float* x, int64_t n, int d, float* out, cudaStream_t s) {
+    normalize_rows_kernel<<<grid_for(n, 128), 128, 0, s>>>(x, n, d, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kmeans_accumulate(const float* x, const int64_t* labels, int64_t n, int d, double* sums,
+                                     unsigned long long* counts, cudaStream_t s) {
+    kmeans_accumulate_kernel<<<grid_for(n * 32, 256), 256, 0, s>>>(x, labels, n, d, sums, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kmeans_update(const double* sums, const unsigned long long* counts, int nlist, int d,
+                                 float* cent, cudaStream_t s) {
+    kmeans_update_kernel<<<grid_for(static_cast<int64_t>(nlist) * d, 256), 256, 0, s>>>(sums, counts, nlist, d,
+                                                                                        cent);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize_centroids(float* cent, int nlist, int d, cudaStream_t s) {
+    normalize_centroids_kernel<<<grid_for(nlist, 128), 128, 0, s>>>(cent, nlist, d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_list(const ArenaLayout& L, const float* codes, int64_t row0, int n, float* out,
+                               cudaStream_t s) {
+    unpack_list_kernel<<<grid_for(static_cast<int64_t>(n) * L.d, 256), 256, 0, s>>>(L, codes, row0, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hy

@@ -1,0 +1,175 @@
+/*
+ * hy.h — C-ABI of the B200 IVF engine (libhy.so).
+ *
+ * This is the drop-in boundary for Harmony's IVF query path.  Every entry
+ * point takes plain pointers and sizes (no C++ or framework types), returns an
+ * int status (HY_OK on success) and records a message for hy_last_error().
+ * The C++ facade in include/harmony/Index.h wraps these calls back into
+ * Harmony's `harmony::Index` class.  Reference paths below are relative to the
+ * Harmony repository.
+ *
+ * Threading: one handle is used by one host thread at a time; calls on a
+ * handle are serialised (the reference's Index is likewise not reentrant:
+ * search mutates its listidqueries member, src/Index.cpp:969).
+ *
+ * Memory: host-pointer calls copy inputs to the GPU and results back before
+ * returning.  *_device calls take device pointers and a cudaStream_t (passed
+ * as void*) and return once the work is enqueued on that stream.
+ */
+#ifndef HY_H
+#define HY_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HY_API __attribute__((visibility("default")))
+
+typedef struct hy_index hy_index;
+
+/* Status codes.  The reference reports errors by C++ exceptions and exit(1)
+ * (src/Index.cpp:60,464,1644,1737; src/node.cpp:129-134); the facade maps
+ * these codes back to std::runtime_error. */
+enum {
+    HY_OK = 0,
+    HY_ERR_ARG = 1,         /* invalid argument or unsupported size */
+    HY_ERR_OOM = 2,         /* device or host allocation failed */
+    HY_ERR_CUDA = 3,        /* CUDA runtime error, or no usable GPU */
+    HY_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    HY_ERR_STATE = 5,       /* call out of order (e.g. search before add) */
+    HY_ERR_IO = 6,          /* file could not be read or written */
+    HY_ERR_UNSUPPORTED = 7  /* feature not built for this configuration */
+};
+
+/* Metric, same values as harmony::MetricType (src/common.h:20-21). */
+enum { HY_METRIC_IP = 0, HY_METRIC_L2 = 1 };
+
+/* Scan forms selectable with hy_index_set_form. */
+enum {
+    HY_FORM_PLAIN = 0 /* exact FP32 query-major scan with dim-block pruning */
+};
+
+/* Largest k the scan kernels keep per query. The reference's distributed
+ * modes assume k <= 100 (presumeK, src/node.h:89). */
+#define HY_MAX_K 256
+/* Largest number of dimension blocks. */
+#define HY_MAX_DIM_BLOCKS 8
+
+typedef struct {
+    size_t d;           /* vector dimension */
+    size_t nlist;       /* number of inverted lists */
+    size_t nprobe;      /* lists probed per query */
+    int metric;         /* HY_METRIC_* */
+    int opt_level;      /* harmony::OptLevel accepted at creation */
+    size_t dim_blocks;  /* dimension blocks used for partial-distance pruning */
+    size_t ntotal;      /* vectors currently held in the lists */
+    size_t arena_rows;  /* rows in the device arena, padding included */
+    int trained;        /* centroids are set */
+    int device;         /* CUDA device ordinal */
+} hy_index_info_t;
+
+/* Counters of the last search on a handle (the reference returns a Stats
+ * object from Index::search, src/Index.h:82; its pruning counters are
+ * src/stats.h). */
+typedef struct {
+    uint64_t nq;              /* queries searched */
+    uint64_t pairs;           /* (query, probed list) pairs scanned */
+    uint64_t rows;            /* (query, row) pairs in the probed lists */
+    uint64_t tile_blocks;     /* 32-row x one-dim-block tiles loaded */
+    uint64_t tile_blocks_max; /* tiles that a scan without pruning would load */
+    double coarse_ms;         /* device time of coarse quantisation */
+    double scan_ms;           /* device time of the list scan */
+    double merge_ms;          /* device time of the top-k merge */
+    uint64_t launches;        /* kernels this library launched for the call */
+} hy_search_stats_t;
+
+HY_API const char* hy_last_error(void);
+HY_API const char* hy_version(void);
+
+/* Index lifecycle.  Replaces harmony::Index::Index(d, nlist, nprobe, metric,
+ * opt_level, ...) (src/Index.h:15-25, src/Index.cpp:24-43).  opt_level is
+ * accepted for compatibility (callers pass OPT_ALL through sub_k,
+ * src/query.cpp:460); only OPT_NONE scanning is implemented.  dim_blocks is
+ * the number of dimension blocks the partial-distance prune checks between
+ * (the reference hard-codes 4, src/node.cpp:639); 0 selects 4. */
+HY_API int hy_index_create(size_t d, size_t nlist, size_t nprobe, int metric, int opt_level, size_t dim_blocks,
+                           int device, hy_index** out);
+HY_API int hy_index_destroy(hy_index* h);
+HY_API int hy_index_info(const hy_index* h, hy_index_info_t* out);
+
+/* k-means training.  Replaces Index::train (src/Index.cpp:381-425): 20 Lloyd
+ * iterations (2 with lite), seed 6666, at most 256 sample rows per centroid;
+ * centroid sums are accumulated in FP64 on the GPU. */
+HY_API int hy_index_train(hy_index* h, size_t n, const float* x, int lite);
+HY_API int hy_index_train_device(hy_index* h, size_t n, const float* dx, int lite, void* stream);
+
+/* Centroids, the public centroid_codes field of the reference (src/Index.h:118):
+ * nlist x d float32, row-major, host memory. */
+HY_API int hy_index_set_centroids(hy_index* h, const float* centroids);
+HY_API int hy_index_get_centroids(const hy_index* h, float* centroids);
+
+/* Build the inverted lists.  Replaces Index::add (src/Index.cpp:581-697):
+ * lists are rebuilt from scratch on every call; row i of x gets id i; rows
+ * are ordered within a list by distance to the centroid. */
+HY_API int hy_index_add(hy_index* h, size_t n, const float* x);
+HY_API int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream);
+
+HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
+
+/* Warm-up threshold parameters.  Mirrors Index::preSearch's warmUpSearchList /
+ * warmUpSearchListSize (src/Index.h:90, src/Index.cpp:45-55): when
+ * warmup_list > 0, each query's pruning threshold starts at the k-th best
+ * distance among the first warmup_list_size rows of its first warmup_list
+ * probed lists (src/Index.cpp:999-1051).  warmup_list_size 0 means k. */
+HY_API int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_list_size);
+
+/* Search.  Replaces Index::search (src/Index.cpp:1638-1706): D and I are n x k
+ * row-major; each row is sorted best first (ascending L2, descending IP);
+ * unfilled entries hold FLT_MAX (L2) / -FLT_MAX (IP) and id -1
+ * (src/heap.hpp:13-25). */
+HY_API int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I);
+HY_API int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI,
+                                  void* stream);
+
+/* Search with caller-given probe lists (n x nprobe list ids, best first; -1
+ * entries are skipped).  This is the list-scan half of the search
+ * (src/Index.cpp:1450-1547) fed with the master's listidqueries
+ * (src/Index.cpp:969-995). */
+HY_API int hy_index_search_preassigned(hy_index* h, size_t n, const float* q, size_t k, size_t nprobe,
+                                       const int64_t* probes, float* D, int64_t* I);
+
+/* Coarse quantisation only: the nprobe nearest lists of each query, best
+ * first (Index::findNearNprobeOfCentroidIds, src/Index.cpp:899-998). */
+HY_API int hy_index_probes(hy_index* h, size_t n, const float* q, int64_t* probes);
+
+/* Warm-up thresholds only (src/Index.cpp:999-1051 and 1300-1303): for each
+ * query the k-th best full-d L2 distance over the first warmup_list_size rows
+ * of its first warmup_list probed lists, FLT_MAX when fewer than k rows. */
+HY_API int hy_index_warmup_tops(hy_index* h, size_t n, const float* q, size_t k, size_t nprobe,
+                                const int64_t* probes, size_t warmup_list, size_t warmup_list_size, float* tops);
+
+HY_API int hy_index_last_stats(const hy_index* h, hy_search_stats_t* out);
+
+/* Inverted-list access (src/IVF.h:51-58): size, then ids / row-major codes /
+ * squared norms of one list (any output pointer may be NULL). */
+HY_API int hy_index_list_size(const hy_index* h, size_t list, size_t* size);
+HY_API int hy_index_get_list(const hy_index* h, size_t list, int64_t* ids, float* codes, float* norms);
+
+/* Persistence in the reference's binary .index format (Index::save_index /
+ * load_index, src/Index.cpp:1708-1770; IVF::save_IVF / load_IVF,
+ * src/IVF.cpp:76-134). */
+HY_API int hy_index_save(const hy_index* h, const char* path);
+HY_API int hy_index_load(hy_index* h, const char* path);
+
+/* Reads the header and list table of a .index file without a GPU. */
+HY_API int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metric, int* opt_level,
+                           size_t* nonempty_lists, size_t* ntotal);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HY_H */

@@ -1,0 +1,36 @@
+// Declarations-only stand-in for MPI, used only to compile the reference's
+// Index.cpp / node.cpp into the oracle library.  The oracle drives the
+// reference's single-process code (ORIGINAL search, add, train, warm-up and
+// the BaseWorker 4-chunk pruning loop); none of those call MPI.  The bodies
+// in ref_mpi_stub.cpp report an error if any MPI routine is reached.
+#pragma once
+typedef int MPI_Comm;
+typedef int MPI_Datatype;
+typedef int MPI_Request;
+typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
+#define MPI_COMM_WORLD 0
+#define MPI_BYTE 1
+#define MPI_INT 2
+#define MPI_FLOAT 3
+#define MPI_DOUBLE 4
+#define MPI_INT64_T 5
+#define MPI_TAG_UB 1
+#define MPI_STATUS_IGNORE ((MPI_Status*)0)
+#define MPI_STATUSES_IGNORE ((MPI_Status*)0)
+#ifdef __cplusplus
+extern "C" {
+#endif
+int MPI_Abort(MPI_Comm, int);
+int MPI_Barrier(MPI_Comm);
+int MPI_Bcast(void*, int, MPI_Datatype, int, MPI_Comm);
+int MPI_Comm_get_attr(MPI_Comm, int, void*, int*);
+int MPI_Irecv(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request*);
+int MPI_Isend(const void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request*);
+int MPI_Recv(void*, int, MPI_Datatype, int, int, MPI_Comm, MPI_Status*);
+int MPI_Send(const void*, int, MPI_Datatype, int, int, MPI_Comm);
+int MPI_Test(MPI_Request*, int*, MPI_Status*);
+int MPI_Wait(MPI_Request*, MPI_Status*);
+int MPI_Waitall(int, MPI_Request*, MPI_Status*);
+#ifdef __cplusplus
+}
+#endif
