@@ -140,6 +140,9 @@ def run_ours(args, rank, world, dist):
     t0 = time.perf_counter()
     idx.train(x)
     idx.add(x)
+    # Warm-up thresholds as the reference's default run uses them
+    # (--warmup_list 10, warmup_list_size = k; src/query.cpp:845-847).
+    idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
     build_s = time.perf_counter() - t0
     cent = idx.centroid_codes
 
@@ -255,6 +258,7 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches) * args.steps,
+        "warmup_list": args.warmup_list,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "build_s": round(build_s, 2),
@@ -310,6 +314,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nprobe", type=int, default=64)
+    ap.add_argument("--warmup-list", type=int, default=10)
     ap.add_argument("--nb", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--recall-sample", type=int, default=200)

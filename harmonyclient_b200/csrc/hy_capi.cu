@@ -567,7 +567,7 @@ int hy_index_train_device(hy_index* h, size_t n, const float* dx, int lite, void
     HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "train: NULL argument");
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
-    return train_impl(h, n, dx, true, lite, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+    return train_impl(h, n, dx, true, lite, static_cast<cudaStream_t>(stream));
 }
 
 int hy_index_set_centroids(hy_index* h, const float* c) {
@@ -600,7 +600,7 @@ int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream) {
     HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "add: NULL argument");
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
-    return add_impl(h, n, dx, true, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+    return add_impl(h, n, dx, true, static_cast<cudaStream_t>(stream));
 }
 
 int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
@@ -623,8 +623,13 @@ int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, flo
     if (n == 0) return HY_OK;
     HY_RET(check_search_args(h, n, k));
     HY_RET(set_device(h));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-    return search_device_impl(h, n, dq, k, dD, dI, s, false);
+    // The caller's stream as given: NULL is the CUDA default stream.
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HY_RET(ensure_common(h));
+    h->launches = 0;
+    HY_RET(search_device_impl(h, n, dq, k, dD, dI, s, false));
+    h->stats.launches = h->launches;
+    return HY_OK;
 }
 
 int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {

@@ -386,17 +386,19 @@ __global__ void __launch_bounds__(256) warmup_kernel(ArenaLayout L, const float*
 // the next block only if some row of the tile is still alive — so pruned
 // tiles stop costing HBM bytes (the reference's DIVIDE_DIM / in-rank 4-chunk
 // prune, src/node.cpp:634-657 and 1055-1114, moved inside one kernel).
-// Survivors enter a per-warp candidate buffer; when it fills, the warp merges
-// it into its sorted top-K' (K' = 32*KR >= k) with register bitonic networks
-// and lowers the CTA threshold to its k-th key.  At the end warp 0 merges the
-// warps' lists and writes the CTA's K' best keys.
+// Survivors enter a per-warp candidate buffer.  The CTA keeps one sorted
+// top-K' (K' = 32*KR >= k) in shared memory; a warp whose buffer fills takes
+// the CTA's merge lock, merges its candidates into that list with register
+// bitonic networks and lowers the CTA threshold to the list's k-th key, so
+// the threshold reflects every row the CTA has seen.  At the end the list
+// holds the CTA's K' best keys.
 //
-// Threshold = min(warm-up threshold, k-th best seen by any warp of this CTA,
-// k-th best published by other splits of the query).  Each is an upper bound
+// Threshold = min(warm-up threshold, the CTA list's k-th key, the k-th key
+// published by other splits of the query).  Each is an upper bound
 // on the query's final k-th distance, so pruning (partial > threshold) and
 // admission (distance <= threshold) never drop a row of the exact top-k.
 template <int KR, int S>
-__global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constant__ ScanParams p) {
+__global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constant__ ScanParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int KP = KR * 32;
     constexpr int CAP = 2 * KP;
@@ -411,12 +413,13 @@ __global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constan
     float* bufs = reinterpret_cast<float*>(smem);
     uint64_t* bars = reinterpret_cast<uint64_t*>(bufs + static_cast<size_t>(W) * S * slot_floats);
     uint64_t* cand = bars + W * S;
-    int64_t* s_row0 = reinterpret_cast<int64_t*>(cand + W * CAP);
+    uint64_t* ctop = cand + W * CAP;  // the CTA's sorted top-K'
+    int64_t* s_row0 = reinterpret_cast<int64_t*>(ctop + KP);
     float* qs = reinterpret_cast<float*>(s_row0 + npa);
     int* s_size = reinterpret_cast<int*>(qs + L.row_pitch);
     int* s_pref = s_size + npa;
     __shared__ unsigned int s_thr;
-    __shared__ int s_next, s_ntiles;
+    __shared__ int s_next, s_ntiles, s_lock;
 
     // --- CTA setup: query, probe table (tile prefix), threshold, barriers.
     stage_query(L, p.q + static_cast<size_t>(qi) * L.d, qs);
@@ -449,9 +452,11 @@ __global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constan
         if (lane == 0) {
             s_ntiles = carry;
             s_next = 0;
+            s_lock = 0;
             s_thr = p.init_thr ? p.init_thr[qi] : 0xffffffffu;
         }
     }
+    for (int i = threadIdx.x; i < KP; i += blockDim.x) ctop[i] = KEY_MAX;
     if (threadIdx.x == 0) {
         for (int i = 0; i < W * S; ++i) mbar_init(&bars[i], 1);
         fence_mbar_init();
@@ -465,9 +470,6 @@ __global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constan
     const bool l2 = p.metric == METRIC_L2;
     const bool prune = p.prune && l2;
 
-    uint64_t t[KR];
-#pragma unroll
-    for (int r = 0; r < KR; ++r) t[r] = KEY_MAX;
     int ccount = 0;
     unsigned long long loaded = 0, possible = 0;
     uint32_t gcache = p.g_thr ? p.g_thr[qi] : 0xffffffffu;
@@ -532,27 +534,52 @@ __global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constan
         return true;
     };
 
+    // Merge this warp's candidates into the CTA list under the merge lock
+    // (bounded spin; on timeout the device status word is raised).
     auto flush = [&]() {
         __syncwarp();
-        for (int base = 0; base < ccount; base += KP) {
-            uint64_t c[KR];
-#pragma unroll
-            for (int r = 0; r < KR; ++r) {
-                const int idx = base + r * 32 + lane;
-                c[r] = idx < ccount ? wc[idx] : KEY_MAX;
+        int got = 0;
+        if (lane == 0) {
+            for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+                if (atomicCAS(&s_lock, 0, 1) == 0) {
+                    got = 1;
+                    break;
+                }
+                __nanosleep(32);
             }
-            warp_sort<KR>(c, lane);
-            warp_merge<KR>(t, c, lane);
+            if (!got) atomicCAS(p.err, 0, DEV_ERR_TIMEOUT);
+        }
+        got = __shfl_sync(FULL, got, 0);
+        if (got) {
+            __threadfence_block();
+            volatile uint64_t* vt = ctop;
+            uint64_t t[KR];
+#pragma unroll
+            for (int r = 0; r < KR; ++r) t[r] = vt[r * 32 + lane];
+            for (int base = 0; base < ccount; base += KP) {
+                uint64_t c[KR];
+#pragma unroll
+                for (int r = 0; r < KR; ++r) {
+                    const int idx = base + r * 32 + lane;
+                    c[r] = idx < ccount ? wc[idx] : KEY_MAX;
+                }
+                warp_sort<KR>(c, lane);
+                warp_merge<KR>(t, c, lane);
+            }
+#pragma unroll
+            for (int r = 0; r < KR; ++r) vt[r * 32 + lane] = t[r];
+            const uint64_t kth = warp_get<KR>(t, p.k - 1);
+            if (kth != KEY_MAX && lane == 0) {
+                const uint32_t key = static_cast<uint32_t>(kth >> 32);
+                atomicMin(&s_thr, key);
+                if (p.g_thr) atomicMin(&p.g_thr[qi], key);
+            }
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) atomicExch(&s_lock, 0);
         }
         __syncwarp();
         ccount = 0;
-        const uint64_t kth = warp_get<KR>(t, p.k - 1);
-        if (kth != KEY_MAX && lane == 0) {
-            const uint32_t key = static_cast<uint32_t>(kth >> 32);
-            atomicMin(&s_thr, key);
-            if (p.g_thr) atomicMin(&p.g_thr[qi], key);
-        }
-        __syncwarp();
     };
 
 #pragma unroll
@@ -561,90 +588,153 @@ __global__ void __launch_bounds__(256, 1) scan_plain_kernel(const __grid_constan
         sact[s] = grab(s);
     }
 
+    // Accumulate the staged block of slot s into one partial sum per lane
+    // (lane = row), dimension by dimension.
+    auto block_sum = [&](int s) -> float {
+        const int b = sblk[s];
+        const int P = L.pitch[b];
+        const float* rowp = wb + static_cast<size_t>(s) * slot_floats + lane * P;
+        const float* qb = qs + L.boff[b];
+        float acc = 0.0f;
+        for (int c8 = 0; c8 < (P >> 2); c8 += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const float4 x = *reinterpret_cast<const float4*>(rowp + 4 * (c8 + (u ^ (lane & 7))));
+                const float4 y = *reinterpret_cast<const float4*>(qb + 4 * (c8 + u));
+                if (l2) {
+                    acc = sq_add(acc, y.x, x.x);
+                    acc = sq_add(acc, y.y, x.y);
+                    acc = sq_add(acc, y.z, x.z);
+                    acc = sq_add(acc, y.w, x.w);
+                } else {
+                    acc = ip_add(acc, y.x, x.x);
+                    acc = ip_add(acc, y.y, x.y);
+                    acc = ip_add(acc, y.z, x.z);
+                    acc = ip_add(acc, y.w, x.w);
+                }
+            }
+        }
+        return acc;
+    };
+
+    // The same for two slots whose blocks have equal pitch, interleaved so
+    // the two dependent add chains overlap.
+    auto block_sum2 = [&](int s0, int s1, float& a0, float& a1) {
+        const int b0 = sblk[s0], b1 = sblk[s1];
+        const int P = L.pitch[b0];
+        const float* r0 = wb + static_cast<size_t>(s0) * slot_floats + lane * P;
+        const float* r1 = wb + static_cast<size_t>(s1) * slot_floats + lane * P;
+        const float* q0 = qs + L.boff[b0];
+        const float* q1 = qs + L.boff[b1];
+        float acc0 = 0.0f, acc1 = 0.0f;
+        for (int c8 = 0; c8 < (P >> 2); c8 += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int pc = 4 * (c8 + (u ^ (lane & 7)));
+                const float4 x0 = *reinterpret_cast<const float4*>(r0 + pc);
+                const float4 x1 = *reinterpret_cast<const float4*>(r1 + pc);
+                const float4 y0 = *reinterpret_cast<const float4*>(q0 + 4 * (c8 + u));
+                const float4 y1 = *reinterpret_cast<const float4*>(q1 + 4 * (c8 + u));
+                if (l2) {
+                    acc0 = sq_add(acc0, y0.x, x0.x);
+                    acc1 = sq_add(acc1, y1.x, x1.x);
+                    acc0 = sq_add(acc0, y0.y, x0.y);
+                    acc1 = sq_add(acc1, y1.y, x1.y);
+                    acc0 = sq_add(acc0, y0.z, x0.z);
+                    acc1 = sq_add(acc1, y1.z, x1.z);
+                    acc0 = sq_add(acc0, y0.w, x0.w);
+                    acc1 = sq_add(acc1, y1.w, x1.w);
+                } else {
+                    acc0 = ip_add(acc0, y0.x, x0.x);
+                    acc1 = ip_add(acc1, y1.x, x1.x);
+                    acc0 = ip_add(acc0, y0.y, x0.y);
+                    acc1 = ip_add(acc1, y1.y, x1.y);
+                    acc0 = ip_add(acc0, y0.z, x0.z);
+                    acc1 = ip_add(acc1, y1.z, x1.z);
+                    acc0 = ip_add(acc0, y0.w, x0.w);
+                    acc1 = ip_add(acc1, y1.w, x1.w);
+                }
+            }
+        }
+        a0 = acc0;
+        a1 = acc1;
+    };
+
+    // After slot s's block is summed: prune and continue the tile, or emit
+    // candidates and take the next tile.
+    auto post = [&](int s, float acc) {
+        const int b = sblk[s];
+        spart[s] = b == 0 ? acc : __fadd_rn(spart[s], acc);
+        const float thr = read_thr();
+        if (b + 1 < L.nb) {
+            if (prune) salive[s] = salive[s] && !(spart[s] > thr);
+            if (__any_sync(FULL, salive[s])) {
+                sblk[s] = b + 1;
+                issue(s);
+                return;
+            }
+        } else {
+            const float score = l2 ? spart[s] : -spart[s];
+            const bool isc = salive[s] && score <= thr;
+            const unsigned bal = __ballot_sync(FULL, isc);
+            if (bal) {
+                const int nc = __popc(bal);
+                // Merge once 32 candidates are buffered (or the buffer would
+                // overflow), so the CTA threshold follows the scan closely.
+                if (ccount + nc > CAP || ccount >= 32) flush();
+                if (isc) {
+                    const int pos = ccount + __popc(bal & ((1u << lane) - 1u));
+                    wc[pos] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(srow[s] + lane);
+                }
+                ccount += nc;
+            }
+        }
+        sact[s] = grab(s);
+    };
+
     for (;;) {
         bool any = false;
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            if (!sact[s]) continue;
+        for (int s0 = 0; s0 < S; s0 += 2) {
+            const int s1 = s0 + 1;
+            bool ok0 = sact[s0], ok1 = sact[s1];
+            if (!(ok0 || ok1)) continue;
             any = true;
-            if (!mbar_wait_bounded(&wbar[s], sphase[s], p.err)) {
-                sact[s] = false;
-                continue;
+            if (ok0 && !mbar_wait_bounded(&wbar[s0], sphase[s0], p.err)) {
+                sact[s0] = false;
+                ok0 = false;
             }
-            sphase[s] ^= 1u;
-            const int b = sblk[s];
-            const int P = L.pitch[b];
-            const float* rowp = wb + static_cast<size_t>(s) * slot_floats + lane * P;
-            const float* qb = qs + L.boff[b];
-            float acc = 0.0f;
-            for (int c8 = 0; c8 < (P >> 2); c8 += 8) {
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const float4 x = *reinterpret_cast<const float4*>(rowp + 4 * (c8 + (u ^ (lane & 7))));
-                    const float4 y = *reinterpret_cast<const float4*>(qb + 4 * (c8 + u));
-                    if (l2) {
-                        acc = sq_add(acc, y.x, x.x);
-                        acc = sq_add(acc, y.y, x.y);
-                        acc = sq_add(acc, y.z, x.z);
-                        acc = sq_add(acc, y.w, x.w);
-                    } else {
-                        acc = ip_add(acc, y.x, x.x);
-                        acc = ip_add(acc, y.y, x.y);
-                        acc = ip_add(acc, y.z, x.z);
-                        acc = ip_add(acc, y.w, x.w);
-                    }
-                }
+            if (ok1 && !mbar_wait_bounded(&wbar[s1], sphase[s1], p.err)) {
+                sact[s1] = false;
+                ok1 = false;
+            }
+            float a0 = 0.0f, a1 = 0.0f;
+            if (ok0 && ok1 && L.pitch[sblk[s0]] == L.pitch[sblk[s1]]) {
+                block_sum2(s0, s1, a0, a1);
+            } else {
+                if (ok0) a0 = block_sum(s0);
+                if (ok1) a1 = block_sum(s1);
             }
             __syncwarp();
-            spart[s] = b == 0 ? acc : __fadd_rn(spart[s], acc);
-            const float thr = read_thr();
-            if (b + 1 < L.nb) {
-                if (prune) salive[s] = salive[s] && !(spart[s] > thr);
-                if (__any_sync(FULL, salive[s])) {
-                    sblk[s] = b + 1;
-                    issue(s);
-                    continue;
-                }
-            } else {
-                const float score = l2 ? spart[s] : -spart[s];
-                const bool isc = salive[s] && score <= thr;
-                const unsigned bal = __ballot_sync(FULL, isc);
-                if (bal) {
-                    const int nc = __popc(bal);
-                    if (ccount + nc > CAP) flush();
-                    if (isc) {
-                        const int pos = ccount + __popc(bal & ((1u << lane) - 1u));
-                        wc[pos] = (static_cast<uint64_t>(f2o(score)) << 32) |
-                                  static_cast<uint32_t>(srow[s] + lane);
-                    }
-                    ccount += nc;
-                }
+            if (ok0) {
+                sphase[s0] ^= 1u;
+                post(s0, a0);
             }
-            sact[s] = grab(s);
+            if (ok1) {
+                sphase[s1] ^= 1u;
+                post(s1, a1);
+            }
         }
         if (!any) break;
     }
-    flush();
-
-    // --- CTA merge of the warps' lists.
-#pragma unroll
-    for (int r = 0; r < KR; ++r) wc[r * 32 + lane] = t[r];
+    if (ccount > 0) flush();
     if (lane == 0 && p.counters) {
         atomicAdd(&p.counters[0], loaded);
         atomicAdd(&p.counters[1], possible);
     }
     __syncthreads();
-    if (warp == 0) {
-        for (int w = 1; w < W; ++w) {
-            uint64_t c[KR];
-#pragma unroll
-            for (int r = 0; r < KR; ++r) c[r] = cand[w * CAP + r * 32 + lane];
-            warp_merge<KR>(t, c, lane);
-        }
-        uint64_t* dst = p.out + (static_cast<size_t>(qi) * p.nsplit + split) * KP;
-#pragma unroll
-        for (int r = 0; r < KR; ++r) dst[r * 32 + lane] = t[r];
-    }
+    uint64_t* dst = p.out + (static_cast<size_t>(qi) * p.nsplit + split) * KP;
+    for (int i = threadIdx.x; i < KP; i += blockDim.x) dst[i] = ctop[i];
 }
 
 // Final merge: per query, the k best of nparts sorted lists of kp keys, then
@@ -859,7 +949,8 @@ template <int KR, int S>
 static cudaError_t launch_scan_t(const ScanParams& p, int W, int* smem_out, cudaStream_t s) {
     const int npa = ((p.nprobe + p.nsplit - 1) / p.nsplit + 3) & ~3;
     const size_t smem = static_cast<size_t>(W) * S * 32 * p.L.max_pitch * 4 + static_cast<size_t>(W) * S * 8 +
-                        static_cast<size_t>(W) * 2 * KR * 32 * 8 + static_cast<size_t>(npa) * 8 +
+                        static_cast<size_t>(W) * 2 * KR * 32 * 8 + static_cast<size_t>(KR) * 32 * 8 +
+                        static_cast<size_t>(npa) * 8 +
                         static_cast<size_t>(p.L.row_pitch) * 4 + static_cast<size_t>(npa) * 8;
     if (smem_out) *smem_out = static_cast<int>(smem);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
@@ -870,17 +961,16 @@ static cudaError_t launch_scan_t(const ScanParams& p, int W, int* smem_out, cuda
     return cudaGetLastError();
 }
 
-// Warps, slots and K' are chosen so that one CTA's shared memory fits: 8 warps
-// with 4 slots for pitches up to 32 floats per block (d <= 128 with 4 blocks),
-// fewer for wider blocks.
+// Warps, slots and K' are chosen so that one CTA's shared memory fits: 16
+// warps with 2 slots each for pitches up to 32 floats per block (d <= 128
+// with 4 blocks), 8 warps for wider blocks.  Slots are processed in pairs.
 cudaError_t launch_scan_plain(const ScanParams& p, int* smem_out, cudaStream_t s) {
     const int kr = p.k <= 32 ? 1 : p.k <= 64 ? 2 : p.k <= 128 ? 4 : 8;
     const int slot_kb = p.L.max_pitch / 8;  // 32 rows x pitch floats, in KiB
-    const int W = slot_kb * 4 * 8 <= 160 ? 8 : 4;
-    const bool four = slot_kb * 4 * W <= 160;
-#define HY_SCAN_CASE(KR)                                                                     \
-    case KR:                                                                                 \
-        return four ? launch_scan_t<KR, 4>(p, W, smem_out, s) : launch_scan_t<KR, 2>(p, W, smem_out, s);
+    const int W = slot_kb * 2 * 16 <= 128 ? 16 : slot_kb * 2 * 8 <= 160 ? 8 : 4;
+#define HY_SCAN_CASE(KR) \
+    case KR:             \
+        return launch_scan_t<KR, 2>(p, W, smem_out, s);
     switch (kr) {
         HY_SCAN_CASE(1)
         HY_SCAN_CASE(2)

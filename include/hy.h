@@ -14,7 +14,8 @@
  *
  * Memory: host-pointer calls copy inputs to the GPU and results back before
  * returning.  *_device calls take device pointers and a cudaStream_t (passed
- * as void*) and return once the work is enqueued on that stream.
+ * as void*; NULL is the CUDA default stream) and return once the work is
+ * enqueued on that stream.
  */
 #ifndef HY_H
 #define HY_H
