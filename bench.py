@@ -33,12 +33,14 @@ METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan 
 
 
 def peaks():
+    """(HBM GB/s, dense bf16 TFLOP/s burst, which) from MEASURED_PEAKS.json,
+    else the pool's earlier fallback measurement."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
             j = json.load(f)
-        return j.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        return j.get("hbm_gbs", 6650.0), j.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
 
 
 class Clocks:
@@ -143,6 +145,7 @@ def run_ours(args, rank, world, dist):
     # Warm-up thresholds as the reference's default run uses them
     # (--warmup_list 10, warmup_list_size = k; src/query.cpp:845-847).
     idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
+    idx.set_form(args.form)
     build_s = time.perf_counter() - t0
     cent = idx.centroid_codes
 
@@ -191,12 +194,13 @@ def run_ours(args, rank, world, dist):
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    scan_ms, loaded, possible, launches = [], 0, 0, 0
+    scan_ms, loaded, possible, launches, fallback = [], 0, 0, 0, 0
     for _ in range(args.steps):
         e2e_step()
         st = idx.last_stats()
         scan_ms.append(st["scan_ms"])
         loaded, possible, launches = st["tile_blocks"], st["tile_blocks_max"], st["launches"]
+        fallback = max(fallback, st["fallback_queries"])
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], device="cuda")
     if dist:
@@ -215,9 +219,23 @@ def run_ours(args, rank, world, dist):
     pair_rows = int(sizes[P].sum())
     alg_bytes = pair_rows * 128 * 4 + q.shape[0] * 128 * 4 + q.shape[0] * k * 12
     scan_avg = statistics.mean(scan_ms)
-    peak, peak_kind = peaks()
-    achieved = alg_bytes / (scan_avg / 1e3) / 1e9
-    loaded_bytes = loaded * 32 * 32 * 4
+    hbm_peak, tc_peak, peak_kind = peaks()
+    if args.form == "plain":
+        achieved = alg_bytes / (scan_avg / 1e3) / 1e9
+        loaded_bytes = loaded * 32 * 32 * 4
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "scan_plain_kernel", "kernel_ms": round(scan_avg, 4), "algorithmic_bytes": alg_bytes,
+                "loaded_bytes": loaded_bytes, "loaded_frac_of_unpruned": round(loaded / max(possible, 1), 4)}
+    else:
+        # Algorithmic work of the batched scan: one 2*d-flop inner product per
+        # (query, probed row) pair, on the bf16 tensor cores.
+        alg_flops = pair_rows * 2 * 128
+        achieved = alg_flops / (scan_avg / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": tc_peak, "unit": "TFLOP/s",
+                "frac": round(achieved / tc_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "batched_scan_kernel", "kernel_ms": round(scan_avg, 4), "algorithmic_flops": alg_flops,
+                "pair_bytes_fp32": alg_bytes}
 
     # recall@10 against FP64 brute force on a query sample
     from oracle import port
@@ -243,22 +261,19 @@ def run_ours(args, rank, world, dist):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Gaussian mixture, integer-valued in [0,255])",
-        "form": "plain FP32 scan, 4 dimension blocks with partial-distance pruning",
+        "form": args.form,
         "config": {"workload": f"{args.nb} x 128 uint8-valued gmm, nlist {nlist}, nprobe {args.nprobe}, "
                                f"k {k}, {q.shape[0]} queries per step per GPU",
                    "nb": args.nb, "d": 128, "nlist": nlist, "nprobe": args.nprobe, "k": k, "nq": q.shape[0],
                    "l2_flush": "not needed: list arena larger than L2", "parallelism": f"replicas x{world}"},
         "recall_at_10": round(recall10, 4),
         "recall_sample": ns,
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "scan_plain_kernel", "kernel_ms": round(scan_avg, 4),
-                     "algorithmic_bytes": alg_bytes, "loaded_bytes": loaded_bytes,
-                     "loaded_frac_of_unpruned": round(loaded / max(possible, 1), 4)},
+        "roofline": roof,
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches) * args.steps,
         "warmup_list": args.warmup_list,
+        "fallback_queries": fallback,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "build_s": round(build_s, 2),
@@ -315,6 +330,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nprobe", type=int, default=64)
     ap.add_argument("--warmup-list", type=int, default=10)
+    ap.add_argument("--form", default="bf16", choices=["plain", "bf16"])
     ap.add_argument("--nb", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--recall-sample", type=int, default=200)

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libhy.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "hy.h")
 
 HY_OK, HY_ERR_ARG, HY_ERR_OOM, HY_ERR_CUDA, HY_ERR_TIMEOUT, HY_ERR_STATE, HY_ERR_IO, HY_ERR_UNSUPPORTED = range(8)
+HY_FORM_PLAIN, HY_FORM_BF16 = 0, 1
 HY_MAX_K = 256
 
 
@@ -30,7 +31,7 @@ class IndexInfo(C.Structure):
 class SearchStats(C.Structure):
     _fields_ = [("nq", C.c_uint64), ("pairs", C.c_uint64), ("rows", C.c_uint64), ("tile_blocks", C.c_uint64),
                 ("tile_blocks_max", C.c_uint64), ("coarse_ms", C.c_double), ("scan_ms", C.c_double),
-                ("merge_ms", C.c_double), ("launches", C.c_uint64)]
+                ("merge_ms", C.c_double), ("launches", C.c_uint64), ("fallback_queries", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -68,6 +69,8 @@ def load():
     L.hy_index_add_device.argtypes = [H, sz, vp, vp]
     L.hy_index_set_nprobe.argtypes = [H, sz]
     L.hy_index_presearch.argtypes = [H, sz, sz]
+    L.hy_index_set_form.argtypes = [H, i]
+    L.hy_index_set_batch_params.argtypes = [H, sz, sz, sz]
     L.hy_index_search.argtypes = [H, sz, vp, sz, vp, vp]
     L.hy_index_search_device.argtypes = [H, sz, vp, sz, vp, vp, vp]
     L.hy_index_search_preassigned.argtypes = [H, sz, vp, sz, sz, vp, vp, vp]
@@ -80,6 +83,7 @@ def load():
     L.hy_index_load.argtypes = [H, C.c_char_p]
     L.hy_file_inspect.argtypes = [C.c_char_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
     _lib = L
     return L
 

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/hy.h"
+#include "hy_batched.cuh"
 #include "hy_kernels.cuh"
 
 using hy::ArenaLayout;
@@ -134,6 +135,17 @@ struct hy_index {
     cudaEvent_t ev[6] = {};
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
+
+    // bf16 (batched tensor-core) form
+    int form = HY_FORM_PLAIN;
+    size_t capq = 8192;       // candidate slots per query
+    size_t oversample = 4;    // exact re-rank of oversample * k candidates
+    size_t row_slice = 2048;  // rows per work item
+    int nsm = 0;
+    DevBuf abf;               // bf16 tensor-core image of the arena
+    DevBuf xaux;              // per arena row {|x~|, |x - x~|}
+    bool abf_valid = false;
+    DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf;
 };
 
 namespace {
@@ -266,10 +278,14 @@ int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, con
     std::vector<int64_t> start(nlist + 1, 0);
     for (size_t l = 0; l < nlist; ++l) {
         start[l + 1] = start[l] + sizes[l];
-        h->h_list_off[l + 1] = h->h_list_off[l] + (sizes[l] + 31) / 32 * 32;
+        // Lists start on 128-row boundaries: a 128-row tensor-core tile (and
+        // four 32-row scan tiles) never straddles two lists.
+        h->h_list_off[l + 1] = h->h_list_off[l] + (sizes[l] + hy::BATCH_ROW_ALIGN - 1) / hy::BATCH_ROW_ALIGN *
+                                                      hy::BATCH_ROW_ALIGN;
     }
     h->arena_rows = (size_t)h->h_list_off[nlist];
-    const size_t rows_alloc = std::max<size_t>(h->arena_rows, 32);
+    const size_t rows_alloc = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
+    h->abf_valid = false;
     HY_RET(h->codes.ensure(rows_alloc * h->L.row_pitch * sizeof(float)));
     HY_RET(h->ids.ensure(rows_alloc * sizeof(int64_t)));
     HY_RET(h->norms.ensure(rows_alloc * sizeof(float)));
@@ -397,10 +413,14 @@ int ensure_common(hy_index* h) {
     return HY_OK;
 }
 
+int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
+                     bool timed);
+
 // Full device search: coarse quantisation, optional warm-up thresholds, scan,
 // merge, in query chunks.
 int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
                        bool timed) {
+    if (h->form == HY_FORM_BF16 && h->arena_rows > 0) return search_bf16_impl(h, n, dq, k, dD, dI, s, timed);
     const size_t nprobe = std::min(h->nprobe, h->nlist);
     HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search: nprobe must be >= 1");
     HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "search: nlist above 40000 is not supported by the coarse selector");
@@ -437,6 +457,114 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
     return HY_OK;
 }
 
+// The bf16 tensor-core image of the arena, built on first use after add/load.
+int ensure_bf16_image(hy_index* h, cudaStream_t s) {
+    if (h->abf_valid) return HY_OK;
+    const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
+    HY_RET(h->abf.ensure(hy::bf16_image_bytes((int64_t)rows, (int)h->d)));
+    HY_RET(h->xaux.ensure(rows * sizeof(float2)));
+    HY_CUDA(hy::launch_to_bf16_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->abf.p, s));
+    HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->xaux.as<float2>(), s));
+    h->abf_valid = true;
+    return HY_OK;
+}
+
+// Batched bf16 search of n device queries: coarse quantisation, warm-up
+// thresholds, probe inversion, the persistent tensor-core scan and the exact
+// re-rank, in query chunks sized so the candidate buffers stay within 2 GiB.
+int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
+                     bool timed) {
+    const size_t nprobe = std::min(h->nprobe, h->nlist);
+    HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search: nprobe must be >= 1");
+    HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "search: nlist above 40000 is not supported by the coarse selector");
+    HY_RET(ensure_common(h));
+    HY_RET(ensure_bf16_image(h, s));
+    if (h->nsm == 0) HY_CUDA(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const size_t capq = h->capq;
+    size_t qc = std::min(query_chunk(h->nlist, n), std::max<size_t>(1, (size_t(2) << 30) / (capq * 8)));
+    qc = std::min(qc, n);
+    const size_t nkb = (h->d + 63) / 64;
+    const size_t nlist = h->nlist;
+    HY_RET(h->w_scores.ensure(qc * nlist * sizeof(float)));
+    HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
+    HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
+    HY_RET(h->b_thr.ensure(qc * sizeof(float)));
+    HY_RET(h->b_qb.ensure(qc * nkb * 64 * 2));
+    HY_RET(h->b_qn.ensure(qc * sizeof(float4)));
+    HY_RET(h->b_pcnt.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_pfill.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_poff.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_RET(h->b_pairs.ensure(qc * nprobe * sizeof(int32_t)));
+    HY_RET(h->b_icnt.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_ioff.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_RET(h->b_work.ensure(sizeof(unsigned int)));
+    HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
+    HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
+    HY_RET(h->b_ovf.ensure((n + 1) * sizeof(int32_t)));
+    HY_CUDA(cudaMemsetAsync(h->b_ovf.p, 0, sizeof(int32_t), s));
+    const size_t wl = h->warmup_list ? h->warmup_list : 10;
+    const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
+    HY_CHECK(std::min(wl, nprobe) * wls <= 32768, HY_ERR_ARG, "presearch: warmup_list * warmup_list_size above 32768");
+    hy::BatchWork w;
+    w.pair_cnt = h->b_pcnt.as<int32_t>();
+    w.pair_fill = h->b_pfill.as<int32_t>();
+    w.pair_off = h->b_poff.as<int64_t>();
+    w.pairs = h->b_pairs.as<int32_t>();
+    w.item_cnt = h->b_icnt.as<int32_t>();
+    w.item_off = h->b_ioff.as<int64_t>();
+    w.work = h->b_work.as<unsigned int>();
+    w.cand = h->b_cand.as<uint64_t>();
+    w.cand_cnt = h->b_ccnt.as<int32_t>();
+    for (size_t q0 = 0; q0 < n; q0 += qc) {
+        const size_t m = std::min(qc, n - q0);
+        const float* qq = dq + q0 * h->d;
+        w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then global query ids
+        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[0], s));
+        HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
+                                         h->w_scores.as<float>(), s));
+        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
+                                  nullptr, s));
+        if (h->metric == HY_METRIC_L2) {
+            HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
+                                      qq, (int)m, h->w_probes.as<int64_t>(), (int)nprobe, (int)k, (int)wl, (int)wls, 1,
+                                      h->w_thr.as<uint32_t>(), h->b_thr.as<float>(), h->w_err.as<int>(), s));
+        } else {
+            // Inner products have no warm-up threshold in the reference; the
+            // candidate buffers then hold every probed row.
+            HY_CUDA(hy::launch_fill_f32(h->b_thr.as<float>(), (int64_t)m, INFINITY, s));
+        }
+        HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(), s));
+        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[1], s));
+        HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, (int)nlist,
+                                         h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+        HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
+        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[2], s));
+        hy::BatchedLaunch b;
+        b.abf = h->abf.p;
+        b.list_off = h->list_off.as<int64_t>();
+        b.list_size = h->list_size.as<int32_t>();
+        b.xn = h->norms.as<float>();
+        b.xaux = h->xaux.as<float2>();
+        b.qb = h->b_qb.p;
+        b.qaux = h->b_qn.as<float4>();
+        b.thr = h->b_thr.as<float>();
+        b.nlist = (int)nlist;
+        b.d = (int)h->d;
+        b.rs = (int)h->row_slice;
+        b.capq = (int)capq;
+        b.metric = h->metric;
+        b.nsm = h->nsm;
+        HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[3], s));
+        HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
+                                  h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, (int)q0, (int)capq, (int)k,
+                                  h->metric, dD + q0 * k, dI + q0 * k, s));
+        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[4], s));
+        h->launches += 14;
+    }
+    return HY_OK;
+}
+
 int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t nprobe) {
     HY_CUDA(cudaStreamSynchronize(s));
     int err = 0;
@@ -469,6 +597,40 @@ int reset_counters(hy_index* h, cudaStream_t s) {
     HY_RET(ensure_common(h));
     h->launches = 0;
     HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 2 * sizeof(unsigned long long), s));
+    return HY_OK;
+}
+
+// Queries whose bf16 candidate buffers overflowed are answered again with the
+// plain FP32 scan (the exact fallback) and their rows patched into D / I.
+int bf16_fallback(hy_index* h, const float* q, size_t n, size_t k, float* D, int64_t* I, cudaStream_t s) {
+    int32_t cnt = 0;
+    HY_CUDA(cudaMemcpy(&cnt, h->b_ovf.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    h->stats.rows = 0;
+    if (cnt <= 0) return HY_OK;
+    std::vector<int32_t> qids(cnt);
+    HY_CUDA(cudaMemcpy(qids.data(), h->b_ovf.as<int32_t>() + 1, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    std::vector<float> sub((size_t)cnt * h->d);
+    for (int i = 0; i < cnt; ++i) std::memcpy(&sub[(size_t)i * h->d], q + (size_t)qids[i] * h->d, h->d * sizeof(float));
+    HY_RET(h->w_q.ensure(sub.size() * sizeof(float)));
+    HY_RET(h->w_D.ensure((size_t)cnt * k * sizeof(float)));
+    HY_RET(h->w_I.ensure((size_t)cnt * k * sizeof(int64_t)));
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, sub.data(), sub.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    const int form = h->form;
+    h->form = HY_FORM_PLAIN;
+    const int rc = search_device_impl(h, (size_t)cnt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s,
+                                      false);
+    h->form = form;
+    HY_RET(rc);
+    std::vector<float> d2((size_t)cnt * k);
+    std::vector<int64_t> i2((size_t)cnt * k);
+    HY_CUDA(cudaMemcpyAsync(d2.data(), h->w_D.p, d2.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(i2.data(), h->w_I.p, i2.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < cnt; ++i) {
+        std::memcpy(D + (size_t)qids[i] * k, &d2[(size_t)i * k], k * sizeof(float));
+        std::memcpy(I + (size_t)qids[i] * k, &i2[(size_t)i * k], k * sizeof(int64_t));
+    }
+    h->stats.fallback_queries = (uint64_t)cnt;
     return HY_OK;
 }
 
@@ -610,6 +772,28 @@ int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
     return HY_OK;
 }
 
+int hy_index_set_form(hy_index* h, int form) {
+    HY_CHECK(h, HY_ERR_ARG, "set_form: NULL handle");
+    HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16, HY_ERR_ARG, "set_form: unknown form");
+    HY_CHECK(form != HY_FORM_BF16 || h->d <= 640, HY_ERR_ARG, "set_form: the bf16 form supports d <= 640");
+    h->form = form;
+    return HY_OK;
+}
+
+int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice) {
+    HY_CHECK(h, HY_ERR_ARG, "set_batch_params: NULL handle");
+    if (capq) {
+        HY_CHECK(capq >= 64 && capq <= 32768, HY_ERR_ARG, "set_batch_params: capq must be in [64, 32768]");
+        h->capq = capq;
+    }
+    if (oversample) h->oversample = oversample;
+    if (row_slice) {
+        HY_CHECK(row_slice % hy::BATCH_ROW_ALIGN == 0, HY_ERR_ARG, "set_batch_params: row_slice must be a multiple of 128");
+        h->row_slice = row_slice;
+    }
+    return HY_OK;
+}
+
 int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_list_size) {
     HY_CHECK(h, HY_ERR_ARG, "presearch: NULL handle");
     h->warmup_list = warmup_list;
@@ -647,7 +831,16 @@ int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, i
     HY_RET(search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true));
     HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    return finish_host_call(h, s, true, n, std::min(h->nprobe, h->nlist));
+    HY_RET(finish_host_call(h, s, true, n, std::min(h->nprobe, h->nlist)));
+    h->stats.fallback_queries = 0;
+    if (h->form == HY_FORM_BF16 && h->arena_rows > 0) {
+        const hy_search_stats_t keep = h->stats;
+        HY_RET(bf16_fallback(h, q, n, k, D, I, s));
+        const uint64_t fb = h->stats.fallback_queries;
+        h->stats = keep;
+        h->stats.fallback_queries = fb;
+    }
+    return HY_OK;
 }
 
 int hy_index_search_preassigned(hy_index* h, size_t n, const float* q, size_t k, size_t nprobe, const int64_t* probes,

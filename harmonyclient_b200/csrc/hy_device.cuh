@@ -61,6 +61,11 @@ __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+// Plain arrival (count 1) on a CTA-local mbarrier.
+__device__ inline void mbar_arrive_cta(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // One 1-D bulk copy global -> shared, completing on `bar`.  dst, src 16-byte
 // aligned; bytes a multiple of 16.
 __device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

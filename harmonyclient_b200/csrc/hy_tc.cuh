@@ -1,0 +1,103 @@
+// Blackwell 5th-generation tensor core (tcgen05) helpers, written against the
+// PTX ISA: shared-memory matrix descriptors for the 128-byte-swizzled K-major
+// canonical layout, the kind::f16 instruction descriptor, MMA issue, commit to
+// an mbarrier, TMEM allocation and 32x32b loads.
+//
+// Operand layout used everywhere (both A and B, K-major, bf16):
+//   a "k-block" holds R rows x 64 bf16 (128 bytes per row); rows are grouped
+//   in 8-row atoms of 1024 bytes; inside a row, 16-byte chunk c of the
+//   logical row lives at chunk c ^ (row % 8).  A k-block starts on a 1024-byte
+//   boundary.  The descriptor of a k-block uses SBO = 1024 bytes (distance
+//   between 8-row atoms), LBO = 16 bytes (unused with swizzling), version 1,
+//   layout SWIZZLE_128B; the four K=16 steps inside a k-block advance the
+//   start address by 32 bytes each.
+#pragma once
+#include <cstdint>
+
+#include "hy_device.cuh"
+
+namespace hy {
+namespace tc {
+
+// Byte offset of bf16 element (row, k) inside a k-block (k < 64).
+__host__ __device__ inline uint32_t kblock_offset(uint32_t row, uint32_t k) {
+    const uint32_t chunk = k >> 3;  // 8 bf16 per 16-byte chunk
+    return row * 128u + (((chunk ^ (row & 7u)) & 7u) << 4) + ((k & 7u) << 1);
+}
+
+__device__ inline uint64_t sdesc_sw128(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu);  // start address, 16-byte units
+    d |= static_cast<uint64_t>(1u) << 16;                    // leading byte offset (16 B)
+    d |= static_cast<uint64_t>(1024u >> 4) << 32;            // stride byte offset (1024 B)
+    d |= static_cast<uint64_t>(1u) << 46;                    // descriptor version (Blackwell)
+    d |= static_cast<uint64_t>(2u) << 61;                    // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor of kind::f16 with bf16 inputs, f32 accumulator,
+// both operands K-major, shape M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+    return (1u << 4)                                   // D format: f32
+           | (1u << 7)                                 // A format: bf16
+           | (1u << 10)                                // B format: bf16
+           | (static_cast<uint32_t>(N >> 3) << 17)     // N / 8
+           | (static_cast<uint32_t>(M >> 4) << 24);    // M / 16
+}
+
+// D[tmem] (+)= A * B^T, issued by one thread.
+__device__ inline void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+// Arrive once on `bar` when every MMA this thread issued so far completes.
+__device__ inline void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ inline void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Whole warp: allocate `ncols` TMEM columns (power of two >= 32); the base
+// address is written to *dst (shared memory).
+__device__ inline void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ inline void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// Whole warp: 32 consecutive f32 columns of this thread's TMEM lane.  The
+// warp may only address the 32-lane quadrant (warp_id % 4); `taddr` carries
+// the lane in bits 16..31 and the column in bits 0..15.
+__device__ inline void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+}  // namespace tc
+}  // namespace hy

@@ -119,6 +119,15 @@ class Index:
         the reference's MPI modes have no meaning on one GPU."""
         check(self._L.hy_index_presearch(self._h, int(warmUpSearchList), int(warmUpSearchListSize)))
 
+    def set_form(self, form):
+        """'plain' (exact FP32 scan) or 'bf16' (batched tensor-core scan with
+        exact FP32 re-rank)."""
+        f = {"plain": _lib.HY_FORM_PLAIN, "bf16": _lib.HY_FORM_BF16}.get(form, form)
+        check(self._L.hy_index_set_form(self._h, int(f)))
+
+    def set_batch_params(self, capq=0, oversample=0, row_slice=0):
+        check(self._L.hy_index_set_batch_params(self._h, int(capq), int(oversample), int(row_slice)))
+
     def search(self, queries, k):
         q = _f32(queries, self.d)
         n = q.shape[0]

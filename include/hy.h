@@ -50,7 +50,8 @@ enum { HY_METRIC_IP = 0, HY_METRIC_L2 = 1 };
 
 /* Scan forms selectable with hy_index_set_form. */
 enum {
-    HY_FORM_PLAIN = 0 /* exact FP32 query-major scan with dim-block pruning */
+    HY_FORM_PLAIN = 0, /* exact FP32 query-major scan with dim-block pruning */
+    HY_FORM_BF16 = 1   /* batched list-major bf16 tensor-core scan + exact FP32 re-rank */
 };
 
 /* Largest k the scan kernels keep per query. The reference's distributed
@@ -85,6 +86,7 @@ typedef struct {
     double scan_ms;           /* device time of the list scan */
     double merge_ms;          /* device time of the top-k merge */
     uint64_t launches;        /* kernels this library launched for the call */
+    uint64_t fallback_queries; /* bf16 form: queries answered again by the plain scan */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -119,6 +121,19 @@ HY_API int hy_index_add(hy_index* h, size_t n, const float* x);
 HY_API int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream);
 
 HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
+
+/* Scan form (no counterpart in the reference, whose only scan is the exact
+ * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16.  The bf16 form batches queries
+ * per list on the tensor cores and re-ranks candidates with exact FP32
+ * distances; on integer-valued data below 256 its results equal the plain
+ * form's.  Queries whose candidates overflow are answered by the plain form
+ * (host-pointer search only). */
+HY_API int hy_index_set_form(hy_index* h, int form);
+
+/* bf16 form parameters (0 keeps the current value): candidate slots per
+ * query (default 8192), re-rank oversampling factor (default 4) and rows per
+ * work item (default 2048, multiple of 128). */
+HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice);
 
 /* Warm-up threshold parameters.  Mirrors Index::preSearch's warmUpSearchList /
  * warmUpSearchListSize (src/Index.h:90, src/Index.cpp:45-55): when
@@ -168,6 +183,12 @@ HY_API int hy_index_load(hy_index* h, const char* path);
 /* Reads the header and list table of a .index file without a GPU. */
 HY_API int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metric, int* opt_level,
                            size_t* nonempty_lists, size_t* ntotal);
+
+/* Diagnostic with no counterpart in the reference: multiplies one 128 x 128
+ * bf16 tile pair on the tensor cores exactly as the batched scan does
+ * (D = A * B^T, A and B row-major 128 x 128 float32 rounded to bf16, D
+ * float32).  Returns HY_OK or an error status. */
+HY_API int hy_selftest_tcgen05(const float* A, const float* B, float* D);
 
 #ifdef __cplusplus
 }
