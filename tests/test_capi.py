@@ -59,3 +59,10 @@ def test_file_inspect_rejects_truncated(tmp_path):
     assert e.value.code == _lib.HY_ERR_IO
     with pytest.raises(HyError):
         file_inspect(tmp_path / "missing.index")
+
+
+def test_cpp_facade_compiles(tmp_path):
+    """include/harmony/Index.h compiles as C++17 and links against libhy.so."""
+    from tests.cpp_facade import build
+    exe = build(tmp_path)
+    assert os.path.exists(exe)
