@@ -78,6 +78,26 @@ __global__ void row_aux_kernel(ArenaLayout L, const float* __restrict__ codes, i
     if (lane == 0) aux[r] = make_float2(sqrtf(nn), sqrtf(ee));
 }
 
+// Per 128-row tile: the largest |x~| and |x - x~| of its rows (the batched
+// kernel's per-tile relaxation of the error bound).
+__global__ void tile_aux_kernel(const float2* __restrict__ row_aux, int64_t tiles, float2* __restrict__ out) {
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= tiles) return;
+    float a = 0.0f, e = 0.0f;
+    for (int r = lane; r < TM; r += 32) {
+        const float2 v = row_aux[t * TM + r];
+        a = fmaxf(a, v.x);
+        e = fmaxf(e, v.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmaxf(a, __shfl_xor_sync(FULL, a, o));
+        e = fmaxf(e, __shfl_xor_sync(FULL, e, o));
+    }
+    if (lane == 0) out[t] = make_float2(a, e);
+}
+
 // Queries: bf16 rows padded to nkb*64, and per query {|q|^2 (sequential f32,
 // the exact arithmetic's value), |q|, |q~|, |q - q~|}.
 __global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, int nkb,
@@ -210,7 +230,7 @@ struct BatchedParams {
     const int32_t* pairs;           // query ids grouped by list
     const int32_t* pair_cnt;        // [nlist]
     const float* xn;                // [arena rows] squared norms (f32)
-    const float2* xaux;             // [arena rows] {|x~|, |x - x~|}
+    const float2* tile_aux;         // [arena tiles] {max |x~|, max |x - x~|} over the tile's rows
     const __nv_bfloat16* qb;        // [nq][nkb*64]
     const float4* qaux;             // [nq] {|q|^2, |q|, |q~|, |q - q~|}
     const float* thr;               // [nq] distance thresholds (score units)
@@ -222,26 +242,63 @@ struct BatchedParams {
     float cK, cN;                   // error-bound constants (see err_coef)
 };
 
-__global__ void __launch_bounds__(256, 1) batched_scan_kernel(const __grid_constant__ BatchedParams p) {
+// Warp roles of the persistent batched kernel (12 warps).
+constexpr int W_PRODUCER = 0;   // lane 0: bulk copies of list k-blocks
+constexpr int W_MMA = 1;        // lane 0: tcgen05.mma issue; whole warp: TMEM alloc
+constexpr int W_GATHER0 = 2;    // warps 2-3: fetch items, gather their queries
+constexpr int N_GATHER = 2;
+constexpr int W_EPI0 = 4;       // warps 4-11: epilogue (two per TMEM lane quadrant)
+constexpr int N_EPI = 8;
+constexpr int BATCH_THREADS = 32 * (W_EPI0 + N_EPI);
+constexpr int CB = 256;         // per-epilogue-warp candidate staging
+
+// Item metadata of one query slot (two slots: the item being scanned and the
+// next one being gathered).
+struct ItemSlot {
+    int ntiles;  // -1 = no more items
+    int nqv;
+    int nrows;
+    long long row0;
+    int qid[QG];
+    float qn[QG];    // |q|^2
+    float V[QG];     // threshold + bound constant - |q|^2 (score units)
+    float aq[QG];    // bound coefficient of |x~|
+    float bq[QG];    // bound coefficient of |x - x~|
+};
+
+__device__ inline bool wait_or_abort(uint64_t* bar, uint32_t parity, int* err, volatile int* abort) {
+    for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && *abort) return false;
+    }
+    if (err) atomicCAS(err, 0, DEV_ERR_TIMEOUT);
+    *abort = 1;
+    return false;
+}
+
+// Barrier over `nthreads` threads (a multiple of 32) on hardware barrier `id`.
+__device__ inline void named_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __grid_constant__ BatchedParams p) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* sB = base;                                   // nkb x 16 KiB (queries)
-    unsigned char* sA = sB + static_cast<size_t>(p.nkb) * KB_BYTES;  // NS x 16 KiB (list k-blocks)
-    __shared__ uint64_t full[NS], empty[NS], accf[2], acce[2];
+    const int nkb = p.nkb;
+    unsigned char* sB = base;                                        // 2 slots x nkb x 16 KiB (queries)
+    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * KB_BYTES;  // NS x 16 KiB (list k-blocks)
+    ItemSlot* slot = reinterpret_cast<ItemSlot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2]
+    float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][64] per-tile test bounds
+    int* s_cq = reinterpret_cast<int*>(sR + N_EPI * 64);             // [N_EPI][CB]
+    uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
+
+    __shared__ uint64_t full[NS], empty[NS], accf[2], acce[2], sfull[2], sfree[2];
     __shared__ uint32_t tbase;
-    __shared__ float s_qn[QG], s_thr[QG], s_aq[QG], s_bq[QG];
-    __shared__ int s_qid[QG];
-    constexpr int CB = 256;  // per-epilogue-warp candidate staging
-    __shared__ int s_cq[4][CB];
-    __shared__ uint64_t s_ck[4][CB];
-    // Two item descriptors: the one being processed and the next one, which
-    // warp 2 fetches and decodes meanwhile.
-    __shared__ int s_il[2], s_iqg[2], s_inqv[2], s_inrows[2];
-    __shared__ long long s_irow0[2];
     __shared__ int s_abort;
+    __shared__ long long s_g[2];
+    __shared__ int s_wcount[N_EPI];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nkb = p.nkb;
     const bool l2 = p.metric == 1;
     volatile int* vabort = &s_abort;
 
@@ -252,30 +309,39 @@ __global__ void __launch_bounds__(256, 1) batched_scan_kernel(const __grid_const
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(&accf[i], 1);
-            mbar_init(&acce[i], 4);
+            mbar_init(&acce[i], N_EPI);
+            mbar_init(&sfull[i], 32 * N_GATHER);
+            mbar_init(&sfree[i], 1 + N_EPI);  // MMA commit + every epilogue warp
         }
         s_abort = 0;
         fence_mbar_init();
     }
-    if (warp == 1) tc::tmem_alloc(&tbase, TMEM_COLS);
+    if (warp == W_MMA) tc::tmem_alloc(&tbase, TMEM_COLS);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tbase;
-    const uint32_t idesc = tc::idesc_bf16_f32(TM, QG);
-
-    uint32_t load_it = 0;  // producer: k-block loads issued
-    uint32_t mma_it = 0;   // MMA issuer: k-blocks consumed
-    uint32_t tile_it = 0;  // tiles accumulated (MMA issuer and epilogue count alike)
     const int64_t total_items = p.item_off[p.nlist];
 
-    // Take the next work item from the queue and decode it into slot `slot`
-    // (list = the last l with item_off[l] <= g; lists without items are
-    // skipped because their item_off equals the next list's).
-    auto fetch = [&](int slot) {
-        const long long g = atomicAdd(p.work, 1u);
-        int l = -1;
-        if (g < total_items && !*vabort) {
+    if (warp >= W_GATHER0 && warp < W_GATHER0 + N_GATHER) {
+        // ---------------- gather: fetch an item, decode it, stage its queries
+        const int gt = threadIdx.x - 32 * W_GATHER0;  // 0..63
+        for (uint32_t it = 0;; ++it) {
+            const int b = it & 1;
+            if (!wait_or_abort(&sfree[b], ((it >> 1) & 1u) ^ 1u, p.err, vabort)) break;
+            ItemSlot& S = slot[b];
+            // One index per slot: a gather thread may still be reading this
+            // item's index while thread 0 already fetches the next one.
+            if (gt == 0) s_g[b] = atomicAdd(p.work, 1u);
+            named_sync(1, 32 * N_GATHER);
+            const long long g = s_g[b];
+            if (g >= total_items || *vabort) {
+                if (gt == 0) S.ntiles = -1;
+                mbar_arrive_cta(&sfull[b]);
+                break;
+            }
+            // list = last l with item_off[l] <= g (lists without items share
+            // the next list's offset and are skipped).
             int lo = 0, hi = p.nlist - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -284,75 +350,65 @@ __global__ void __launch_bounds__(256, 1) batched_scan_kernel(const __grid_const
                 else
                     hi = mid - 1;
             }
-            l = lo;
+            const int l = lo;
             const int w = static_cast<int>(g - p.item_off[l]);
             const int sz = p.list_size[l];
             const int nrs = (sz + p.rs - 1) / p.rs;
             const int qg = w / nrs, rsl = w % nrs;
-            s_iqg[slot] = qg;
-            s_inqv[slot] = min(QG, p.pair_cnt[l] - qg * QG);
-            s_irow0[slot] = p.list_off[l] + static_cast<long long>(rsl) * p.rs;
-            s_inrows[slot] = min(p.rs, sz - rsl * p.rs);
-        }
-        s_il[slot] = l;
-    };
-    if (threadIdx.x == 64) fetch(0);
-    __syncthreads();
-
-    for (int it = 0;; ++it) {
-        const int cur = it & 1;
-        const int l = s_il[cur];
-        if (l < 0) break;
-        const int qg = s_iqg[cur], nqv = s_inqv[cur];
-        const long long row0 = s_irow0[cur];
-        const int nrows = s_inrows[cur];
-        const int ntiles = (nrows + TM - 1) / TM;
-
-        // --- gather the group's queries (bf16, swizzled) as the B operand
-        const int32_t* grp = p.pairs + p.pair_off[l] + static_cast<int64_t>(qg) * QG;
-        for (int i = threadIdx.x; i < QG; i += blockDim.x) {
-            const int qid = i < nqv ? grp[i] : -1;
-            s_qid[i] = qid;
-            if (qid >= 0) {
-                const float4 qa = p.qaux[qid];
-                const ErrCoef ec = err_coef(qa, l2, p.cK, p.cN);
-                s_qn[i] = qa.x;
-                s_aq[i] = ec.aq;
-                s_bq[i] = ec.bq;
-                // A row is a candidate when its bf16 distance minus the error
-                // bound is within the query's threshold.
-                s_thr[i] = p.thr[qid] + ec.cq;
-            } else {
-                s_qn[i] = 0.0f;
-                s_aq[i] = 0.0f;
-                s_bq[i] = 0.0f;
-                s_thr[i] = -INFINITY;
+            const int nqv = min(QG, p.pair_cnt[l] - qg * QG);
+            const int nrows = min(p.rs, sz - rsl * p.rs);
+            const int32_t* grp = p.pairs + p.pair_off[l] + static_cast<int64_t>(qg) * QG;
+            if (gt == 0) {
+                S.nqv = nqv;
+                S.nrows = nrows;
+                S.row0 = p.list_off[l] + static_cast<long long>(rsl) * p.rs;
+                S.ntiles = (nrows + TM - 1) / TM;
             }
-        }
-        for (int e = threadIdx.x; e < QG * nkb * 8; e += blockDim.x) {
-            const int i = e / (nkb * 8), rem = e % (nkb * 8);
-            const int kb = rem >> 3, c = rem & 7;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (i < nqv) {
-                const int qid = grp[i];
-                v = *reinterpret_cast<const uint4*>(p.qb + static_cast<size_t>(qid) * nkb * 64 + kb * 64 + c * 8);
+            for (int i = gt; i < QG; i += 32 * N_GATHER) {
+                const int qid = i < nqv ? grp[i] : -1;
+                S.qid[i] = qid;
+                if (qid >= 0) {
+                    const float4 qa = p.qaux[qid];
+                    const ErrCoef ec = err_coef(qa, l2, p.cK, p.cN);
+                    S.qn[i] = l2 ? qa.x : 0.0f;
+                    S.V[i] = p.thr[qid] + ec.cq - (l2 ? qa.x : 0.0f);
+                    S.aq[i] = ec.aq;
+                    S.bq[i] = ec.bq;
+                } else {
+                    S.qn[i] = 0.0f;
+                    S.V[i] = -INFINITY;
+                    S.aq[i] = 0.0f;
+                    S.bq[i] = 0.0f;
+                }
             }
-            *reinterpret_cast<uint4*>(sB + kb * KB_BYTES + i * 128 + (((c ^ (i & 7)) & 7) << 4)) = v;
+            unsigned char* dst = sB + static_cast<size_t>(b) * nkb * KB_BYTES;
+            for (int e = gt; e < QG * nkb * 8; e += 32 * N_GATHER) {
+                const int i = e / (nkb * 8), rem = e % (nkb * 8);
+                const int kb = rem >> 3, c = rem & 7;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (i < nqv)
+                    v = *reinterpret_cast<const uint4*>(p.qb + static_cast<size_t>(grp[i]) * nkb * 64 + kb * 64 + c * 8);
+                *reinterpret_cast<uint4*>(dst + kb * KB_BYTES + i * 128 + (((c ^ (i & 7)) & 7) << 4)) = v;
+            }
+            fence_proxy_async();  // generic-proxy writes -> tensor-core reads
+            mbar_arrive_cta(&sfull[b]);
         }
-        fence_proxy_async();
-        __syncthreads();
-        if (threadIdx.x == 64) fetch(cur ^ 1);
-
-        if (warp == 0) {
-            // --- producer: k-blocks of the slice's tiles into the stage ring
-            if (lane == 0) {
-                const int64_t tile0 = row0 / TM;
-                for (int t = 0; t < ntiles && !*vabort; ++t) {
+    } else if (warp == W_PRODUCER) {
+        // ---------------- producer: list k-blocks into the stage ring
+        if (lane == 0) {
+            uint32_t load_it = 0;
+            for (uint32_t it = 0;; ++it) {
+                const int b = it & 1;
+                if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+                const int ntiles = slot[b].ntiles;
+                if (ntiles < 0) break;
+                const int64_t tile0 = slot[b].row0 / TM;
+                bool ok = true;
+                for (int t = 0; t < ntiles && ok; ++t) {
                     for (int kb = 0; kb < nkb; ++kb, ++load_it) {
                         const int s = load_it % NS;
-                        const uint32_t round = load_it / NS;
-                        if (!mbar_wait_bounded(&empty[s], (round & 1u) ^ 1u, p.err)) {
-                            s_abort = 1;
+                        if (!wait_or_abort(&empty[s], ((load_it / NS) & 1u) ^ 1u, p.err, vabort)) {
+                            ok = false;
                             break;
                         }
                         mbar_expect_tx(&full[s], KB_BYTES);
@@ -361,111 +417,148 @@ __global__ void __launch_bounds__(256, 1) batched_scan_kernel(const __grid_const
                                  &full[s]);
                     }
                 }
+                if (!ok) break;
             }
-        } else if (warp == 1) {
-            // --- MMA issuer
-            if (lane == 0) {
-                for (int t = 0; t < ntiles && !*vabort; ++t, ++tile_it) {
+        }
+    } else if (warp == W_MMA) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16_f32(TM, QG);
+            uint32_t mma_it = 0, tile_it = 0;
+            bool ok = true;
+            for (uint32_t it = 0; ok; ++it) {
+                const int b = it & 1;
+                if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+                const int ntiles = slot[b].ntiles;
+                if (ntiles < 0) break;
+                tc::fence_after_sync();
+                const uint32_t b0 = smem_u32(sB + static_cast<size_t>(b) * nkb * KB_BYTES);
+                for (int t = 0; t < ntiles && ok; ++t, ++tile_it) {
                     const int buf = tile_it & 1;
-                    const uint32_t round = tile_it >> 1;
-                    if (!mbar_wait_bounded(&acce[buf], (round & 1u) ^ 1u, p.err)) {
-                        s_abort = 1;
+                    if (!wait_or_abort(&acce[buf], ((tile_it >> 1) & 1u) ^ 1u, p.err, vabort)) {
+                        ok = false;
                         break;
                     }
                     tc::fence_after_sync();
                     const uint32_t dcol = tmem + static_cast<uint32_t>(buf * QG);
                     for (int kb = 0; kb < nkb; ++kb, ++mma_it) {
                         const int s = mma_it % NS;
-                        const uint32_t r2 = mma_it / NS;
-                        if (!mbar_wait_bounded(&full[s], r2 & 1u, p.err)) {
-                            s_abort = 1;
+                        if (!wait_or_abort(&full[s], (mma_it / NS) & 1u, p.err, vabort)) {
+                            ok = false;
                             break;
                         }
                         tc::fence_after_sync();
                         const uint32_t a0 = smem_u32(sA + static_cast<size_t>(s) * KB_BYTES);
-                        const uint32_t b0 = smem_u32(sB + kb * KB_BYTES);
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk)
-                            tc::mma_bf16(dcol, tc::sdesc_sw128(a0 + kk * 32), tc::sdesc_sw128(b0 + kk * 32), idesc,
+                            tc::mma_bf16(dcol, tc::sdesc_sw128(a0 + kk * 32),
+                                         tc::sdesc_sw128(b0 + kb * KB_BYTES + kk * 32), idesc,
                                          (kb | kk) != 0 ? 1u : 0u);
                         tc::mma_commit(&empty[s]);
                     }
-                    tc::mma_commit(&accf[buf]);
+                    if (ok) tc::mma_commit(&accf[buf]);
                 }
+                if (ok) tc::mma_commit(&sfree[b]);  // the slot's queries are no longer read
             }
-        } else if (warp >= 4) {
-            // --- epilogue: thread = row of the tile, 32 queries per TMEM load.
-            // Candidates are staged per warp in shared memory (ballot, no
-            // atomics) and flushed with one independent atomic per lane.
-            const int quad = warp & 3;
-            int* wq = s_cq[quad];
-            uint64_t* wk = s_ck[quad];
-            int wcount = 0;
-            auto flush = [&]() {
+        }
+    } else if (warp >= W_EPI0) {
+        // ---------------- epilogue: thread = row of the tile; each warp of a
+        // TMEM lane quadrant handles half of the 128 query columns.
+        const int e = warp - W_EPI0;       // 0..7
+        const int quad = warp & 3;         // TMEM lanes [32*quad, 32*quad+32)
+        const int half = e >> 2;           // columns [64*half, 64*half+64)
+        int* wq = s_cq + e * CB;
+        uint64_t* wk = s_ck + e * CB;
+        int* wcount = &s_wcount[e];
+        if (lane == 0) *wcount = 0;
+        __syncwarp();
+        auto flush = [&]() {
+            __syncwarp();
+            const int n = min(*reinterpret_cast<volatile int*>(wcount), CB);
+            for (int i = lane; i < n; i += 32) {
+                const int qid = wq[i];
+                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
+                if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = wk[i];
+            }
+            __syncwarp();
+            if (lane == 0) *wcount = 0;
+            __syncwarp();
+        };
+        const float cf = l2 ? -2.0f : -1.0f;
+        uint32_t tile_it = 0;
+        for (uint32_t it = 0;; ++it) {
+            const int b = it & 1;
+            if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+            const ItemSlot& S = slot[b];
+            const int ntiles = S.ntiles;
+            if (ntiles < 0) break;
+            const int nqv = S.nqv, nrows = S.nrows;
+            const long long row0 = S.row0;
+            bool ok = true;
+            float* R = sR + e * 64;  // this warp's 64 columns
+            for (int t = 0; t < ntiles; ++t, ++tile_it) {
+                const int buf = tile_it & 1;
+                // Per-tile test bound of this warp's queries:
+                // V + max|x~| aq + max|x - x~| bq over the tile's rows.
+                const float2 ta = p.tile_aux[row0 / TM + t];
                 __syncwarp();
-                for (int i = lane; i < wcount; i += 32) {
-                    const int qid = wq[i];
-                    const int pos = atomicAdd(&p.cand_cnt[qid], 1);
-                    if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = wk[i];
+                for (int cc = lane; cc < 64; cc += 32) {
+                    const int q = half * 64 + cc;
+                    R[cc] = S.V[q] + fmaf(ta.x, S.aq[q], ta.y * S.bq[q]);
                 }
                 __syncwarp();
-                wcount = 0;
-            };
-            for (int t = 0; t < ntiles && !*vabort; ++t, ++tile_it) {
-                const int buf = tile_it & 1;
-                const uint32_t round = tile_it >> 1;
-                if (!mbar_wait_bounded(&accf[buf], round & 1u, p.err)) {
-                    s_abort = 1;
+                if (!wait_or_abort(&accf[buf], (tile_it >> 1) & 1u, p.err, vabort)) {
+                    ok = false;
                     break;
                 }
                 tc::fence_after_sync();
-                const int rs_row = t * TM + quad * 32 + lane;  // row within the slice
+                const int rs_row = t * TM + quad * 32 + lane;
                 const bool rvalid = rs_row < nrows;
-                const int64_t arow = row0 + rs_row;
-                float xnv = 0.0f, xnn = 0.0f, xe = 0.0f;
-                if (rvalid) {
-                    xnv = p.xn[arow];
-                    const float2 xa = p.xaux[arow];
-                    xnn = xa.x;
-                    xe = xa.y;
-                }
-                const float cx = err_row_const(xnv, l2, p.cN);
-                for (int c = 0; c < QG / 32; ++c) {
+                const long long arow = row0 + rs_row;
+                float xnv = 0.0f;
+                if (rvalid) xnv = p.xn[arow];
+                // Rows past the slice end compare as NaN: never candidates.
+                const float ax = rvalid ? (l2 ? xnv - err_row_const(xnv, l2, p.cN) : 0.0f) : __int_as_float(0x7fffffff);
+                for (int c = 0; c < 2; ++c) {
+                    const int col0 = half * 64 + c * 32;
                     float v[32];
-                    tc::tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) +
-                                      static_cast<uint32_t>(buf * QG + c * 32),
+                    tc::tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + col0),
                                   v);
-                    if (c * 32 >= nqv) continue;
+                    if (col0 >= nqv) continue;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        const int qi = c * 32 + j;
-                        const float score = l2 ? __fadd_rn(__fadd_rn(xnv, s_qn[qi]), -2.0f * v[j]) : -v[j];
-                        const float bound = fmaf(xnn, s_aq[qi], fmaf(xe, s_bq[qi], cx));
-                        const bool pass = rvalid && qi < nqv && score - bound <= s_thr[qi];
-                        const unsigned m = __ballot_sync(FULL, pass);
-                        if (m) {
-                            if (wcount + 32 > CB) flush();
-                            if (pass) {
-                                const int slot = wcount + __popc(m & ((1u << lane) - 1u));
-                                wq[slot] = s_qid[qi];
-                                wk[slot] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                        // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef)
+                        if (fmaf(cf, v[j], ax) <= R[c * 32 + j]) {
+                            const int q = col0 + j;
+                            const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * v[j]) : -v[j];
+                            const int slotpos = atomicAdd(wcount, 1);
+                            if (slotpos < CB) {
+                                wq[slotpos] = S.qid[q];
+                                wk[slotpos] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                            } else {
+                                // staging full: emit directly
+                                const int qid = S.qid[q];
+                                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
+                                if (pos < p.capq)
+                                    p.cand[static_cast<int64_t>(qid) * p.capq + pos] =
+                                        (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
                             }
-                            wcount += __popc(m);
                         }
                     }
                 }
                 tc::fence_before_sync();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cta(&acce[buf]);
+                if (__any_sync(FULL, *reinterpret_cast<volatile int*>(wcount) > CB - 64)) flush();
             }
-            if (wcount > 0) flush();
+            flush();
+            if (lane == 0) mbar_arrive_cta(&sfree[b]);
+            if (!ok) break;
         }
-        __syncthreads();
-        if (*vabort) break;
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 1) tc::tmem_dealloc(tmem, TMEM_COLS);
+    if (warp == W_MMA) tc::tmem_dealloc(tmem, TMEM_COLS);
 }
 
 // ---------------------------------------------------------------------------
@@ -603,8 +696,11 @@ cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4*
     return cudaGetLastError();
 }
 
-cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, cudaStream_t s) {
+cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, float2* tile_aux,
+                           cudaStream_t s) {
     row_aux_kernel<<<grid_for(rows * 32, 256), 256, 0, s>>>(L, codes, rows, aux);
+    const int64_t tiles = rows / TM;
+    tile_aux_kernel<<<grid_for(tiles * 32, 256), 256, 0, s>>>(aux, tiles, tile_aux);
     return cudaGetLastError();
 }
 
@@ -632,7 +728,7 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.pairs = w.pairs;
     p.pair_cnt = w.pair_cnt;
     p.xn = b.xn;
-    p.xaux = b.xaux;
+    p.tile_aux = b.tile_aux;
     p.qb = static_cast<const __nv_bfloat16*>(b.qb);
     p.qaux = b.qaux;
     p.thr = b.thr;
@@ -646,14 +742,15 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.capq = b.capq;
     p.metric = b.metric;
     err_consts(b.d, &p.cK, &p.cN);
-    const size_t smem = 1024 + static_cast<size_t>(p.nkb) * KB_BYTES + static_cast<size_t>(NS) * KB_BYTES;
+    const size_t smem = 1024 + 2 * static_cast<size_t>(p.nkb) * KB_BYTES + static_cast<size_t>(NS) * KB_BYTES +
+                        2 * sizeof(ItemSlot) + N_EPI * 64 * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t));
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(batched_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem))) != cudaSuccess)
         return e;
-    batched_scan_kernel<<<b.nsm, 256, smem, s>>>(p);
+    batched_scan_kernel<<<b.nsm, BATCH_THREADS, smem, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -19,8 +19,10 @@ inline size_t bf16_image_bytes(int64_t rows, int d) {
 
 cudaError_t launch_to_bf16_arena(const ArenaLayout& L, const float* codes, int64_t rows, void* out, cudaStream_t s);
 cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, cudaStream_t s);
-// Per arena row {|x~|, |x - x~|} for the bf16 error bound.
-cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, cudaStream_t s);
+// Per arena row {|x~|, |x - x~|} for the bf16 error bound, and per 128-row
+// tile the maxima of both.
+cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, float2* tile_aux,
+                           cudaStream_t s);
 
 // Work buffers of one batched search.
 struct BatchWork {
@@ -44,7 +46,7 @@ struct BatchedLaunch {
     const int64_t* list_off;
     const int32_t* list_size;
     const float* xn;
-    const float2* xaux;
+    const float2* tile_aux;
     const void* qb;
     const float4* qaux;
     const float* thr;

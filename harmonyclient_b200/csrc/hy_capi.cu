@@ -144,6 +144,7 @@ struct hy_index {
     int nsm = 0;
     DevBuf abf;               // bf16 tensor-core image of the arena
     DevBuf xaux;              // per arena row {|x~|, |x - x~|}
+    DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf;
 };
@@ -463,8 +464,10 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
     const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
     HY_RET(h->abf.ensure(hy::bf16_image_bytes((int64_t)rows, (int)h->d)));
     HY_RET(h->xaux.ensure(rows * sizeof(float2)));
+    HY_RET(h->taux.ensure(rows / hy::BATCH_ROW_ALIGN * sizeof(float2)));
     HY_CUDA(hy::launch_to_bf16_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->abf.p, s));
-    HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->xaux.as<float2>(), s));
+    HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->xaux.as<float2>(), h->taux.as<float2>(),
+                               s));
     h->abf_valid = true;
     return HY_OK;
 }
@@ -544,7 +547,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         b.list_off = h->list_off.as<int64_t>();
         b.list_size = h->list_size.as<int32_t>();
         b.xn = h->norms.as<float>();
-        b.xaux = h->xaux.as<float2>();
+        b.tile_aux = h->taux.as<float2>();
         b.qb = h->b_qb.p;
         b.qaux = h->b_qn.as<float4>();
         b.thr = h->b_thr.as<float>();
@@ -775,7 +778,7 @@ int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
 int hy_index_set_form(hy_index* h, int form) {
     HY_CHECK(h, HY_ERR_ARG, "set_form: NULL handle");
     HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16, HY_ERR_ARG, "set_form: unknown form");
-    HY_CHECK(form != HY_FORM_BF16 || h->d <= 640, HY_ERR_ARG, "set_form: the bf16 form supports d <= 640");
+    HY_CHECK(form != HY_FORM_BF16 || h->d <= 192, HY_ERR_ARG, "set_form: the bf16 form supports d <= 192");
     h->form = form;
     return HY_OK;
 }

@@ -123,7 +123,7 @@ HY_API int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* str
 HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
 
 /* Scan form (no counterpart in the reference, whose only scan is the exact
- * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16.  The bf16 form batches queries
+ * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16 (d <= 192).  The bf16 form batches queries
  * per list on the tensor cores and re-ranks candidates with exact FP32
  * distances; on integer-valued data below 256 its results equal the plain
  * form's.  Queries whose candidates overflow are answered by the plain form
