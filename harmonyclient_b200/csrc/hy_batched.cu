@@ -24,6 +24,7 @@
 #include <cuda_bf16.h>
 
 #include <cfloat>
+#include <cstddef>
 
 #include "hy_batched.cuh"
 #include "hy_common.cuh"
@@ -166,10 +167,14 @@ __device__ inline float err_row_const(float xn, bool l2, float cN) { return l2 ?
 
 // ---------------------------------------------------------------------------
 // Inverting the probe lists.
-__global__ void probe_hist_kernel(const int64_t* __restrict__ probes, int64_t n, int32_t* __restrict__ cnt) {
+// Only probe columns [j0, j1) of each query take part (probe rank ranges).
+__global__ void probe_hist_kernel(const int64_t* __restrict__ probes, int nq, int nprobe, int j0, int j1,
+                                  int32_t* __restrict__ cnt) {
+    const int w = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * w;
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t l = probes[i];
+        const int64_t l = probes[(i / w) * nprobe + j0 + i % w];
         if (l >= 0) atomicAdd(&cnt[l], 1);
     }
 }
@@ -198,16 +203,17 @@ __global__ void __launch_bounds__(1024) scan_kernel(const int32_t* __restrict__ 
     if (t == blockDim.x - 1) out[n] = part[t];
 }
 
-__global__ void probe_fill_kernel(const int64_t* __restrict__ probes, int nq, int nprobe,
+__global__ void probe_fill_kernel(const int64_t* __restrict__ probes, int nq, int nprobe, int j0, int j1,
                                   const int64_t* __restrict__ off, int32_t* __restrict__ fill,
                                   int32_t* __restrict__ pairs) {
-    const int64_t n = static_cast<int64_t>(nq) * nprobe;
+    const int w = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * w;
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t l = probes[i];
+        const int64_t l = probes[(i / w) * nprobe + j0 + i % w];
         if (l < 0) continue;
         const int pos = atomicAdd(&fill[l], 1);
-        pairs[off[l] + pos] = static_cast<int32_t>(i / nprobe);
+        pairs[off[l] + pos] = static_cast<int32_t>(i / w);
     }
 }
 
@@ -220,12 +226,29 @@ __global__ void item_count_kernel(const int32_t* __restrict__ cnt, const int32_t
     items[l] = (c > 0 && s > 0) ? ((c + QG - 1) / QG) * ((s + rs - 1) / rs) : 0;
 }
 
+// Item descriptors {list, query group, row slice} for the first `cap` items,
+// so the batched kernel decodes an item with one load (one warp per list).
+__global__ void item_fill_kernel(const int64_t* __restrict__ item_off, const int32_t* __restrict__ list_size,
+                                 int nlist, int rs, int64_t cap, int4* __restrict__ items) {
+    const int lane = threadIdx.x & 31;
+    const int64_t l = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (l >= nlist) return;
+    const int64_t a = item_off[l], b = item_off[l + 1];
+    const int nrs = (list_size[l] + rs - 1) / rs;
+    for (int64_t g = a + lane; g < b && g < cap; g += 32) {
+        const int w = static_cast<int>(g - a);
+        items[g] = make_int4(static_cast<int>(l), w / max(nrs, 1), w % max(nrs, 1), 0);
+    }
+}
+
 // ---------------------------------------------------------------------------
 struct BatchedParams {
     const unsigned char* abf;       // bf16 arena image
     const int64_t* list_off;        // [nlist+1]
     const int32_t* list_size;       // [nlist]
     const int64_t* item_off;        // [nlist+1]
+    const int4* items;              // [item_cap] {list, group, slice}
+    int64_t item_cap;
     const int64_t* pair_off;        // [nlist+1]
     const int32_t* pairs;           // query ids grouped by list
     const int32_t* pair_cnt;        // [nlist]
@@ -254,11 +277,14 @@ constexpr int CB = 256;         // per-epilogue-warp candidate staging
 
 // Item metadata of one query slot (two slots: the item being scanned and the
 // next one being gathered).
+constexpr int RS_MAX = 2048;  // largest row slice (rows staged per slot)
 struct ItemSlot {
     int ntiles;  // -1 = no more items
     int nqv;
     int nrows;
     long long row0;
+    alignas(16) float xn[RS_MAX];  // |x|^2 of the slice's rows (cp.async target: 16-byte aligned)
+    float2 taux[RS_MAX / TM];    // per tile {max |x~|, max |x - x~|}
     int qid[QG];
     float qn[QG];    // |q|^2
     float V[QG];     // threshold + bound constant - |q|^2 (score units)
@@ -287,7 +313,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     const int nkb = p.nkb;
     unsigned char* sB = base;                                        // 2 slots x nkb x 16 KiB (queries)
     unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * KB_BYTES;  // NS x 16 KiB (list k-blocks)
-    ItemSlot* slot = reinterpret_cast<ItemSlot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2]
+    ItemSlot* slot = reinterpret_cast<ItemSlot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2], 1024-aligned
+    static_assert(offsetof(ItemSlot, xn) % 16 == 0 && sizeof(ItemSlot) % 16 == 0, "ItemSlot alignment");
     float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][64] per-tile test bounds
     int* s_cq = reinterpret_cast<int*>(sR + N_EPI * 64);             // [N_EPI][CB]
     uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
@@ -340,30 +367,45 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 mbar_arrive_cta(&sfull[b]);
                 break;
             }
-            // list = last l with item_off[l] <= g (lists without items share
-            // the next list's offset and are skipped).
-            int lo = 0, hi = p.nlist - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (p.item_off[mid] <= g)
-                    lo = mid;
-                else
-                    hi = mid - 1;
+            int l, qg, rsl;
+            if (g < p.item_cap) {
+                const int4 d = p.items[g];
+                l = d.x;
+                qg = d.y;
+                rsl = d.z;
+            } else {
+                // list = last l with item_off[l] <= g (lists without items
+                // share the next list's offset and are skipped).
+                int lo = 0, hi = p.nlist - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (p.item_off[mid] <= g)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                l = lo;
+                const int w = static_cast<int>(g - p.item_off[l]);
+                const int nrs = (p.list_size[l] + p.rs - 1) / p.rs;
+                qg = w / nrs;
+                rsl = w % nrs;
             }
-            const int l = lo;
-            const int w = static_cast<int>(g - p.item_off[l]);
             const int sz = p.list_size[l];
-            const int nrs = (sz + p.rs - 1) / p.rs;
-            const int qg = w / nrs, rsl = w % nrs;
             const int nqv = min(QG, p.pair_cnt[l] - qg * QG);
             const int nrows = min(p.rs, sz - rsl * p.rs);
             const int32_t* grp = p.pairs + p.pair_off[l] + static_cast<int64_t>(qg) * QG;
+            const long long row0 = p.list_off[l] + static_cast<long long>(rsl) * p.rs;
             if (gt == 0) {
                 S.nqv = nqv;
                 S.nrows = nrows;
-                S.row0 = p.list_off[l] + static_cast<long long>(rsl) * p.rs;
+                S.row0 = row0;
                 S.ntiles = (nrows + TM - 1) / TM;
             }
+            // Row norms and tile bounds of the slice: asynchronous 16-byte
+            // copies (the arena is padded to whole tiles, so the rounded-up
+            // ranges stay inside it).
+            for (int c = gt; c < (nrows + 3) / 4; c += 32 * N_GATHER) cp_async16(&S.xn[4 * c], p.xn + row0 + 4 * c);
+            for (int c = gt; c < (nrows + TM - 1) / TM; c += 32 * N_GATHER) S.taux[c] = p.tile_aux[row0 / TM + c];
             for (int i = gt; i < QG; i += 32 * N_GATHER) {
                 const int qid = i < nqv ? grp[i] : -1;
                 S.qid[i] = qid;
@@ -381,15 +423,25 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     S.bq[i] = 0.0f;
                 }
             }
+            // The group's bf16 queries into the swizzled B operand: every
+            // 16-byte chunk is its own asynchronous copy, all in flight at
+            // once; empty query slots are zero-filled.
             unsigned char* dst = sB + static_cast<size_t>(b) * nkb * KB_BYTES;
-            for (int e = gt; e < QG * nkb * 8; e += 32 * N_GATHER) {
-                const int i = e / (nkb * 8), rem = e % (nkb * 8);
-                const int kb = rem >> 3, c = rem & 7;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (i < nqv)
-                    v = *reinterpret_cast<const uint4*>(p.qb + static_cast<size_t>(grp[i]) * nkb * 64 + kb * 64 + c * 8);
-                *reinterpret_cast<uint4*>(dst + kb * KB_BYTES + i * 128 + (((c ^ (i & 7)) & 7) << 4)) = v;
+            for (int i = gt; i < QG; i += 32 * N_GATHER) {
+                if (i < nqv) {
+                    const __nv_bfloat16* src = p.qb + static_cast<size_t>(grp[i]) * nkb * 64;
+                    for (int kb = 0; kb < nkb; ++kb)
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            cp_async16(dst + kb * KB_BYTES + i * 128 + (((c ^ (i & 7)) & 7) << 4), src + kb * 64 + c * 8);
+                } else {
+                    for (int kb = 0; kb < nkb; ++kb)
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            *reinterpret_cast<uint4*>(dst + kb * KB_BYTES + i * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
+                }
             }
+            cp_async_wait_all();
             fence_proxy_async();  // generic-proxy writes -> tensor-core reads
             mbar_arrive_cta(&sfull[b]);
         }
@@ -500,7 +552,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const int buf = tile_it & 1;
                 // Per-tile test bound of this warp's queries:
                 // V + max|x~| aq + max|x - x~| bq over the tile's rows.
-                const float2 ta = p.tile_aux[row0 / TM + t];
+                const float2 ta = S.taux[t];
                 __syncwarp();
                 for (int cc = lane; cc < 64; cc += 32) {
                     const int q = half * 64 + cc;
@@ -515,33 +567,50 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const int rs_row = t * TM + quad * 32 + lane;
                 const bool rvalid = rs_row < nrows;
                 const long long arow = row0 + rs_row;
-                float xnv = 0.0f;
-                if (rvalid) xnv = p.xn[arow];
+                const float xnv = rvalid ? S.xn[rs_row] : 0.0f;
                 // Rows past the slice end compare as NaN: never candidates.
                 const float ax = rvalid ? (l2 ? xnv - err_row_const(xnv, l2, p.cN) : 0.0f) : __int_as_float(0x7fffffff);
+                // This warp's 64 columns in one TMEM load.
+                uint32_t u[64];
+                tc::tmem_ld64(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * 64), u);
+#pragma unroll
                 for (int c = 0; c < 2; ++c) {
                     const int col0 = half * 64 + c * 32;
-                    float v[32];
-                    tc::tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + col0),
-                                  v);
                     if (col0 >= nqv) continue;
+                    // The chunk's 32 test bounds, in registers (no memory
+                    // access inside the test loop).
+                    float r[32];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef)
-                        if (fmaf(cf, v[j], ax) <= R[c * 32 + j]) {
-                            const int q = col0 + j;
-                            const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * v[j]) : -v[j];
-                            const int slotpos = atomicAdd(wcount, 1);
-                            if (slotpos < CB) {
-                                wq[slotpos] = S.qid[q];
-                                wk[slotpos] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
-                            } else {
-                                // staging full: emit directly
-                                const int qid = S.qid[q];
-                                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
-                                if (pos < p.capq)
-                                    p.cand[static_cast<int64_t>(qid) * p.capq + pos] =
-                                        (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                    for (int j = 0; j < 32; j += 4) {
+                        const float4 t4 = *reinterpret_cast<const float4*>(R + c * 32 + j);
+                        r[j] = t4.x;
+                        r[j + 1] = t4.y;
+                        r[j + 2] = t4.z;
+                        r[j + 3] = t4.w;
+                    }
+                    // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef)
+                    uint32_t mask = 0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        mask |= (fmaf(cf, __uint_as_float(u[c * 32 + j]), ax) <= r[j]) ? (1u << j) : 0u;
+                    if (mask) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            if (mask & (1u << j)) {
+                                const int q = col0 + j;
+                                const float ip = __uint_as_float(u[c * 32 + j]);
+                                const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
+                                const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                                const int slotpos = atomicAdd(wcount, 1);
+                                if (slotpos < CB) {
+                                    wq[slotpos] = S.qid[q];
+                                    wk[slotpos] = key;
+                                } else {
+                                    // staging full: emit directly
+                                    const int qid = S.qid[q];
+                                    const int pos = atomicAdd(&p.cand_cnt[qid], 1);
+                                    if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = key;
+                                }
                             }
                         }
                     }
@@ -559,6 +628,36 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     tc::fence_before_sync();
     __syncthreads();
     if (warp == W_MMA) tc::tmem_dealloc(tmem, TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// Threshold tightening between the two batched passes: each candidate's exact
+// distance is at most s + e, so the k-th smallest s + e over a query's
+// candidates bounds its final k-th distance from above; thr := min(thr, that).
+__global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ xn, const float2* __restrict__ xaux,
+                                                      const float4* __restrict__ qaux, BatchWork w, int capq, int k,
+                                                      int metric, float cK, float cN, float* __restrict__ thr) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    uint32_t* hi = reinterpret_cast<uint32_t*>(sm);  // [capq]
+    __shared__ int hist[256];
+    __shared__ uint32_t sh[2];
+    const bool l2 = metric == 1;
+    const int qi = blockIdx.x;
+    const int n = min(w.cand_cnt[qi], capq);
+    if (n < k) return;
+    const uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint64_t key = cq[i];
+        const int64_t row = static_cast<int64_t>(key & 0xffffffffu);
+        const float2 xa = xaux[row];
+        const float e = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+        hi[i] = f2o(o2f(static_cast<uint32_t>(key >> 32)) + e);
+    }
+    __syncthreads();
+    int need;
+    const float U = o2f(cta_radix_select(hi, n, k, &need, hist, sh));
+    if (threadIdx.x == 0 && U < thr[qi]) thr[qi] = U;
 }
 
 // ---------------------------------------------------------------------------
@@ -685,6 +784,18 @@ static void err_consts(int d, float* cK, float* cN) {
     *cN = static_cast<float>((3.0 * d + 16) * u * inflate);
 }
 
+cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
+                           int capq, int k, int metric, int d, float* thr, cudaStream_t s) {
+    const size_t smem = static_cast<size_t>(capq) * 4;
+    cudaError_t e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    float cK, cN;
+    err_consts(d, &cK, &cN);
+    tighten_kernel<<<nq, 256, smem, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s) {
     fill_f32_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n, v);
     return cudaGetLastError();
@@ -704,17 +815,20 @@ cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t row
     return cudaGetLastError();
 }
 
-cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int nlist, const int32_t* list_size,
-                                 int rs, const BatchWork& w, cudaStream_t s) {
-    const int64_t n = static_cast<int64_t>(nq) * nprobe;
+cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
+                                 const int32_t* list_size, int rs, const BatchWork& w, cudaStream_t s) {
+    const int64_t n = static_cast<int64_t>(nq) * (j1 - j0);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.pair_cnt, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.pair_fill, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
-    probe_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, n, w.pair_cnt);
+    probe_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_cnt);
     scan_kernel<<<1, 1024, 0, s>>>(w.pair_cnt, nlist, w.pair_off);
-    probe_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, w.pair_off, w.pair_fill, w.pairs);
+    probe_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_off, w.pair_fill,
+                                                       w.pairs);
     item_count_kernel<<<grid_for(nlist, 256), 256, 0, s>>>(w.pair_cnt, list_size, nlist, rs, w.item_cnt);
     scan_kernel<<<1, 1024, 0, s>>>(w.item_cnt, nlist, w.item_off);
+    item_fill_kernel<<<grid_for(static_cast<int64_t>(nlist) * 32, 256), 256, 0, s>>>(w.item_off, list_size, nlist, rs,
+                                                                                     w.item_cap, w.items);
     return cudaGetLastError();
 }
 
@@ -724,6 +838,8 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.list_off = b.list_off;
     p.list_size = b.list_size;
     p.item_off = w.item_off;
+    p.items = w.items;
+    p.item_cap = w.item_cap;
     p.pair_off = w.pair_off;
     p.pairs = w.pairs;
     p.pair_cnt = w.pair_cnt;

@@ -32,14 +32,21 @@ struct BatchWork {
     int32_t* pairs;      // [nq*nprobe]
     int32_t* item_cnt;   // [nlist]
     int64_t* item_off;   // [nlist+1]
+    int4* items;         // [item_cap] item descriptors
+    int64_t item_cap;
     unsigned int* work;  // [1]
     uint64_t* cand;      // [nq*capq]
     int32_t* cand_cnt;   // [nq]
     int32_t* overflow;   // [1 + nq]: count, then query ids
 };
 
-cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int nlist, const int32_t* list_size,
-                                 int rs, const BatchWork& w, cudaStream_t s);
+// Inverts probe columns [j0, j1) of every query into per-list query groups
+// and builds the work items.
+cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
+                                 const int32_t* list_size, int rs, const BatchWork& w, cudaStream_t s);
+// thr := min(thr, k-th smallest upper bound over each query's candidates).
+cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
+                           int capq, int k, int metric, int d, float* thr, cudaStream_t s);
 
 struct BatchedLaunch {
     const void* abf;

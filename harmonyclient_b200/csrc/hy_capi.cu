@@ -146,7 +146,7 @@ struct hy_index {
     DevBuf xaux;              // per arena row {|x~|, |x - x~|}
     DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
-    DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf;
+    DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
 };
 
 namespace {
@@ -508,7 +508,17 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     const size_t wl = h->warmup_list ? h->warmup_list : 10;
     const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
     HY_CHECK(std::min(wl, nprobe) * wls <= 32768, HY_ERR_ARG, "presearch: warmup_list * warmup_list_size above 32768");
+    // Item descriptors: an upper bound on the item count from host-known
+    // sizes (groups <= pairs/128 + lists, slices per list <= the largest
+    // list's), capped at 4M; items beyond the cap are decoded by search.
+    size_t max_slices = 1;
+    for (size_t l = 0; l < nlist; ++l)
+        max_slices = std::max(max_slices, ((size_t)h->h_list_size[l] + h->row_slice - 1) / h->row_slice);
+    const size_t item_cap = std::min<size_t>((qc * nprobe / 128 + nlist) * max_slices, size_t(4) << 20);
+    HY_RET(h->b_items.ensure(item_cap * sizeof(int4)));
     hy::BatchWork w;
+    w.items = h->b_items.as<int4>();
+    w.item_cap = (int64_t)item_cap;
     w.pair_cnt = h->b_pcnt.as<int32_t>();
     w.pair_fill = h->b_pfill.as<int32_t>();
     w.pair_off = h->b_poff.as<int64_t>();
@@ -538,8 +548,6 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         }
         HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(), s));
         if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[1], s));
-        HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, (int)nlist,
-                                         h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
         HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[2], s));
         hy::BatchedLaunch b;
@@ -557,13 +565,25 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         b.capq = (int)capq;
         b.metric = h->metric;
         b.nsm = h->nsm;
+        // Pass 1: each query's nearest list under the warm-up threshold; the
+        // threshold is then tightened to the k-th smallest candidate upper
+        // bound; pass 2: the remaining probed lists under the tight threshold.
+        HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
+                                         h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        if (nprobe > 1) {
+            HY_CUDA(hy::launch_tighten(h->norms.as<float>(), h->xaux.as<float2>(), h->b_qn.as<float4>(), (int)m, w,
+                                       (int)capq, (int)k, h->metric, (int)h->d, h->b_thr.as<float>(), s));
+            HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
+                                             (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+            HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        }
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[3], s));
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
                                   h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, (int)q0, (int)capq, (int)k,
                                   h->metric, dD + q0 * k, dI + q0 * k, s));
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[4], s));
-        h->launches += 14;
+        h->launches += nprobe > 1 ? 22 : 14;
     }
     return HY_OK;
 }
@@ -791,7 +811,8 @@ int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_
     }
     if (oversample) h->oversample = oversample;
     if (row_slice) {
-        HY_CHECK(row_slice % hy::BATCH_ROW_ALIGN == 0, HY_ERR_ARG, "set_batch_params: row_slice must be a multiple of 128");
+        HY_CHECK(row_slice % hy::BATCH_ROW_ALIGN == 0 && row_slice <= 2048, HY_ERR_ARG,
+                 "set_batch_params: row_slice must be a multiple of 128, at most 2048");
         h->row_slice = row_slice;
     }
     return HY_OK;

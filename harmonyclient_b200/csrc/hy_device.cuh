@@ -61,6 +61,13 @@ __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (L2 only), and the wait for
+// every such copy this thread issued.  Both addresses 16-byte aligned.
+__device__ inline void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Plain arrival (count 1) on a CTA-local mbarrier.
 __device__ inline void mbar_arrive_cta(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
