@@ -35,7 +35,7 @@ namespace {
 
 constexpr int QG = 128;      // queries per group (MMA N)
 constexpr int TM = 128;      // rows per tile (MMA M)
-constexpr int NS = 6;        // A stages (one 16 KiB k-block each)
+constexpr int NS = 4;        // A stages (one 16 KiB k-block each)
 constexpr int KB_BYTES = 16384;
 constexpr int TMEM_COLS = 256;  // two accumulators of QG columns
 
@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][64] per-tile test bounds
     int* s_cq = reinterpret_cast<int*>(sR + N_EPI * 64);             // [N_EPI][CB]
     uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
+    float* s_ip = reinterpret_cast<float*>(s_ck + N_EPI * CB);       // [N_EPI][32 lanes][32] candidate chunks
 
     __shared__ uint64_t full[NS], empty[NS], accf[2], acce[2], sfull[2], sfree[2];
     __shared__ uint32_t tbase;
@@ -594,23 +595,31 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     for (int j = 0; j < 32; ++j)
                         mask |= (fmaf(cf, __uint_as_float(u[c * 32 + j]), ax) <= r[j]) ? (1u << j) : 0u;
                     if (mask) {
+                        // Rare: this lane has candidates in the chunk.  Its 32
+                        // inner products go to a private shared-memory row so
+                        // the set bits can be visited with a compact loop.
+                        float* sip = s_ip + (e * 32 + lane) * 32;
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            if (mask & (1u << j)) {
-                                const int q = col0 + j;
-                                const float ip = __uint_as_float(u[c * 32 + j]);
-                                const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
-                                const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
-                                const int slotpos = atomicAdd(wcount, 1);
-                                if (slotpos < CB) {
-                                    wq[slotpos] = S.qid[q];
-                                    wk[slotpos] = key;
-                                } else {
-                                    // staging full: emit directly
-                                    const int qid = S.qid[q];
-                                    const int pos = atomicAdd(&p.cand_cnt[qid], 1);
-                                    if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = key;
-                                }
+                        for (int j = 0; j < 32; j += 4)
+                            *reinterpret_cast<float4*>(sip + j) =
+                                make_float4(__uint_as_float(u[c * 32 + j]), __uint_as_float(u[c * 32 + j + 1]),
+                                            __uint_as_float(u[c * 32 + j + 2]), __uint_as_float(u[c * 32 + j + 3]));
+                        while (mask) {
+                            const int j = __ffs(mask) - 1;
+                            mask &= mask - 1u;
+                            const int q = col0 + j;
+                            const float ip = sip[j];
+                            const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
+                            const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                            const int slotpos = atomicAdd(wcount, 1);
+                            if (slotpos < CB) {
+                                wq[slotpos] = S.qid[q];
+                                wk[slotpos] = key;
+                            } else {
+                                // staging full: emit directly
+                                const int qid = S.qid[q];
+                                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
+                                if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = key;
                             }
                         }
                     }
@@ -631,33 +640,63 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
 }
 
 // ---------------------------------------------------------------------------
-// Threshold tightening between the two batched passes: each candidate's exact
-// distance is at most s + e, so the k-th smallest s + e over a query's
-// candidates bounds its final k-th distance from above; thr := min(thr, that).
+// Threshold tightening between the two batched passes.  Each candidate's
+// exact distance lies in [s - e, s + e], so U = the k-th smallest s + e over a
+// query's candidates bounds its final k-th distance from above:
+// thr := min(thr, U), and candidates with s - e > U can never enter the top-k
+// and are dropped from the buffer (kept ones are compacted to its front).  A
+// query whose buffer already overflowed is left untouched so the re-rank still
+// reports it.
+constexpr int TIGHTEN_PER_THREAD = 48;  // 256 threads x 48 >= the largest capq (12288)
+
 __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ xn, const float2* __restrict__ xaux,
                                                       const float4* __restrict__ qaux, BatchWork w, int capq, int k,
                                                       int metric, float cK, float cN, float* __restrict__ thr) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint32_t* hi = reinterpret_cast<uint32_t*>(sm);  // [capq]
+    float* lo = reinterpret_cast<float*>(hi + capq);  // [capq]
     __shared__ int hist[256];
     __shared__ uint32_t sh[2];
+    __shared__ int s_m;
     const bool l2 = metric == 1;
     const int qi = blockIdx.x;
-    const int n = min(w.cand_cnt[qi], capq);
-    if (n < k) return;
-    const uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
+    const int cnt = w.cand_cnt[qi];
+    if (cnt < k || cnt > capq) return;
+    const int n = cnt;
+    uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint64_t key = cq[i];
-        const int64_t row = static_cast<int64_t>(key & 0xffffffffu);
-        const float2 xa = xaux[row];
-        const float e = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
-        hi[i] = f2o(o2f(static_cast<uint32_t>(key >> 32)) + e);
+    // Keys stay in registers (element i = threadIdx.x + 256 t) so the buffer
+    // can be compacted in place after every thread has read it.
+    uint64_t kr[TIGHTEN_PER_THREAD];
+#pragma unroll
+    for (int t = 0; t < TIGHTEN_PER_THREAD; ++t) {
+        const int i = threadIdx.x + 256 * t;
+        kr[t] = 0;
+        if (i < n) {
+            const uint64_t key = cq[i];
+            const int64_t row = static_cast<int64_t>(key & 0xffffffffu);
+            const float2 xa = xaux[row];
+            const float e = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+            const float sc = o2f(static_cast<uint32_t>(key >> 32));
+            kr[t] = key;
+            hi[i] = f2o(sc + e);
+            lo[i] = sc - e;
+        }
     }
+    if (threadIdx.x == 0) s_m = 0;
     __syncthreads();
     int need;
     const float U = o2f(cta_radix_select(hi, n, k, &need, hist, sh));
-    if (threadIdx.x == 0 && U < thr[qi]) thr[qi] = U;
+#pragma unroll
+    for (int t = 0; t < TIGHTEN_PER_THREAD; ++t) {
+        const int i = threadIdx.x + 256 * t;
+        if (i < n && lo[i] <= U) cq[atomicAdd(&s_m, 1)] = kr[t];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        w.cand_cnt[qi] = s_m;
+        if (U < thr[qi]) thr[qi] = U;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -786,7 +825,7 @@ static void err_consts(int d, float* cK, float* cN) {
 
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
                            int capq, int k, int metric, int d, float* thr, cudaStream_t s) {
-    const size_t smem = static_cast<size_t>(capq) * 4;
+    const size_t smem = static_cast<size_t>(capq) * 8;
     cudaError_t e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -859,7 +898,8 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.metric = b.metric;
     err_consts(b.d, &p.cK, &p.cN);
     const size_t smem = 1024 + 2 * static_cast<size_t>(p.nkb) * KB_BYTES + static_cast<size_t>(NS) * KB_BYTES +
-                        2 * sizeof(ItemSlot) + N_EPI * 64 * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t));
+                        2 * sizeof(ItemSlot) + N_EPI * 64 * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
+                        N_EPI * 32 * 32 * sizeof(float);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s)) != cudaSuccess) return e;

@@ -505,7 +505,9 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((n + 1) * sizeof(int32_t)));
     HY_CUDA(cudaMemsetAsync(h->b_ovf.p, 0, sizeof(int32_t), s));
-    const size_t wl = h->warmup_list ? h->warmup_list : 10;
+    // Warm-up for the bf16 form: its threshold only bounds the first pass
+    // (each query's nearest list), so three lists suffice by default.
+    const size_t wl = h->warmup_list ? std::min<size_t>(h->warmup_list, 3) : 3;
     const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
     HY_CHECK(std::min(wl, nprobe) * wls <= 32768, HY_ERR_ARG, "presearch: warmup_list * warmup_list_size above 32768");
     // Item descriptors: an upper bound on the item count from host-known
@@ -806,7 +808,7 @@ int hy_index_set_form(hy_index* h, int form) {
 int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice) {
     HY_CHECK(h, HY_ERR_ARG, "set_batch_params: NULL handle");
     if (capq) {
-        HY_CHECK(capq >= 64 && capq <= 32768, HY_ERR_ARG, "set_batch_params: capq must be in [64, 32768]");
+        HY_CHECK(capq >= 64 && capq <= 12288, HY_ERR_ARG, "set_batch_params: capq must be in [64, 12288]");
         h->capq = capq;
     }
     if (oversample) h->oversample = oversample;

@@ -131,8 +131,10 @@ HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
 HY_API int hy_index_set_form(hy_index* h, int form);
 
 /* bf16 form parameters (0 keeps the current value): candidate slots per
- * query (default 8192), re-rank oversampling factor (default 4) and rows per
- * work item (default 2048, multiple of 128). */
+ * query (default 8192, at most 12288), re-rank oversampling factor (kept for
+ * compatibility: the re-rank set is chosen by error bounds) and rows per work
+ * item (default 2048, a multiple of 128, at most 2048).  The bf16 form uses at
+ * most 3 warm-up lists (its warm-up threshold only bounds the first pass). */
 HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice);
 
 /* Warm-up threshold parameters.  Mirrors Index::preSearch's warmUpSearchList /
