@@ -84,6 +84,7 @@ def load():
     L.hy_file_inspect.argtypes = [C.c_char_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
+    L.hy_index_search_preassigned_noalloc.argtypes = [H, sz, vp, sz, sz, vp, vp, vp, vp]
     _lib = L
     return L
 

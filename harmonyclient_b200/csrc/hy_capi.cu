@@ -1007,6 +1007,39 @@ int hy_index_get_list(const hy_index* hc, size_t list, int64_t* ids, float* code
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Read-only view of an index's device data for entry points defined in other
+// files of the library (hy_noalloc.cu).
+namespace hy {
+struct IndexView {
+    ArenaLayout L;
+    const float* codes;
+    const int64_t* list_off;
+    const int32_t* list_size;
+    const int64_t* ids;
+    int metric;
+    size_t d, nlist;
+    int device;
+    bool trained, has_lists;
+};
+int index_view(const hy_index* h, IndexView* v) {
+    if (!h || !v) return fail(HY_ERR_ARG, "index_view: NULL argument");
+    v->L = h->L;
+    v->codes = h->codes.as<float>();
+    v->list_off = h->list_off.as<int64_t>();
+    v->list_size = h->list_size.as<int32_t>();
+    v->ids = h->ids.as<int64_t>();
+    v->metric = h->metric;
+    v->d = h->d;
+    v->nlist = h->nlist;
+    v->device = h->device;
+    v->trained = h->trained;
+    v->has_lists = !h->h_list_size.empty();
+    return HY_OK;
+}
+int set_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace hy
+
+// ---------------------------------------------------------------------------
 // The reference's .index format (src/Index.cpp:1708-1770, src/IVF.cpp:76-134):
 //   size_t d, size_t nlist, int32 metric, int32 opt_level, size_t sub_k,
 //   size_t sub_nlist, size_t sub_nprobe, float centroids[nlist*d], then for

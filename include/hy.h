@@ -186,6 +186,24 @@ HY_API int hy_index_load(hy_index* h, const char* path);
 HY_API int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metric, int* opt_level,
                            size_t* nonempty_lists, size_t* ntotal);
 
+/* Search with caller-given probe lists that allocates no device memory (no
+ * counterpart in the reference).  For callers that cannot call cudaMalloc
+ * while serving — their device memory belongs to another allocator (a
+ * framework's caching pool, an arena reserved at start-up), and cudaMalloc can
+ * synchronise the device or fail under memory pressure mid-serving.  dq
+ * (n x d float32), dprobes (n x nprobe list ids, -1 = skip), dD (n x k) and dI
+ * (n x k) are device pointers the caller owns; all temporaries live in a fixed
+ * 8 MiB __device__ array inside libhy.so, so a call needs
+ * n*nprobe*8 + n*nsplit*K'*8 bytes to fit (K' = k rounded up to 32/64/128/256,
+ * nsplit = 1 for n >= 296 queries) and larger batches are rejected with
+ * HY_ERR_ARG.  Results equal hy_index_search_preassigned's.  The call enqueues
+ * on `stream` and waits for it; its first call on a device looks up the
+ * array's device address, so make that call before any stream capture.  The
+ * array is shared by every call on a device: calls whose GPU work overlaps
+ * race and must be serialised by the caller. */
+HY_API int hy_index_search_preassigned_noalloc(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe,
+                                               const int64_t* dprobes, float* dD, int64_t* dI, void* stream);
+
 /* Diagnostic with no counterpart in the reference: multiplies one 128 x 128
  * bf16 tile pair on the tensor cores exactly as the batched scan does
  * (D = A * B^T, A and B row-major 128 x 128 float32 rounded to bf16, D
