@@ -21,6 +21,7 @@
 #include "../../include/hy.h"
 #include "hy_batched.cuh"
 #include "hy_kernels.cuh"
+#include "hy_mlp.cuh"
 
 using hy::ArenaLayout;
 
@@ -147,6 +148,15 @@ struct hy_index {
     DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
+
+    // learned probe predictor
+    bool model_ready = false;
+    int learned = 0;
+    float judge_fraction = 0.01f, judge_recall = 0.95f;
+    float margin = 0.0f;
+    int model_P = 0;
+    DevBuf m_params, m_mu, m_sd, m_X, m_y, m_work, m_pscore, m_total;
+    DevBuf t_X, t_t, t_Xb, t_tb, t_dy, t_loss, t_grads, t_am, t_av, t_perm, t_rows, t_D, t_I;
 };
 
 namespace {
@@ -361,7 +371,8 @@ int check_search_args(hy_index* h, size_t n, size_t k) {
 // Search n device queries with device probe lists (nprobe per query) into
 // device D/I.  Runs on stream s; does not synchronise.
 int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe, const int64_t* dprobes,
-                   const uint32_t* init_thr, float* dD, int64_t* dI, cudaStream_t s, bool timed) {
+                   const uint32_t* init_thr, float* dD, int64_t* dI, cudaStream_t s, bool timed,
+                   int64_t* drows = nullptr) {
     const int kp = k <= 32 ? 32 : k <= 64 ? 64 : k <= 128 ? 128 : 256;
     int nsplit = 1;
     const size_t target_ctas = 2 * 148;
@@ -403,7 +414,7 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
         return fail(HY_ERR_CUDA, std::string("scan launch (") + std::to_string(smem) + " B shared): " + cudaGetErrorString(e));
     if (timed) HY_CUDA(cudaEventRecord(h->ev[3], s));
     HY_CUDA(hy::launch_merge(h->w_parts.as<uint64_t>(), (int)n, nsplit, kp, (int)k, h->metric, h->ids.as<int64_t>(),
-                             dD, dI, s));
+                             dD, dI, s, drows));
     if (timed) HY_CUDA(cudaEventRecord(h->ev[4], s));
     return HY_OK;
 }
@@ -417,6 +428,32 @@ int ensure_common(hy_index* h) {
 int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
                      bool timed);
 
+bool learned_on(const hy_index* h) { return h->learned && h->model_ready; }
+
+// Chunk of queries whose probes (m x nprobe, best first) and their coarse
+// scores (h->m_pscore) are on the device: the probe network predicts each
+// query's nprobe and the probes beyond it become -1.
+int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s) {
+    const int B = 8192;
+    HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
+    HY_RET(h->m_X.ensure((size_t)B * hy::MLP_IN * sizeof(float)));
+    HY_RET(h->m_y.ensure((size_t)B * sizeof(float)));
+    HY_RET(h->m_work.ensure(hy::mlp_work_floats(B) * sizeof(float)));
+    hy::MlpWork w;
+    hy::mlp_work_bind(w, h->m_work.as<float>(), B);
+    for (size_t r0 = 0; r0 < m; r0 += B) {
+        const int b = (int)std::min<size_t>(B, m - r0);
+        HY_CUDA(hy::launch_probe_features(h->m_pscore.as<float>() + r0 * nprobe, b, (int)nprobe, h->m_mu.as<float>(),
+                                          h->m_sd.as<float>(), h->m_X.as<float>(), s));
+        HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), b, h->m_X.as<float>(), w, h->m_y.as<float>(), s));
+        HY_CUDA(hy::launch_apply_nprobe(h->m_y.as<float>(), b, h->margin, (int)nprobe,
+                                        h->w_probes.as<int64_t>() + r0 * nprobe, h->m_total.as<unsigned long long>(),
+                                        s));
+        h->launches += 9;
+    }
+    return HY_OK;
+}
+
 // Full device search: coarse quantisation, optional warm-up thresholds, scan,
 // merge, in query chunks.
 int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
@@ -429,6 +466,7 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
     const size_t qc = query_chunk(h->nlist, n);
     HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
     HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
+    if (learned_on(h)) HY_RET(h->m_pscore.ensure(qc * nprobe * sizeof(float)));
     const bool warm = h->warmup_list > 0 && h->metric == HY_METRIC_L2;
     if (warm) HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
     for (size_t q0 = 0; q0 < n; q0 += qc) {
@@ -438,8 +476,9 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
-                                  h->w_probes.as<int64_t>(), nullptr, s));
+                                  h->w_probes.as<int64_t>(), learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
         h->launches += 2;
+        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
         const uint32_t* thr = nullptr;
         if (warm) {
             h->launches += 1;
@@ -490,6 +529,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     const size_t nlist = h->nlist;
     HY_RET(h->w_scores.ensure(qc * nlist * sizeof(float)));
     HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
+    if (learned_on(h)) HY_RET(h->m_pscore.ensure(qc * nprobe * sizeof(float)));
     HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
     HY_RET(h->b_thr.ensure(qc * sizeof(float)));
     HY_RET(h->b_qb.ensure(qc * nkb * 64 * 2));
@@ -538,7 +578,8 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
-                                  nullptr, s));
+                                  learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
         if (h->metric == HY_METRIC_L2) {
             HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
                                       qq, (int)m, h->w_probes.as<int64_t>(), (int)nprobe, (int)k, (int)wl, (int)wls, 1,
@@ -621,6 +662,8 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
 int reset_counters(hy_index* h, cudaStream_t s) {
     HY_RET(ensure_common(h));
     h->launches = 0;
+    HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
+    HY_CUDA(cudaMemsetAsync(h->m_total.p, 0, sizeof(unsigned long long), s));
     HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 2 * sizeof(unsigned long long), s));
     return HY_OK;
 }
@@ -842,12 +885,13 @@ int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, flo
     return HY_OK;
 }
 
-int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
-    HY_CHECK(h && (n == 0 || (q && D && I)), HY_ERR_ARG, "search: NULL argument");
-    std::lock_guard<std::mutex> g(h->mu);
-    if (n == 0) return HY_OK;
-    HY_RET(check_search_args(h, n, k));
-    HY_RET(set_device(h));
+}  // extern "C"
+
+namespace {
+
+// The host-pointer search of one batch: upload, device search, download,
+// bf16 overflow fallback, statistics.
+int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
     cudaStream_t s = h->stream;
     HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
     HY_RET(h->w_D.ensure(n * k * sizeof(float)));
@@ -859,6 +903,12 @@ int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, i
     HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     HY_RET(finish_host_call(h, s, true, n, std::min(h->nprobe, h->nlist)));
     h->stats.fallback_queries = 0;
+    h->stats.mean_nprobe = (double)std::min(h->nprobe, h->nlist);
+    if (learned_on(h)) {
+        unsigned long long tot = 0;
+        HY_CUDA(cudaMemcpy(&tot, h->m_total.p, sizeof(tot), cudaMemcpyDeviceToHost));
+        h->stats.mean_nprobe = (double)tot / (double)n;
+    }
     if (h->form == HY_FORM_BF16 && h->arena_rows > 0) {
         const hy_search_stats_t keep = h->stats;
         HY_RET(bf16_fallback(h, q, n, k, D, I, s));
@@ -866,6 +916,281 @@ int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, i
         h->stats = keep;
         h->stats.fallback_queries = fb;
     }
+    return HY_OK;
+}
+
+// The learned nprobe is judged on every batch: a sample of the batch is
+// searched again with the fixed nprobe and the learned results' recall@10
+// against those is measured; below the target, the whole batch is searched
+// again with the fixed nprobe.
+int judge_learned(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
+    const size_t step = std::max<size_t>(1, (size_t)std::lround(1.0 / std::max(1e-6f, h->judge_fraction)));
+    std::vector<size_t> rows;
+    for (size_t i = 0; i < n; i += step) rows.push_back(i);
+    const size_t m = rows.size();
+    std::vector<float> sq(m * h->d), sD(m * k);
+    std::vector<int64_t> sI(m * k);
+    for (size_t i = 0; i < m; ++i) std::memcpy(&sq[i * h->d], q + rows[i] * h->d, h->d * sizeof(float));
+    const hy_search_stats_t keep = h->stats;
+    h->learned = 0;
+    const int rc = search_host(h, m, sq.data(), k, sD.data(), sI.data());
+    h->learned = 1;
+    h->stats = keep;
+    HY_RET(rc);
+    const size_t kk = std::min<size_t>(10, k);
+    size_t hit = 0, tot = 0;
+    for (size_t i = 0; i < m; ++i) {
+        const int64_t* a = I + rows[i] * k;
+        const int64_t* b = &sI[i * k];
+        for (size_t j = 0; j < kk; ++j) {
+            if (b[j] < 0) continue;
+            ++tot;
+            for (size_t t = 0; t < kk; ++t)
+                if (a[t] == b[j]) {
+                    ++hit;
+                    break;
+                }
+        }
+    }
+    const double recall = tot ? (double)hit / (double)tot : 1.0;
+    h->stats.judge_recall = recall;
+    h->stats.learned_fallback = 0;
+    if (recall < h->judge_recall) {
+        h->learned = 0;
+        const int rc2 = search_host(h, n, q, k, D, I);
+        h->learned = 1;
+        HY_RET(rc2);
+        h->stats.judge_recall = recall;
+        h->stats.learned_fallback = 1;
+    }
+    return HY_OK;
+}
+
+// Chunked exact labelling for the probe network: for every query, coarse
+// scores of its P best lists (features) and its stop label.
+int probe_training_data(hy_index* h, size_t n, const float* q, size_t P, size_t kl, float* X, float* lab,
+                        cudaStream_t s) {
+    const size_t qc = std::min<size_t>(query_chunk(h->nlist, n), 8192);
+    HY_RET(ensure_common(h));
+    HY_RET(h->w_q.ensure(qc * h->d * sizeof(float)));
+    HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
+    HY_RET(h->w_probes.ensure(qc * P * sizeof(int64_t)));
+    HY_RET(h->m_pscore.ensure(qc * P * sizeof(float)));
+    HY_RET(h->t_D.ensure(qc * kl * sizeof(float)));
+    HY_RET(h->t_I.ensure(qc * kl * sizeof(int64_t)));
+    HY_RET(h->t_rows.ensure(qc * kl * sizeof(int64_t)));
+    HY_RET(h->t_t.ensure(qc * sizeof(float)));
+    HY_RET(h->m_X.ensure(qc * hy::MLP_IN * sizeof(float)));
+    for (size_t q0 = 0; q0 < n; q0 += qc) {
+        const size_t m = std::min(qc, n - q0);
+        HY_CUDA(cudaMemcpyAsync(h->w_q.p, q + q0 * h->d, m * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+        HY_CUDA(hy::launch_coarse_scores(h->w_q.as<float>(), (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d,
+                                         h->metric, h->w_scores.as<float>(), s));
+        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)P, h->w_probes.as<int64_t>(),
+                                  h->m_pscore.as<float>(), s));
+        HY_CUDA(hy::launch_probe_features(h->m_pscore.as<float>(), (int)m, (int)P, nullptr, nullptr,
+                                          h->m_X.as<float>(), s));
+        HY_RET(scan_and_merge(h, m, h->w_q.as<float>(), kl, P, h->w_probes.as<int64_t>(), nullptr, h->t_D.as<float>(),
+                              h->t_I.as<int64_t>(), s, false, h->t_rows.as<int64_t>()));
+        HY_CUDA(hy::launch_stop_labels(h->t_rows.as<int64_t>(), (int)m, (int)kl, h->w_probes.as<int64_t>(), (int)P,
+                                       h->list_off.as<int64_t>(), (int)h->nlist, h->t_t.as<float>(), s));
+        HY_CUDA(cudaMemcpyAsync(X + q0 * hy::MLP_IN, h->m_X.p, m * hy::MLP_IN * sizeof(float), cudaMemcpyDeviceToHost, s));
+        HY_CUDA(cudaMemcpyAsync(lab + q0, h->t_t.p, m * sizeof(float), cudaMemcpyDeviceToHost, s));
+        HY_CUDA(cudaStreamSynchronize(s));
+    }
+    return HY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
+    HY_CHECK(h && (n == 0 || (q && D && I)), HY_ERR_ARG, "search: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    HY_RET(set_device(h));
+    HY_RET(search_host(h, n, q, k, D, I));
+    h->stats.judge_recall = -1.0;
+    h->stats.learned_fallback = 0;
+    if (learned_on(h) && h->judge_fraction > 0) HY_RET(judge_learned(h, n, q, k, D, I));
+    return HY_OK;
+}
+
+int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max_nprobe, size_t k_label, int epochs,
+                               float lr, float coverage, float* report) {
+    HY_CHECK(h && q && n >= 100, HY_ERR_ARG, "train_probe_model: need a handle and at least 100 queries");
+    HY_CHECK(k_label >= 1 && k_label <= HY_MAX_K && epochs >= 1 && lr > 0 && coverage > 0 && coverage < 1, HY_ERR_ARG,
+             "train_probe_model: bad k_label / epochs / lr / coverage");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_CHECK(h->trained && !h->h_list_size.empty(), HY_ERR_STATE, "train_probe_model: build the index first");
+    HY_RET(set_device(h));
+    cudaStream_t s = h->stream;
+    const size_t P = std::max<size_t>(1, std::min(max_nprobe, h->nlist));
+    // 1. features and exact stop labels
+    std::vector<float> X(n * hy::MLP_IN), lab(n);
+    HY_RET(probe_training_data(h, n, q, P, k_label, X.data(), lab.data(), s));
+    const size_t ntr = std::max<size_t>(1, n * 9 / 10), nva = n - ntr;
+    std::vector<float> t(n);
+    for (size_t i = 0; i < n; ++i) t[i] = std::log2(std::max(1.0f, lab[i]));
+    // 2. feature standardisation from the training part
+    std::vector<float> mu(hy::MLP_IN, 0.0f), sd(hy::MLP_IN, 0.0f);
+    for (size_t i = 0; i < ntr; ++i)
+        for (int f = 0; f < hy::MLP_IN; ++f) mu[f] += X[i * hy::MLP_IN + f];
+    for (int f = 0; f < hy::MLP_IN; ++f) mu[f] /= (float)ntr;
+    for (size_t i = 0; i < ntr; ++i)
+        for (int f = 0; f < hy::MLP_IN; ++f) {
+            const float dlt = X[i * hy::MLP_IN + f] - mu[f];
+            sd[f] += dlt * dlt;
+        }
+    for (int f = 0; f < hy::MLP_IN; ++f) sd[f] = std::sqrt(sd[f] / (float)ntr) + 1e-6f;
+    for (size_t i = 0; i < n; ++i)
+        for (int f = 0; f < hy::MLP_IN; ++f) X[i * hy::MLP_IN + f] = (X[i * hy::MLP_IN + f] - mu[f]) / sd[f];
+    // 3. initial weights (uniform, scaled by fan-in + fan-out; fixed seed)
+    std::vector<float> params(hy::MLP_NPARAM, 0.0f);
+    std::mt19937 rng(1234);
+    auto fill = [&](int off, int fin, int fout) {
+        const float a = std::sqrt(6.0f / (float)(fin + fout));
+        std::uniform_real_distribution<float> U(-a, a);
+        for (int i = 0; i < fin * fout; ++i) params[off + i] = U(rng);
+    };
+    fill(hy::MLP_W1, hy::MLP_IN, hy::MLP_H);
+    fill(hy::MLP_W2, hy::MLP_H, hy::MLP_H);
+    fill(hy::MLP_W3, hy::MLP_H, 1);
+    const int B = 256;
+    HY_RET(h->m_params.ensure(hy::MLP_NPARAM * sizeof(float)));
+    HY_RET(h->t_grads.ensure(hy::MLP_NPARAM * sizeof(float)));
+    HY_RET(h->t_am.ensure(hy::MLP_NPARAM * sizeof(float)));
+    HY_RET(h->t_av.ensure(hy::MLP_NPARAM * sizeof(float)));
+    HY_RET(h->t_X.ensure(n * hy::MLP_IN * sizeof(float)));
+    HY_RET(h->t_t.ensure(n * sizeof(float)));
+    HY_RET(h->t_Xb.ensure((size_t)B * hy::MLP_IN * sizeof(float)));
+    HY_RET(h->t_tb.ensure((size_t)B * sizeof(float)));
+    HY_RET(h->t_dy.ensure((size_t)B * sizeof(float)));
+    HY_RET(h->m_y.ensure(std::max<size_t>(B, 8192) * sizeof(float)));
+    HY_RET(h->t_loss.ensure(sizeof(float)));
+    HY_RET(h->t_perm.ensure(ntr * sizeof(int64_t)));
+    HY_RET(h->m_work.ensure(hy::mlp_work_floats(8192) * sizeof(float)));
+    HY_CUDA(cudaMemcpyAsync(h->m_params.p, params.data(), params.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemsetAsync(h->t_am.p, 0, hy::MLP_NPARAM * sizeof(float), s));
+    HY_CUDA(cudaMemsetAsync(h->t_av.p, 0, hy::MLP_NPARAM * sizeof(float), s));
+    HY_CUDA(cudaMemcpyAsync(h->t_X.p, X.data(), X.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->t_t.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    hy::MlpWork w;
+    hy::mlp_work_bind(w, h->m_work.as<float>(), B);
+    // 4. Adam on mini-batches of 256, reshuffled every epoch
+    std::vector<int64_t> perm(ntr);
+    std::iota(perm.begin(), perm.end(), 0);
+    int step = 0;
+    double last_loss = 0.0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        HY_CUDA(cudaMemcpyAsync(h->t_perm.p, perm.data(), ntr * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        HY_CUDA(cudaStreamSynchronize(s));
+        double eloss = 0.0;
+        int nb = 0;
+        for (size_t b0 = 0; b0 + B <= ntr; b0 += B) {
+            const int64_t* idx = h->t_perm.as<int64_t>() + b0;
+            HY_CUDA(hy::launch_gather_rows(h->t_X.as<float>(), idx, B, hy::MLP_IN, h->t_Xb.as<float>(), s));
+            HY_CUDA(hy::launch_gather_rows(h->t_t.as<float>(), idx, B, 1, h->t_tb.as<float>(), s));
+            HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), B, h->t_Xb.as<float>(), w, h->m_y.as<float>(), s));
+            HY_CUDA(hy::mlp_mse(B, h->m_y.as<float>(), h->t_tb.as<float>(), h->t_dy.as<float>(), h->t_loss.as<float>(), s));
+            HY_CUDA(hy::mlp_backward(h->m_params.as<float>(), B, h->t_Xb.as<float>(), w, h->t_dy.as<float>(),
+                                     h->t_grads.as<float>(), s));
+            HY_CUDA(hy::mlp_adam(h->m_params.as<float>(), h->t_grads.as<float>(), h->t_am.as<float>(), h->t_av.as<float>(),
+                                 ++step, lr, s));
+            if (ep == epochs - 1) {
+                float lv = 0.0f;
+                HY_CUDA(cudaMemcpyAsync(&lv, h->t_loss.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+                HY_CUDA(cudaStreamSynchronize(s));
+                eloss += lv;
+                ++nb;
+            }
+        }
+        if (ep == epochs - 1) last_loss = nb ? eloss / nb : 0.0;
+    }
+    // 5. margin: the `coverage` quantile of (label - prediction) on held-out
+    // queries, so that fraction of them gets at least its stop point.
+    const size_t nv = nva ? nva : ntr;
+    const size_t v0 = nva ? ntr : 0;
+    std::vector<float> yv(nv);
+    hy::MlpWork wv;
+    hy::mlp_work_bind(wv, h->m_work.as<float>(), 8192);
+    for (size_t r0 = 0; r0 < nv; r0 += 8192) {
+        const int b = (int)std::min<size_t>(8192, nv - r0);
+        HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), b, h->t_X.as<float>() + (v0 + r0) * hy::MLP_IN, wv,
+                                h->m_y.as<float>(), s));
+        HY_CUDA(cudaMemcpyAsync(yv.data() + r0, h->m_y.p, b * sizeof(float), cudaMemcpyDeviceToHost, s));
+        HY_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<float> resid(nv);
+    for (size_t i = 0; i < nv; ++i) resid[i] = t[v0 + i] - yv[i];
+    std::vector<float> sorted = resid;
+    std::sort(sorted.begin(), sorted.end());
+    const float margin = sorted[std::min(nv - 1, (size_t)std::ceil(coverage * (double)nv) - 1)];
+    double mean_np = 0.0, covered = 0.0, mean_lab = 0.0;
+    for (size_t i = 0; i < nv; ++i) {
+        const float e = std::exp2(std::min(yv[i] + margin, 30.0f));
+        const double np = std::max(1.0, std::min((double)P, std::ceil((double)e)));
+        mean_np += np;
+        covered += np >= lab[v0 + i] ? 1.0 : 0.0;
+        mean_lab += lab[v0 + i];
+    }
+    h->margin = margin;
+    h->model_P = (int)P;
+    HY_RET(h->m_mu.ensure(hy::MLP_IN * sizeof(float)));
+    HY_RET(h->m_sd.ensure(hy::MLP_IN * sizeof(float)));
+    HY_CUDA(cudaMemcpy(h->m_mu.p, mu.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    HY_CUDA(cudaMemcpy(h->m_sd.p, sd.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    h->model_ready = true;
+    if (report) {
+        report[0] = (float)last_loss;
+        report[1] = (float)(covered / (double)nv);
+        report[2] = (float)(mean_np / (double)nv);
+        report[3] = (float)(mean_lab / (double)nv);
+    }
+    return HY_OK;
+}
+
+int hy_index_set_learned(hy_index* h, int enabled, float judge_fraction, float judge_recall) {
+    HY_CHECK(h, HY_ERR_ARG, "set_learned: NULL handle");
+    HY_CHECK(!enabled || h->model_ready, HY_ERR_STATE, "set_learned: no probe model (train or set one first)");
+    HY_CHECK(judge_fraction >= 0 && judge_fraction <= 1 && judge_recall >= 0 && judge_recall <= 1, HY_ERR_ARG,
+             "set_learned: judge_fraction and judge_recall must be in [0, 1]");
+    h->learned = enabled ? 1 : 0;
+    h->judge_fraction = judge_fraction;
+    h->judge_recall = judge_recall;
+    return HY_OK;
+}
+
+size_t hy_probe_model_size(void) { return (size_t)hy::MLP_NPARAM + 2 * hy::MLP_IN + 2; }
+
+int hy_index_get_probe_model(const hy_index* hc, float* out) {
+    HY_CHECK(hc && out, HY_ERR_ARG, "get_probe_model: NULL argument");
+    HY_CHECK(hc->model_ready, HY_ERR_STATE, "get_probe_model: no probe model");
+    hy_index* h = const_cast<hy_index*>(hc);
+    HY_RET(set_device(h));
+    HY_CUDA(cudaMemcpy(out, h->m_params.p, hy::MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    HY_CUDA(cudaMemcpy(out + hy::MLP_NPARAM, h->m_mu.p, hy::MLP_IN * sizeof(float), cudaMemcpyDeviceToHost));
+    HY_CUDA(cudaMemcpy(out + hy::MLP_NPARAM + hy::MLP_IN, h->m_sd.p, hy::MLP_IN * sizeof(float), cudaMemcpyDeviceToHost));
+    out[hy::MLP_NPARAM + 2 * hy::MLP_IN] = h->margin;
+    out[hy::MLP_NPARAM + 2 * hy::MLP_IN + 1] = (float)h->model_P;
+    return HY_OK;
+}
+
+int hy_index_set_probe_model(hy_index* h, const float* in) {
+    HY_CHECK(h && in, HY_ERR_ARG, "set_probe_model: NULL argument");
+    HY_RET(set_device(h));
+    HY_RET(h->m_params.ensure(hy::MLP_NPARAM * sizeof(float)));
+    HY_RET(h->m_mu.ensure(hy::MLP_IN * sizeof(float)));
+    HY_RET(h->m_sd.ensure(hy::MLP_IN * sizeof(float)));
+    HY_CUDA(cudaMemcpy(h->m_params.p, in, hy::MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    HY_CUDA(cudaMemcpy(h->m_mu.p, in + hy::MLP_NPARAM, hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    HY_CUDA(cudaMemcpy(h->m_sd.p, in + hy::MLP_NPARAM + hy::MLP_IN, hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    h->margin = in[hy::MLP_NPARAM + 2 * hy::MLP_IN];
+    h->model_P = (int)in[hy::MLP_NPARAM + 2 * hy::MLP_IN + 1];
+    h->model_ready = true;
     return HY_OK;
 }
 

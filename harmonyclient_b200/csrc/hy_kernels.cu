@@ -559,7 +559,8 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
 // values (FLT_MAX / -FLT_MAX, id -1; src/heap.hpp:13-25).
 __global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__ parts, int nparts, int kp, int k,
                                                     int metric, const int64_t* __restrict__ ids,
-                                                    float* __restrict__ D, int64_t* __restrict__ I) {
+                                                    float* __restrict__ D, int64_t* __restrict__ I,
+                                                    int64_t* __restrict__ rows) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t* a = reinterpret_cast<uint64_t*>(sm);
     const size_t qi = blockIdx.x;
@@ -587,6 +588,7 @@ __global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__
         }
         D[qi * k + i] = dv;
         I[qi * k + i] = iv;
+        if (rows) rows[qi * k + i] = key == KEY_MAX ? -1 : static_cast<int64_t>(key & 0xffffffffu);
     }
 }
 
@@ -800,14 +802,14 @@ cudaError_t launch_scan_plain(const ScanParams& p, int* smem_out, cudaStream_t s
 }
 
 cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int k, int metric, const int64_t* ids,
-                         float* D, int64_t* I, cudaStream_t s) {
+                         float* D, int64_t* I, cudaStream_t s, int64_t* rows) {
     const size_t smem = nparts > 1 ? static_cast<size_t>(next_pow2(nparts * kp)) * 8 : 0;
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         configured = true;
     }
-    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I);
+    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I, rows);
     return cudaGetLastError();
 }
 
@@ -871,6 +873,93 @@ cudaError_t launch_normalize_centroids(float* cent, int nlist, int d, cudaStream
 cudaError_t launch_unpack_list(const ArenaLayout& L, const float* codes, int64_t row0, int n, float* out,
                                cudaStream_t s) {
     unpack_list_kernel<<<grid_for(static_cast<int64_t>(n) * L.d, 256), 256, 0, s>>>(L, codes, row0, n, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Learned probe predictor: features, stop labels, per-query nprobe.
+namespace {
+
+// Features of one query from its P best centroid scores (ascending): f0 =
+// log|s0|, fi = log1p((si - s0) / |s0|) for the next 63 (the last score is
+// repeated when P < 64); then standardised with the model's mean and std.
+__global__ void probe_features_kernel(const float* __restrict__ scores, int n, int P, const float* __restrict__ mu,
+                                      const float* __restrict__ sd, float* __restrict__ X) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= static_cast<int64_t>(n) * 64) return;
+    const int64_t q = i / 64;
+    const int f = static_cast<int>(i % 64);
+    const float* sc = scores + q * P;
+    const float s0 = sc[0];
+    const float a0 = fabsf(s0) + 1e-6f;
+    float v;
+    if (f == 0)
+        v = logf(a0);
+    else
+        v = log1pf(fmaxf(sc[min(f, P - 1)] - s0, 0.0f) / a0);
+    X[i] = mu ? (v - mu[f]) / sd[f] : v;
+}
+
+// Stop label of each query: 1 + the largest probe rank among the lists that
+// hold its exact top-kl rows (arena rows from the merge), i.e. the smallest
+// nprobe whose lists contain all of them.
+__global__ void stop_labels_kernel(const int64_t* __restrict__ rows, int n, int kl, const int64_t* __restrict__ probes,
+                                   int P, const int64_t* __restrict__ list_off, int nlist, float* __restrict__ label) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int worst = 0;
+    for (int i = 0; i < kl; ++i) {
+        const int64_t r = rows[static_cast<int64_t>(q) * kl + i];
+        if (r < 0) continue;
+        int lo = 0, hi = nlist - 1;  // list = last l with list_off[l] <= r
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (list_off[mid] <= r)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        int rank = P - 1;
+        for (int j = 0; j < P; ++j)
+            if (probes[static_cast<int64_t>(q) * P + j] == lo) {
+                rank = j;
+                break;
+            }
+        worst = max(worst, rank);
+    }
+    label[q] = static_cast<float>(worst + 1);
+}
+
+// Per-query nprobe = clamp(ceil(2^(y + margin)), 1, P); probes beyond it
+// become -1.  Adds the chosen counts to *total.
+__global__ void apply_nprobe_kernel(const float* __restrict__ y, int n, float margin, int P,
+                                    int64_t* __restrict__ probes, unsigned long long* __restrict__ total) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const float e = exp2f(fminf(y[q] + margin, 30.0f));
+    int np = static_cast<int>(ceilf(e));
+    np = max(1, min(P, np));
+    for (int j = np; j < P; ++j) probes[static_cast<int64_t>(q) * P + j] = -1;
+    atomicAdd(total, static_cast<unsigned long long>(np));
+}
+
+}  // namespace
+
+cudaError_t launch_probe_features(const float* scores, int n, int P, const float* mu, const float* sd, float* X,
+                                  cudaStream_t s) {
+    probe_features_kernel<<<grid_for(static_cast<int64_t>(n) * 64, 256), 256, 0, s>>>(scores, n, P, mu, sd, X);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stop_labels(const int64_t* rows, int n, int kl, const int64_t* probes, int P,
+                               const int64_t* list_off, int nlist, float* label, cudaStream_t s) {
+    stop_labels_kernel<<<grid_for(n, 128), 128, 0, s>>>(rows, n, kl, probes, P, list_off, nlist, label);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_nprobe(const float* y, int n, float margin, int P, int64_t* probes,
+                                unsigned long long* total, cudaStream_t s) {
+    apply_nprobe_kernel<<<grid_for(n, 128), 128, 0, s>>>(y, n, margin, P, probes, total);
     return cudaGetLastError();
 }
 

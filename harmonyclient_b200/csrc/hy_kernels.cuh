@@ -61,8 +61,17 @@ cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_
                           const int32_t* list_size, const float* q, int nq, const int64_t* probes, int nprobe, int k,
                           int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s);
 cudaError_t launch_scan_plain(const ScanParams& p, int* smem_bytes_out, cudaStream_t s);
+// rows (optional): the arena row of every result (-1 when unfilled).
 cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int k, int metric, const int64_t* ids,
-                         float* D, int64_t* I, cudaStream_t s);
+                         float* D, int64_t* I, cudaStream_t s, int64_t* rows = nullptr);
+
+// Learned probe predictor helpers (see hy_kernels.cu).
+cudaError_t launch_probe_features(const float* scores, int n, int P, const float* mu, const float* sd, float* X,
+                                  cudaStream_t s);
+cudaError_t launch_stop_labels(const int64_t* rows, int n, int kl, const int64_t* probes, int P,
+                               const int64_t* list_off, int nlist, float* label, cudaStream_t s);
+cudaError_t launch_apply_nprobe(const float* y, int n, float margin, int P, int64_t* probes,
+                                unsigned long long* total, cudaStream_t s);
 
 // Index construction.
 cudaError_t launch_histogram(const int64_t* labels, int64_t n, int32_t* counts, cudaStream_t s);

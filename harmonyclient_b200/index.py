@@ -171,6 +171,30 @@ class Index:
         check(self._L.hy_index_last_stats(self._h, C.byref(st)))
         return st.as_dict()
 
+    def train_probe_model(self, queries, max_nprobe=64, k_label=10, epochs=30, lr=1e-3, coverage=0.97):
+        """Train the learned probe predictor on sample queries (labels come
+        from the exact scan at max_nprobe).  Returns the held-out report."""
+        q = _f32(queries, self.d)
+        rep = np.zeros(4, np.float32)
+        check(self._L.hy_index_train_probe_model(self._h, q.shape[0], _p(q), int(max_nprobe), int(k_label),
+                                                  int(epochs), float(lr), float(coverage), _p(rep)))
+        return {"loss": float(rep[0]), "coverage": float(rep[1]), "mean_nprobe": float(rep[2]),
+                "mean_label": float(rep[3])}
+
+    def set_learned(self, enabled=True, judge_fraction=0.01, judge_recall=0.95):
+        check(self._L.hy_index_set_learned(self._h, int(bool(enabled)), float(judge_fraction), float(judge_recall)))
+
+    def get_probe_model(self):
+        m = np.zeros(self._L.hy_probe_model_size(), np.float32)
+        check(self._L.hy_index_get_probe_model(self._h, _p(m)))
+        return m
+
+    def set_probe_model(self, model):
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.size != self._L.hy_probe_model_size():
+            raise ValueError("probe model has the wrong size")
+        check(self._L.hy_index_set_probe_model(self._h, _p(m)))
+
     def list_size(self, l):
         s = C.c_size_t()
         check(self._L.hy_index_list_size(self._h, int(l), C.byref(s)))

@@ -87,6 +87,9 @@ typedef struct {
     double merge_ms;          /* device time of the top-k merge */
     uint64_t launches;        /* kernels this library launched for the call */
     uint64_t fallback_queries; /* bf16 form: queries answered again by the plain scan */
+    double mean_nprobe;       /* lists probed per query (learned: the predicted mean) */
+    double judge_recall;      /* learned: recall@10 of the judged sample vs fixed nprobe (-1: not judged) */
+    uint64_t learned_fallback; /* learned: 1 when the batch was searched again with fixed nprobe */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -203,6 +206,36 @@ HY_API int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metr
  * race and must be serialised by the caller. */
 HY_API int hy_index_search_preassigned_noalloc(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe,
                                                const int64_t* dprobes, float* dD, int64_t* dI, void* stream);
+
+/* Learned probe predictor (no counterpart in the reference, whose nprobe is
+ * fixed per call).  A small MLP (64 -> 256 -> 256 -> 1, GELU, bf16 matrix
+ * products with f32 accumulation) reads a query's sorted coarse distances to
+ * its 64 nearest lists and predicts how many lists it needs.
+ * hy_index_train_probe_model labels n training queries with the exact scan at
+ * max_nprobe (stop label = the smallest nprobe whose lists hold the exact
+ * top-k_label), trains the network on the GPU with Adam (epochs, lr) and sets
+ * a margin so that a `coverage` fraction of held-out queries gets at least
+ * its stop label.  report (may be NULL) receives {final training loss,
+ * held-out coverage, held-out mean predicted nprobe, held-out mean stop
+ * label}.  With hy_index_set_learned(h, 1, judge_fraction, judge_recall) every
+ * search predicts a per-query nprobe (at most the index's nprobe); the host
+ * search also searches every (1/judge_fraction)-th query again with the fixed
+ * nprobe, and if the learned results' recall@10 on that sample is below
+ * judge_recall the batch is searched again with the fixed nprobe.  The model
+ * is hy_probe_model_size() floats (weights, feature mean and scale, margin,
+ * max nprobe). */
+HY_API int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max_nprobe, size_t k_label,
+                                      int epochs, float lr, float coverage, float* report);
+HY_API int hy_index_set_learned(hy_index* h, int enabled, float judge_fraction, float judge_recall);
+HY_API size_t hy_probe_model_size(void);
+HY_API int hy_index_get_probe_model(const hy_index* h, float* model);
+HY_API int hy_index_set_probe_model(hy_index* h, const float* model);
+
+/* Loss and gradients of the probe network on one batch (host pointers:
+ * params hy_probe_model_size()-2*64-2 floats, X B x 64, targets B; grads like
+ * params) for checking the training kernels against a reference.  No
+ * counterpart in the reference. */
+HY_API int hy_mlp_loss_grad(const float* params, int B, const float* X, const float* t, float* loss, float* grads);
 
 /* Diagnostic with no counterpart in the reference: multiplies one 128 x 128
  * bf16 tile pair on the tensor cores exactly as the batched scan does
