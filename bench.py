@@ -1,14 +1,19 @@
 """Benchmark of the IVF query hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--nprobe 64] [--nb 1000000] [--nq 10000]
+                    [--form learned|bf16|plain] [--nprobe 64] [--nb 1000000] [--nq 10000]
 
 Workload (one "step" = one batch search): 1,000,000 x 128 integer-valued
 float32 vectors in [0,255] from a 4,096-component Gaussian mixture (seeded,
 synthetic), nlist 1024 trained on the GPU, 10,000 queries from the same
-mixture, k 100, nprobe 64 (recall@10 against an FP64 brute force is reported
-for the first 10 of the 100).  The list arena (~550 MB) is larger than L2,
-so no L2 flush is needed between steps.
+mixture, k 100, nprobe 64; recall@10 against an FP64 brute force on a query
+sample.  The list arena (~550 MB) is larger than L2, so no L2 flush is
+needed between steps.
+
+The headline form (--form learned) trains the probe network on 20,000 other
+queries from the mixture, then searches with per-query nprobe on the bf16
+tensor-core scan with the exact FP32 re-rank; the plain FP32 scan at the
+fixed nprobe is timed in the same run ("plain_fp32", with its HBM roofline).
 
 Prints one JSON line on rank 0.  Under torchrun each rank holds a replica of
 the index and searches its own query batch (weak scaling, no collective on
@@ -95,7 +100,8 @@ def workload(args, rank):
     from harmonyclient_b200 import datasets
     x, q = datasets.gmm_uint8(args.nb, args.nq, seed=0)
     if rank:
-        _, q = datasets.gmm_uint8(args.nb, args.nq, seed=1000 + rank)
+        # Other ranks search their own queries from the same mixture.
+        _, q = datasets.gmm_uint8(0, args.nq, seed=0, query_seed=1000 + rank)
     return x, q
 
 
@@ -122,62 +128,106 @@ def cpu_baseline_ref(x, q, cent, nprobe, k, budget_s):
             "sample": f"{m2} of {q.shape[0]} queries, reference Index::search ORIGINAL mode, OpenMP x{nt}"}
 
 
+def _time_device(idx, dq, dD, dI, k, steps, stream, dist, dev):
+    """Device-timed loop of `steps` batch searches (CUDA events on the
+    launching stream, max over ranks); the last step's stats come back."""
+    import torch
+    n = dq.shape[0]
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")  # profilers select the timed launches by this range
+        e0.record()
+        for _ in range(steps):
+            idx.search_device(n, dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        e1.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+    st = idx.last_stats()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), st, clk.summary()
+
+
+def _kernel_ms(idx, dq, dD, dI, k, reps, stream):
+    """Average duration of the dominant scan kernel's launches: every
+    launch is bracketed by CUDA events on its own stream inside the library;
+    `reps` further searches, each read back."""
+    import torch
+    tot, launches = 0.0, 0
+    for _ in range(reps):
+        idx.search_device(dq.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        st = idx.last_stats()
+        tot += st["kernel_ms"]
+        launches += st["kernel_launches"]
+    torch.cuda.synchronize()
+    return tot / max(launches, 1), launches / max(reps, 1)
+
+
+def _recall10(x, q, I, ns):
+    from oracle import port
+    ns = min(ns, q.shape[0])
+    _, It = port.bruteforce_f64(x, q[:ns], 10)
+    return float(np.mean([len(set(a) & set(b)) / 10 for a, b in zip(I[:ns, :10].tolist(), It.tolist())])), ns
+
+
 def run_ours(args, rank, world, dist):
+    import ctypes as C
+
     import torch
 
     import harmonyclient_b200 as hb
-    from harmonyclient_b200 import _lib
+    from harmonyclient_b200 import _lib, datasets
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     x, q = workload(args, rank)
-    nlist, k = 1024, 100
-    idx = hb.Index(128, nlist, args.nprobe, hb.METRIC_L2, device=dev)
+    nlist, k, d = 1024, 100, 128
+    idx = hb.Index(d, nlist, args.nprobe, hb.METRIC_L2, device=dev)
     t0 = time.perf_counter()
     idx.train(x)
     idx.add(x)
     # Warm-up thresholds as the reference's default run uses them
     # (--warmup_list 10, warmup_list_size = k; src/query.cpp:845-847).
     idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
-    idx.set_form(args.form)
     build_s = time.perf_counter() - t0
-    cent = idx.centroid_codes
+    learned = args.form == "learned"
+    probe_report, train_s = None, 0.0
+    if learned:
+        # The probe network is trained on its own query sample from the same
+        # mixture (labels from the exact scan at the index's nprobe).
+        _, tq = datasets.gmm_uint8(0, args.train_queries, seed=0, query_seed=777)
+        t0 = time.perf_counter()
+        probe_report = idx.train_probe_model(tq, max_nprobe=args.nprobe, k_label=10, epochs=args.epochs,
+                                             lr=1e-3, coverage=args.coverage)
+        train_s = time.perf_counter() - t0
+        idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
+    idx.set_form("plain" if args.form == "plain" else "bf16")
 
     stream = torch.cuda.current_stream().cuda_stream
     dq = torch.from_numpy(q).cuda()
     dD = torch.empty((q.shape[0], k), dtype=torch.float32, device="cuda")
     dI = torch.empty((q.shape[0], k), dtype=torch.int64, device="cuda")
-
-    def step():
-        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
-
     for _ in range(args.warmup):
-        step()
+        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(dev) as clk:
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(args.steps):
-            step()
-        e1.record()
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max, st_dev, clocks = _time_device(idx, dq, dD, dI, k, args.steps, stream, dist, dev)
     value = world * q.shape[0] * args.steps / (ms_max / 1e3)
+    I_main = dI.cpu().numpy()
+    kern_ms, kern_per_search = _kernel_ms(idx, dq, dD, dI, k, 3, stream)
 
     # End to end through the public host API: pinned host queries in, results
-    # back to pinned host memory, every step.
+    # back to pinned host memory, every step (with the learned form this
+    # includes the recall judge's fixed-nprobe search of 1% of the batch).
     hq = torch.from_numpy(q).pin_memory()
     hD = torch.empty((q.shape[0], k), dtype=torch.float32).pin_memory()
     hI = torch.empty((q.shape[0], k), dtype=torch.int64).pin_memory()
     L = _lib.load()
-    import ctypes as C
 
     def e2e_step():
         _lib.check(L.hy_index_search(idx._h, q.shape[0], C.c_void_p(hq.data_ptr()), k, C.c_void_p(hD.data_ptr()),
@@ -188,60 +238,93 @@ def run_ours(args, rank, world, dist):
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    scan_ms, loaded, possible, launches, fallback = [], 0, 0, 0, 0
+    launches, fallback, judge, learned_fb, mean_np = 0, 0, [], 0, []
     for _ in range(args.steps):
         e2e_step()
         st = idx.last_stats()
-        scan_ms.append(st["scan_ms"])
-        loaded, possible, launches = st["tile_blocks"], st["tile_blocks_max"], st["launches"]
+        launches = st["launches"]
         fallback = max(fallback, st["fallback_queries"])
+        judge.append(st["judge_recall"])
+        learned_fb += st["learned_fallback"]
+        mean_np.append(st["mean_nprobe"])
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], device="cuda")
     if dist:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * q.shape[0] * args.steps / float(te.item())
 
+    # The plain FP32 scan on the same index and queries (fixed nprobe), the
+    # comparison the headline metric names; it also gives the scan's HBM
+    # fraction.
+    plain = None
+    P_main = idx.probes(q)
+    if args.form != "plain" and args.plain_steps > 0:
+        if learned:
+            idx.set_learned(False)
+        idx.set_form("plain")
+        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev)
+        pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream)
+        plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "clocks": pclk}
+        idx.set_form("bf16")
+        if learned:
+            idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
+
     if rank != 0:
         return None
 
-    # Roofline of the dominant kernel (the list scan): algorithmic bytes are
-    # the pair bytes sum_q sum_{l in probes(q)} |l| * d * 4 plus query and
-    # result bytes; the bytes the kernel actually loads after pruning are
-    # reported beside them.
-    P = idx.probes(q)
     sizes = np.array([idx.list_size(l) for l in range(nlist)], np.int64)
-    pair_rows = int(sizes[P].sum())
-    alg_bytes = pair_rows * 128 * 4 + q.shape[0] * 128 * 4 + q.shape[0] * k * 12
-    scan_avg = statistics.mean(scan_ms)
+
+    def pair_rows(P):
+        return int(np.where(P >= 0, sizes[np.maximum(P, 0)], 0).sum())
+
     hbm_peak, tc_peak, peak_kind = peaks()
+    learned_probes = int((P_main >= 0).sum())
+    rows_main = pair_rows(P_main)
     if args.form == "plain":
-        achieved = alg_bytes / (scan_avg / 1e3) / 1e9
-        loaded_bytes = loaded * 32 * 32 * 4
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "kernel": "scan_plain_kernel", "kernel_ms": round(scan_avg, 4), "algorithmic_bytes": alg_bytes,
-                "loaded_bytes": loaded_bytes, "loaded_frac_of_unpruned": round(loaded / max(possible, 1), 4)}
+        # Algorithmic bytes of one scan launch: every (query, probed row)
+        # pair's row, d x 4 bytes, plus the queries and the results.
+        alg = rows_main * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
+        ach = alg / (kern_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(ach / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "scan_plain_kernel", "kernel_ms": round(kern_ms, 4), "algorithmic_bytes": alg}
     else:
-        # Algorithmic work of the batched scan: one 2*d-flop inner product per
-        # (query, probed row) pair, on the bf16 tensor cores.
-        alg_flops = pair_rows * 2 * 128
-        achieved = alg_flops / (scan_avg / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": tc_peak, "unit": "TFLOP/s",
-                "frac": round(achieved / tc_peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "kernel": "batched_scan_kernel", "kernel_ms": round(scan_avg, 4), "algorithmic_flops": alg_flops,
-                "pair_bytes_fp32": alg_bytes}
+        # Algorithmic work of one batched-scan launch: a 2d-flop inner product
+        # per (query, probed row) pair on the bf16 tensor cores; the two
+        # passes of a search together cover all pairs once.
+        alg = rows_main * 2 * d / kern_per_search
+        ach = alg / (kern_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": tc_peak, "unit": "TFLOP/s",
+                "frac": round(ach / tc_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "batched_scan_kernel", "kernel_ms": round(kern_ms, 4),
+                "algorithmic_flops": int(alg), "launches_per_search": kern_per_search}
 
-    # recall@10 against FP64 brute force on a query sample
-    from oracle import port
-    ns = min(args.recall_sample, q.shape[0])
-    Dt, It = port.bruteforce_f64(x, q[:ns], 10)
-    I_ours = dI[:ns, :10].cpu().numpy()
-    recall10 = float(np.mean([len(set(a) & set(b)) / 10 for a, b in zip(I_ours.tolist(), It.tolist())]))
+    recall10, ns = _recall10(x, q, I_main, args.recall_sample)
+    plain_line = None
+    if plain is not None:
+        if learned:
+            idx.set_learned(False)
+        P_plain = idx.probes(q)
+        prow = pair_rows(P_plain)
+        palg = prow * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
+        pach = palg / (plain["kernel_ms"] / 1e3) / 1e9
+        prec, _ = _recall10(x, q, plain["I"], args.recall_sample)
+        pv = world * q.shape[0] * args.plain_steps / (plain["ms"] / 1e3)
+        plain_line = {"value": round(pv, 1), "unit": "queries/s", "steps": args.plain_steps,
+                      "ms_per_step": round(plain["ms"] / args.plain_steps, 3), "recall_at_10": round(prec, 4),
+                      "nprobe": args.nprobe, "speedup_of_headline": round(value / pv, 2),
+                      "roofline": {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
+                                   "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
+                                   "kernel": "scan_plain_kernel", "kernel_ms": round(plain["kernel_ms"], 4),
+                                   "algorithmic_bytes": palg},
+                      "clocks": plain["clocks"]}
 
-    cpu = cpu_baseline_ref(x, q, cent, args.nprobe, k, args.cpu_budget)
-
+    cpu = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
     h2d = q.nbytes
     d2h = q.shape[0] * k * 12
+    form_name = {"learned": "learned probes + bf16 tcgen05 scan + exact FP32 re-rank",
+                 "bf16": "bf16 tcgen05 scan + exact FP32 re-rank", "plain": "plain FP32 scan"}[args.form]
     line = {
         "metric": METRIC,
         "value": round(value, 1),
@@ -253,25 +336,34 @@ def run_ours(args, rank, world, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f32" if args.form == "plain" else "bf16",
         "data": "synthetic (seeded Gaussian mixture, integer-valued in [0,255])",
-        "form": args.form,
-        "config": {"workload": f"{args.nb} x 128 uint8-valued gmm, nlist {nlist}, nprobe {args.nprobe}, "
-                               f"k {k}, {q.shape[0]} queries per step per GPU",
-                   "nb": args.nb, "d": 128, "nlist": nlist, "nprobe": args.nprobe, "k": k, "nq": q.shape[0],
+        "form": form_name,
+        "config": {"workload": f"{args.nb} x {d} uint8-valued gmm (4096 components, sigma 20), nlist {nlist}, "
+                               f"nprobe {args.nprobe}, k {k}, {q.shape[0]} queries per step per GPU",
+                   "nb": args.nb, "d": d, "nlist": nlist, "nprobe": args.nprobe, "k": k, "nq": q.shape[0],
                    "l2_flush": "not needed: list arena larger than L2", "parallelism": f"replicas x{world}"},
         "recall_at_10": round(recall10, 4),
-        "recall_sample": ns,
+        "recall_vs": f"FP64 brute force, first {ns} queries",
+        "mean_nprobe": round(learned_probes / q.shape[0], 3),
         "roofline": roof,
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches) * args.steps,
+        "gpu_launches": int(st_dev["launches"]) * args.steps,
+        "plain_fp32": plain_line,
         "warmup_list": args.warmup_list,
         "fallback_queries": fallback,
         "cpu_baseline": cpu,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "build_s": round(build_s, 2),
     }
+    if learned:
+        line["probe_model"] = {"train_queries": args.train_queries, "epochs": args.epochs,
+                               "coverage_target": args.coverage, "train_s": round(train_s, 2),
+                               "heldout": {kk: round(v, 4) for kk, v in probe_report.items()},
+                               "judge_fraction": args.judge_fraction,
+                               "judge_recall_min": round(min(judge), 4) if judge else None,
+                               "judge_fallbacks": learned_fb}
     return line
 
 
@@ -324,7 +416,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nprobe", type=int, default=64)
     ap.add_argument("--warmup-list", type=int, default=10)
-    ap.add_argument("--form", default="bf16", choices=["plain", "bf16"])
+    ap.add_argument("--form", default="learned", choices=["learned", "bf16", "plain"])
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--train-queries", type=int, default=20000)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--coverage", type=float, default=0.97)
+    ap.add_argument("--judge-fraction", type=float, default=0.01)
     ap.add_argument("--nb", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--recall-sample", type=int, default=200)

@@ -133,7 +133,9 @@ struct hy_index {
     DevBuf w_x, w_lab, w_dist, w_keys, w_keys2, w_vals, w_vals2, w_sort, w_start, w_sums, w_cnt, w_rows, w_xn;
 
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[10] = {};  // 0-4: phases; 6-9: the batched scan launches
+    int kev = 0;              // batched scan launches timed by ev[6..9]
+    bool times_pending = false;  // a device-API search recorded events not yet read
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
 
@@ -433,7 +435,8 @@ bool learned_on(const hy_index* h) { return h->learned && h->model_ready; }
 // Chunk of queries whose probes (m x nprobe, best first) and their coarse
 // scores (h->m_pscore) are on the device: the probe network predicts each
 // query's nprobe and the probes beyond it become -1.
-int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s) {
+int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, int64_t* probes = nullptr) {
+    if (!probes) probes = h->w_probes.as<int64_t>();
     const int B = 8192;
     HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
     HY_RET(h->m_X.ensure((size_t)B * hy::MLP_IN * sizeof(float)));
@@ -447,7 +450,7 @@ int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s) {
                                           h->m_sd.as<float>(), h->m_X.as<float>(), s));
         HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), b, h->m_X.as<float>(), w, h->m_y.as<float>(), s));
         HY_CUDA(hy::launch_apply_nprobe(h->m_y.as<float>(), b, h->margin, (int)nprobe,
-                                        h->w_probes.as<int64_t>() + r0 * nprobe, h->m_total.as<unsigned long long>(),
+                                        probes + r0 * nprobe, h->m_total.as<unsigned long long>(),
                                         s));
         h->launches += 9;
     }
@@ -611,15 +614,22 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         // Pass 1: each query's nearest list under the warm-up threshold; the
         // threshold is then tightened to the k-th smallest candidate upper
         // bound; pass 2: the remaining probed lists under the tight threshold.
+        const bool last = timed && q0 + qc >= n;
         HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
                                          h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+        if (last) HY_CUDA(cudaEventRecord(h->ev[6], s));
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        if (last) HY_CUDA(cudaEventRecord(h->ev[7], s));
+        if (last) h->kev = 1;
         if (nprobe > 1) {
             HY_CUDA(hy::launch_tighten(h->norms.as<float>(), h->xaux.as<float2>(), h->b_qn.as<float4>(), (int)m, w,
                                        (int)capq, (int)k, h->metric, (int)h->d, h->b_thr.as<float>(), s));
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
                                              (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+            if (last) HY_CUDA(cudaEventRecord(h->ev[8], s));
             HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+            if (last) HY_CUDA(cudaEventRecord(h->ev[9], s));
+            if (last) h->kev = 2;
         }
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[3], s));
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
@@ -629,6 +639,32 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         h->launches += nprobe > 1 ? 22 : 14;
     }
     return HY_OK;
+}
+
+// Device times of the phases and of the scan kernel's launches, from the
+// events the last timed search recorded (they must have completed).
+void collect_times(hy_index* h) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    h->stats.coarse_ms = ms;
+    cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+    h->stats.scan_ms = ms;
+    cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
+    h->stats.merge_ms = ms;
+    if (h->kev > 0) {
+        double km = 0.0;
+        for (int i = 0; i < h->kev; ++i) {
+            cudaEventElapsedTime(&ms, h->ev[6 + 2 * i], h->ev[7 + 2 * i]);
+            km += ms;
+        }
+        h->stats.kernel_ms = km;
+        h->stats.kernel_launches = (uint64_t)h->kev;
+    } else {
+        h->stats.kernel_ms = h->stats.scan_ms;
+        h->stats.kernel_launches = 1;
+    }
+    h->kev = 0;
+    h->times_pending = false;
 }
 
 int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t nprobe) {
@@ -647,15 +683,8 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
     h->stats.tile_blocks_max = c[1];
     h->stats.launches = h->launches;
     h->launches = 0;
-    if (timed) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
-        h->stats.coarse_ms = ms;
-        cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
-        h->stats.scan_ms = ms;
-        cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]);
-        h->stats.merge_ms = ms;
-    }
+    if (timed) collect_times(h);
+    h->kev = 0;
     return HY_OK;
 }
 
@@ -739,7 +768,7 @@ int hy_index_create(size_t d, size_t nlist, size_t nprobe, int metric, int opt_l
     int rc = set_device(h);
     if (rc == HY_OK) {
         e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-        for (int i = 0; e == cudaSuccess && i < 6; ++i) e = cudaEventCreate(&h->ev[i]);
+        for (int i = 0; e == cudaSuccess && i < 10; ++i) e = cudaEventCreate(&h->ev[i]);
         if (e != cudaSuccess) rc = fail(HY_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
     }
     if (rc == HY_OK) rc = ensure_common(h);
@@ -880,8 +909,10 @@ int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, flo
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     HY_RET(ensure_common(h));
     h->launches = 0;
-    HY_RET(search_device_impl(h, n, dq, k, dD, dI, s, false));
+    HY_RET(search_device_impl(h, n, dq, k, dD, dI, s, true));
     h->stats.launches = h->launches;
+    h->stats.nq = n;
+    h->times_pending = true;
     return HY_OK;
 }
 
@@ -1246,13 +1277,19 @@ int hy_index_probes(hy_index* h, size_t n, const float* q, int64_t* probes) {
     HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
     HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
     HY_RET(h->w_probes.ensure(n * nprobe * sizeof(int64_t)));
+    if (learned_on(h)) {
+        HY_RET(h->m_pscore.ensure(qc * nprobe * sizeof(float)));
+        HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
+    }
     HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         HY_CUDA(hy::launch_coarse_scores(h->w_q.as<float>() + q0 * h->d, (int)m, h->cent.as<float>(), (int)h->nlist,
                                          (int)h->d, h->metric, h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
-                                  h->w_probes.as<int64_t>() + q0 * nprobe, nullptr, s));
+                                  h->w_probes.as<int64_t>() + q0 * nprobe,
+                                  learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s, h->w_probes.as<int64_t>() + q0 * nprobe));
     }
     HY_CUDA(cudaMemcpyAsync(probes, h->w_probes.p, n * nprobe * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
@@ -1295,8 +1332,17 @@ int hy_index_warmup_tops(hy_index* h, size_t n, const float* q, size_t k, size_t
     return HY_OK;
 }
 
-int hy_index_last_stats(const hy_index* h, hy_search_stats_t* out) {
-    HY_CHECK(h && out, HY_ERR_ARG, "last_stats: NULL argument");
+int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
+    HY_CHECK(hc && out, HY_ERR_ARG, "last_stats: NULL argument");
+    hy_index* h = const_cast<hy_index*>(hc);
+    if (h->times_pending) {
+        // The device-API search returns before its kernels finish; its
+        // device times are read here, once its last event has completed.
+        std::lock_guard<std::mutex> g(h->mu);
+        HY_RET(set_device(h));
+        HY_CUDA(cudaEventSynchronize(h->ev[4]));
+        collect_times(h);
+    }
     *out = h->stats;
     return HY_OK;
 }

@@ -53,8 +53,10 @@ def gmm_float(n, nq, d=128, ncomp=100, lo=0.0, hi=100.0, sigma=8.0, seed=0):
     return x, q
 
 
-def gmm_uint8(n, nq, d=128, ncomp=4096, sigma=20.0, seed=0, zipf=None):
-    """Integer-valued mixture in [0,255] (configs c2 and, with zipf, c4)."""
+def gmm_uint8(n, nq, d=128, ncomp=4096, sigma=20.0, seed=0, zipf=None, query_seed=None):
+    """Integer-valued mixture in [0,255] (configs c2 and, with zipf, c4).
+    With query_seed the queries are drawn from the same mixture by their own
+    generator (other query sets over the same base; n may then be 0)."""
     rng = np.random.default_rng(seed)
     centres = rng.uniform(0.0, 255.0, size=(ncomp, d)).astype(np.float32)
     w = None
@@ -63,7 +65,7 @@ def gmm_uint8(n, nq, d=128, ncomp=4096, sigma=20.0, seed=0, zipf=None):
         w /= w.sum()
     x = _mixture(rng, n, centres, sigma, w)
     np.clip(np.rint(x, out=x), 0, 255, out=x)
-    q = _mixture(rng, nq, centres, sigma, w)
+    q = _mixture(rng if query_seed is None else np.random.default_rng(query_seed), nq, centres, sigma, w)
     np.clip(np.rint(q, out=q), 0, 255, out=q)
     return x, q
 

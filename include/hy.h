@@ -90,6 +90,9 @@ typedef struct {
     double mean_nprobe;       /* lists probed per query (learned: the predicted mean) */
     double judge_recall;      /* learned: recall@10 of the judged sample vs fixed nprobe (-1: not judged) */
     uint64_t learned_fallback; /* learned: 1 when the batch was searched again with fixed nprobe */
+    double kernel_ms;         /* device time of the scan kernel's launches (plain: scan_plain_kernel;
+                                 bf16: batched_scan_kernel, both passes) in the last query chunk */
+    uint64_t kernel_launches; /* launches kernel_ms covers */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -163,7 +166,9 @@ HY_API int hy_index_search_preassigned(hy_index* h, size_t n, const float* q, si
                                        const int64_t* probes, float* D, int64_t* I);
 
 /* Coarse quantisation only: the nprobe nearest lists of each query, best
- * first (Index::findNearNprobeOfCentroidIds, src/Index.cpp:899-998). */
+ * first (Index::findNearNprobeOfCentroidIds, src/Index.cpp:899-998).  With
+ * the learned predictor on, the lists beyond each query's predicted nprobe
+ * are -1, exactly as the search uses them. */
 HY_API int hy_index_probes(hy_index* h, size_t n, const float* q, int64_t* probes);
 
 /* Warm-up thresholds only (src/Index.cpp:999-1051 and 1300-1303): for each
