@@ -36,6 +36,19 @@ sys.path.insert(0, ROOT)
 METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan HBM %"
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from ncu
+# captures of this script (dram__bytes_read.sum + dram__bytes_write.sum; the
+# capture commands are listed in profiles/), keyed by (form, nb, nq, nprobe).
+# The plain entry is a 1,000-query capture scaled by 10 to the 10,000-query
+# launch (traffic grows with the query count: every query streams its own
+# probed lists).
+KNOWN_TRAFFIC = {
+    ("plain", 1_000_000, 10_000, 64): 218_703_690_000,
+    ("learned", 1_000_000, 10_000, 64): 250_758_000,
+    ("bf16", 1_000_000, 10_000, 64): 279_463_000,
+}
+
+
 def peaks():
     """(HBM GB/s, dense bf16 TFLOP/s burst, which) from MEASURED_PEAKS.json,
     else the pool's earlier fallback measurement."""
@@ -287,18 +300,35 @@ def run_ours(args, rank, world, dist):
         alg = rows_main * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
         ach = alg / (kern_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "kernel": "scan_plain_kernel", "kernel_ms": round(kern_ms, 4), "algorithmic_bytes": alg}
+                "frac": round(ach / hbm_peak, 4), "traffic": KNOWN_TRAFFIC.get(("plain", args.nb, args.nq,
+                                                                               args.nprobe)),
+                "peak_kind": peak_kind, "kernel": "scan_plain_kernel", "kernel_ms": round(kern_ms, 4),
+                "algorithmic_bytes": alg}
     else:
-        # Algorithmic work of one batched-scan launch: a 2d-flop inner product
-        # per (query, probed row) pair on the bf16 tensor cores; the two
-        # passes of a search together cover all pairs once.
-        alg = rows_main * 2 * d / kern_per_search
-        ach = alg / (kern_ms / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": tc_peak, "unit": "TFLOP/s",
-                "frac": round(ach / tc_peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "kernel": "batched_scan_kernel", "kernel_ms": round(kern_ms, 4),
-                "algorithmic_flops": int(alg), "launches_per_search": kern_per_search}
+        # One batched-scan launch does a 2d-flop bf16 inner product per
+        # (query, probed row) pair of its pass and reads each list that some
+        # query probes in that pass once, as bf16 rows (d x 2 bytes).  The
+        # bound is whichever of the two takes longer at the measured peaks.
+        flops = rows_main * 2 * d / kern_per_search
+        distinct = 0
+        for j0, j1 in ((0, 1), (1, P_main.shape[1])):
+            cols = P_main[:, j0:j1]
+            used = np.unique(cols[cols >= 0])
+            distinct += int(sizes[used].sum())
+        lbytes = distinct * d * 2 / kern_per_search
+        t_tc, t_hbm = flops / (tc_peak * 1e12), lbytes / (hbm_peak * 1e9)
+        if t_tc >= t_hbm:
+            ach = flops / (kern_ms / 1e3) / 1e12
+            roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": tc_peak, "unit": "TFLOP/s",
+                    "frac": round(ach / tc_peak, 4)}
+        else:
+            ach = lbytes / (kern_ms / 1e3) / 1e9
+            roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
+                    "frac": round(ach / hbm_peak, 4)}
+        roof.update({"traffic": KNOWN_TRAFFIC.get((args.form, args.nb, args.nq, args.nprobe)),
+                     "peak_kind": peak_kind, "kernel": "batched_scan_kernel", "kernel_ms": round(kern_ms, 4),
+                     "algorithmic_flops": int(flops), "algorithmic_bytes": int(lbytes),
+                     "launches_per_search": kern_per_search})
 
     recall10, ns = _recall10(x, q, I_main, args.recall_sample)
     plain_line = None
@@ -316,6 +346,7 @@ def run_ours(args, rank, world, dist):
                       "nprobe": args.nprobe, "speedup_of_headline": round(value / pv, 2),
                       "roofline": {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
                                    "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
+                                   "traffic": KNOWN_TRAFFIC.get(("plain", args.nb, args.nq, args.nprobe)),
                                    "kernel": "scan_plain_kernel", "kernel_ms": round(plain["kernel_ms"], 4),
                                    "algorithmic_bytes": palg},
                       "clocks": plain["clocks"]}
