@@ -33,7 +33,7 @@ class SearchStats(C.Structure):
                 ("tile_blocks_max", C.c_uint64), ("coarse_ms", C.c_double), ("scan_ms", C.c_double),
                 ("merge_ms", C.c_double), ("launches", C.c_uint64), ("fallback_queries", C.c_uint64),
                 ("mean_nprobe", C.c_double), ("judge_recall", C.c_double), ("learned_fallback", C.c_uint64),
-                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64)]
+                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("unresolved_queries", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -87,6 +87,8 @@ def load():
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
     L.hy_index_search_preassigned_noalloc.argtypes = [H, sz, vp, sz, sz, vp, vp, vp, vp]
+    L.hy_index_search_nprobes.argtypes = [H, sz, vp, sz, vp, vp, vp]
+    L.hy_index_search_nprobes_device.argtypes = [H, sz, vp, sz, vp, sz, vp, vp, vp]
     L.hy_index_train_probe_model.argtypes = [H, sz, vp, sz, sz, i, C.c_float, C.c_float, vp]
     L.hy_index_set_learned.argtypes = [H, i, C.c_float, C.c_float]
     L.hy_probe_model_size.restype = sz

@@ -792,6 +792,38 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
     }
 }
 
+// Device-side fallback: gather / scatter of the overflowed queries.
+__global__ void fb_gather_kernel(const int32_t* __restrict__ ovf, const float* __restrict__ q,
+                                 const int64_t* __restrict__ probes, int nprobe, int d, int cap, float* __restrict__ fq,
+                                 int64_t* __restrict__ fprobes, int32_t* __restrict__ fcount) {
+    const int cnt = min(ovf[0], cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *fcount = cnt;
+    for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
+        const int qi = ovf[1 + i];
+        for (int j = threadIdx.x; j < d; j += blockDim.x) fq[static_cast<size_t>(i) * d + j] = q[static_cast<size_t>(qi) * d + j];
+        for (int j = threadIdx.x; j < nprobe; j += blockDim.x)
+            fprobes[static_cast<size_t>(i) * nprobe + j] = probes[static_cast<size_t>(qi) * nprobe + j];
+    }
+}
+
+__global__ void fb_scatter_kernel(const int32_t* __restrict__ ovf, const float* __restrict__ fD,
+                                  const int64_t* __restrict__ fI, int k, int cap, float* __restrict__ D,
+                                  int64_t* __restrict__ I, unsigned long long* total, unsigned long long* unresolved) {
+    const int all = ovf[0];
+    const int cnt = min(all, cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(total, static_cast<unsigned long long>(cnt));
+        if (all > cnt) atomicAdd(unresolved, static_cast<unsigned long long>(all - cnt));
+    }
+    for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
+        const int qi = ovf[1 + i];
+        for (int j = threadIdx.x; j < k; j += blockDim.x) {
+            D[static_cast<size_t>(qi) * k + j] = fD[static_cast<size_t>(i) * k + j];
+            I[static_cast<size_t>(qi) * k + j] = fI[static_cast<size_t>(i) * k + j];
+        }
+    }
+}
+
 __global__ void fill_f32_kernel(float* p, int64_t n, float v) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -832,6 +864,18 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
     float cK, cN;
     err_consts(d, &cK, &cN);
     tighten_kernel<<<nq, 256, smem, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fb_gather(const int32_t* ovf, const float* q, const int64_t* probes, int nprobe, int d, int cap,
+                             float* fq, int64_t* fprobes, int32_t* fcount, cudaStream_t s) {
+    fb_gather_kernel<<<64, 128, 0, s>>>(ovf, q, probes, nprobe, d, cap, fq, fprobes, fcount);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fb_scatter(const int32_t* ovf, const float* fD, const int64_t* fI, int k, int cap, float* D,
+                              int64_t* I, unsigned long long* total, unsigned long long* unresolved, cudaStream_t s) {
+    fb_scatter_kernel<<<64, 128, 0, s>>>(ovf, fD, fI, k, cap, D, I, total, unresolved);
     return cudaGetLastError();
 }
 

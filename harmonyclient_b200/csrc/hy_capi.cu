@@ -135,6 +135,8 @@ struct hy_index {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[10] = {};  // 0-4: phases; 6-9: the batched scan launches
     int kev = 0;              // batched scan launches timed by ev[6..9]
+    const int32_t* q_nprobe = nullptr;  // per-query nprobe (device) during a search_nprobes call
+    DevBuf w_np;
     bool times_pending = false;  // a device-API search recorded events not yet read
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
@@ -150,6 +152,7 @@ struct hy_index {
     DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
+    DevBuf b_fq, b_fpr, b_fD, b_fI, b_fcnt, b_fbtot;  // device-side exact fallback
 
     // learned probe predictor
     bool model_ready = false;
@@ -370,11 +373,16 @@ int check_search_args(hy_index* h, size_t n, size_t k) {
     return HY_OK;
 }
 
+// Overflowed queries per chunk that the bf16 form answers again on the
+// device with the plain scan (more fall back to a plain search of the batch
+// in the host-pointer API).
+constexpr size_t FB_CAP = 296;
+
 // Search n device queries with device probe lists (nprobe per query) into
 // device D/I.  Runs on stream s; does not synchronise.
 int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe, const int64_t* dprobes,
                    const uint32_t* init_thr, float* dD, int64_t* dI, cudaStream_t s, bool timed,
-                   int64_t* drows = nullptr) {
+                   int64_t* drows = nullptr, const int32_t* nq_dev = nullptr) {
     const int kp = k <= 32 ? 32 : k <= 64 ? 64 : k <= 128 ? 128 : 256;
     int nsplit = 1;
     const size_t target_ctas = 2 * 148;
@@ -408,6 +416,7 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
     p.k = (int)k;
     p.metric = h->metric;
     p.prune = 1;
+    p.nq_dev = nq_dev;
     if (timed) HY_CUDA(cudaEventRecord(h->ev[2], s));
     h->launches += 2 + (nsplit > 1 ? 1 : 0);
     int smem = 0;
@@ -416,7 +425,7 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
         return fail(HY_ERR_CUDA, std::string("scan launch (") + std::to_string(smem) + " B shared): " + cudaGetErrorString(e));
     if (timed) HY_CUDA(cudaEventRecord(h->ev[3], s));
     HY_CUDA(hy::launch_merge(h->w_parts.as<uint64_t>(), (int)n, nsplit, kp, (int)k, h->metric, h->ids.as<int64_t>(),
-                             dD, dI, s, drows));
+                             dD, dI, s, drows, nq_dev));
     if (timed) HY_CUDA(cudaEventRecord(h->ev[4], s));
     return HY_OK;
 }
@@ -482,6 +491,10 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
                                   h->w_probes.as<int64_t>(), learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
         h->launches += 2;
         if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
+        if (h->q_nprobe) {
+            HY_CUDA(hy::launch_cut_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, h->q_nprobe + q0, s));
+            h->launches += 1;
+        }
         const uint32_t* thr = nullptr;
         if (warm) {
             h->launches += 1;
@@ -546,8 +559,17 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_work.ensure(sizeof(unsigned int)));
     HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
-    HY_RET(h->b_ovf.ensure((n + 1) * sizeof(int32_t)));
-    HY_CUDA(cudaMemsetAsync(h->b_ovf.p, 0, sizeof(int32_t), s));
+    HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
+    // Exact fallback on the device: up to FB_CAP overflowed queries per chunk
+    // are searched again by the plain scan over the same probe lists.
+    const size_t fbcap = std::min<size_t>(qc, FB_CAP);
+    HY_RET(h->b_fq.ensure(fbcap * h->d * sizeof(float)));
+    HY_RET(h->b_fpr.ensure(fbcap * nprobe * sizeof(int64_t)));
+    HY_RET(h->b_fD.ensure(fbcap * k * sizeof(float)));
+    HY_RET(h->b_fI.ensure(fbcap * k * sizeof(int64_t)));
+    HY_RET(h->b_fcnt.ensure(sizeof(int32_t)));
+    HY_RET(h->b_fbtot.ensure(2 * sizeof(unsigned long long)));
+    HY_CUDA(cudaMemsetAsync(h->b_fbtot.p, 0, 2 * sizeof(unsigned long long), s));
     // Warm-up for the bf16 form: its threshold only bounds the first pass
     // (each query's nearest list), so three lists suffice by default.
     const size_t wl = h->warmup_list ? std::min<size_t>(h->warmup_list, 3) : 3;
@@ -576,13 +598,18 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
-        w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then global query ids
+        w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then chunk-local query ids
+        HY_CUDA(cudaMemsetAsync(w.overflow, 0, sizeof(int32_t), s));
         if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[0], s));
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
                                   learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
         if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
+        if (h->q_nprobe) {
+            HY_CUDA(hy::launch_cut_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, h->q_nprobe + q0, s));
+            h->launches += 1;
+        }
         if (h->metric == HY_METRIC_L2) {
             HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
                                       qq, (int)m, h->w_probes.as<int64_t>(), (int)nprobe, (int)k, (int)wl, (int)wls, 1,
@@ -633,9 +660,18 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         }
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[3], s));
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
-                                  h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, (int)q0, (int)capq, (int)k,
+                                  h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, 0, (int)capq, (int)k,
                                   h->metric, dD + q0 * k, dI + q0 * k, s));
         if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[4], s));
+        const int fb = (int)std::min<size_t>(m, fbcap);
+        HY_CUDA(hy::launch_fb_gather(w.overflow, qq, h->w_probes.as<int64_t>(), (int)nprobe, (int)h->d, fb,
+                                     h->b_fq.as<float>(), h->b_fpr.as<int64_t>(), h->b_fcnt.as<int32_t>(), s));
+        HY_RET(scan_and_merge(h, (size_t)fb, h->b_fq.as<float>(), k, nprobe, h->b_fpr.as<int64_t>(), nullptr,
+                              h->b_fD.as<float>(), h->b_fI.as<int64_t>(), s, false, nullptr, h->b_fcnt.as<int32_t>()));
+        HY_CUDA(hy::launch_fb_scatter(w.overflow, h->b_fD.as<float>(), h->b_fI.as<int64_t>(), (int)k, fb, dD + q0 * k,
+                                      dI + q0 * k, h->b_fbtot.as<unsigned long long>(),
+                                      h->b_fbtot.as<unsigned long long>() + 1, s));
+        h->launches += 5;
         h->launches += nprobe > 1 ? 22 : 14;
     }
     return HY_OK;
@@ -697,37 +733,25 @@ int reset_counters(hy_index* h, cudaStream_t s) {
     return HY_OK;
 }
 
-// Queries whose bf16 candidate buffers overflowed are answered again with the
-// plain FP32 scan (the exact fallback) and their rows patched into D / I.
-int bf16_fallback(hy_index* h, const float* q, size_t n, size_t k, float* D, int64_t* I, cudaStream_t s) {
-    int32_t cnt = 0;
-    HY_CUDA(cudaMemcpy(&cnt, h->b_ovf.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    h->stats.rows = 0;
-    if (cnt <= 0) return HY_OK;
-    std::vector<int32_t> qids(cnt);
-    HY_CUDA(cudaMemcpy(qids.data(), h->b_ovf.as<int32_t>() + 1, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    std::vector<float> sub((size_t)cnt * h->d);
-    for (int i = 0; i < cnt; ++i) std::memcpy(&sub[(size_t)i * h->d], q + (size_t)qids[i] * h->d, h->d * sizeof(float));
-    HY_RET(h->w_q.ensure(sub.size() * sizeof(float)));
-    HY_RET(h->w_D.ensure((size_t)cnt * k * sizeof(float)));
-    HY_RET(h->w_I.ensure((size_t)cnt * k * sizeof(int64_t)));
-    HY_CUDA(cudaMemcpyAsync(h->w_q.p, sub.data(), sub.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+// Fallback accounting of a bf16 host-pointer search.  Overflowed queries were
+// answered again on the device by the plain scan (up to FB_CAP per chunk);
+// if more overflowed in some chunk, the whole batch is searched again here
+// with the plain form (its queries are still in h->w_q).
+int bf16_fallback(hy_index* h, size_t n, size_t k, float* D, int64_t* I, cudaStream_t s) {
+    unsigned long long c[2] = {0, 0};
+    HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
+    h->stats.fallback_queries = c[0];
+    h->stats.unresolved_queries = 0;
+    if (c[1] == 0) return HY_OK;
     const int form = h->form;
     h->form = HY_FORM_PLAIN;
-    const int rc = search_device_impl(h, (size_t)cnt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s,
-                                      false);
+    const int rc = search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, false);
     h->form = form;
     HY_RET(rc);
-    std::vector<float> d2((size_t)cnt * k);
-    std::vector<int64_t> i2((size_t)cnt * k);
-    HY_CUDA(cudaMemcpyAsync(d2.data(), h->w_D.p, d2.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
-    HY_CUDA(cudaMemcpyAsync(i2.data(), h->w_I.p, i2.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < cnt; ++i) {
-        std::memcpy(D + (size_t)qids[i] * k, &d2[(size_t)i * k], k * sizeof(float));
-        std::memcpy(I + (size_t)qids[i] * k, &i2[(size_t)i * k], k * sizeof(int64_t));
-    }
-    h->stats.fallback_queries = (uint64_t)cnt;
+    h->stats.fallback_queries = n;
     return HY_OK;
 }
 
@@ -872,7 +896,7 @@ int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
 int hy_index_set_form(hy_index* h, int form) {
     HY_CHECK(h, HY_ERR_ARG, "set_form: NULL handle");
     HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16, HY_ERR_ARG, "set_form: unknown form");
-    HY_CHECK(form != HY_FORM_BF16 || h->d <= 192, HY_ERR_ARG, "set_form: the bf16 form supports d <= 192");
+    HY_CHECK(form != HY_FORM_BF16 || h->d <= 128, HY_ERR_ARG, "set_form: the bf16 form supports d <= 128");
     h->form = form;
     return HY_OK;
 }
@@ -942,7 +966,7 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     }
     if (h->form == HY_FORM_BF16 && h->arena_rows > 0) {
         const hy_search_stats_t keep = h->stats;
-        HY_RET(bf16_fallback(h, q, n, k, D, I, s));
+        HY_RET(bf16_fallback(h, n, k, D, I, s));
         const uint64_t fb = h->stats.fallback_queries;
         h->stats = keep;
         h->stats.fallback_queries = fb;
@@ -1046,6 +1070,60 @@ int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, i
     h->stats.judge_recall = -1.0;
     h->stats.learned_fallback = 0;
     if (learned_on(h) && h->judge_fraction > 0) HY_RET(judge_learned(h, n, q, k, D, I));
+    return HY_OK;
+}
+
+int hy_index_search_nprobes(hy_index* h, size_t n, const float* q, size_t k, const int32_t* nprobes, float* D,
+                            int64_t* I) {
+    HY_CHECK(h && (n == 0 || (q && nprobes && D && I)), HY_ERR_ARG, "search_nprobes: NULL argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    int32_t mx = 0;
+    double sum = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        HY_CHECK(nprobes[i] >= 1, HY_ERR_ARG, "search_nprobes: every nprobe must be >= 1");
+        const int32_t c = (int32_t)std::min<size_t>((size_t)nprobes[i], h->nlist);
+        mx = std::max(mx, c);
+        sum += c;
+    }
+    HY_RET(set_device(h));
+    HY_RET(h->w_np.ensure(n * sizeof(int32_t)));
+    HY_CUDA(cudaMemcpy(h->w_np.p, nprobes, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    const size_t keep = h->nprobe;
+    h->nprobe = (size_t)mx;
+    h->q_nprobe = h->w_np.as<int32_t>();
+    const int rc = search_host(h, n, q, k, D, I);
+    h->q_nprobe = nullptr;
+    h->nprobe = keep;
+    HY_RET(rc);
+    if (!learned_on(h)) h->stats.mean_nprobe = sum / (double)n;
+    h->stats.judge_recall = -1.0;
+    h->stats.learned_fallback = 0;
+    return HY_OK;
+}
+
+int hy_index_search_nprobes_device(hy_index* h, size_t n, const float* dq, size_t k, const int32_t* dnprobes,
+                                   size_t max_nprobe, float* dD, int64_t* dI, void* stream) {
+    HY_CHECK(h && (n == 0 || (dq && dnprobes && dD && dI)), HY_ERR_ARG, "search_nprobes: NULL argument");
+    HY_CHECK(max_nprobe >= 1, HY_ERR_ARG, "search_nprobes: max_nprobe must be >= 1");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (n == 0) return HY_OK;
+    HY_RET(check_search_args(h, n, k));
+    HY_RET(set_device(h));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HY_RET(ensure_common(h));
+    h->launches = 0;
+    const size_t keep = h->nprobe;
+    h->nprobe = std::min(max_nprobe, h->nlist);
+    h->q_nprobe = dnprobes;
+    const int rc = search_device_impl(h, n, dq, k, dD, dI, s, true);
+    h->q_nprobe = nullptr;
+    h->nprobe = keep;
+    HY_RET(rc);
+    h->stats.launches = h->launches;
+    h->stats.nq = n;
+    h->times_pending = true;
     return HY_OK;
 }
 
@@ -1342,6 +1420,12 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
         HY_RET(set_device(h));
         HY_CUDA(cudaEventSynchronize(h->ev[4]));
         collect_times(h);
+        if (h->form == HY_FORM_BF16 && h->b_fbtot.p) {
+            unsigned long long c[2] = {0, 0};
+            HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
+            h->stats.fallback_queries = c[0];
+            h->stats.unresolved_queries = c[1];
+        }
     }
     *out = h->stats;
     return HY_OK;

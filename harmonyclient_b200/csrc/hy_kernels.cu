@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x / p.nsplit, split = blockIdx.x % p.nsplit;
+    if (p.nq_dev && qi >= *p.nq_dev) return;  // whole CTA, before any barrier
     const int npc = (p.nprobe - split + p.nsplit - 1) / p.nsplit;  // probes of this CTA
     const int npa = ((p.nprobe + p.nsplit - 1) / p.nsplit + 3) & ~3;  // table entries, padded for alignment
     const size_t slot_floats = static_cast<size_t>(32) * L.max_pitch;
@@ -560,10 +561,11 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
 __global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__ parts, int nparts, int kp, int k,
                                                     int metric, const int64_t* __restrict__ ids,
                                                     float* __restrict__ D, int64_t* __restrict__ I,
-                                                    int64_t* __restrict__ rows) {
+                                                    int64_t* __restrict__ rows, const int32_t* __restrict__ nq_dev) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t* a = reinterpret_cast<uint64_t*>(sm);
     const size_t qi = blockIdx.x;
+    if (nq_dev && static_cast<int>(qi) >= *nq_dev) return;
     const int n = nparts * kp;
     const uint64_t* src = parts + qi * n;
     const uint64_t* best = src;
@@ -802,14 +804,11 @@ cudaError_t launch_scan_plain(const ScanParams& p, int* smem_out, cudaStream_t s
 }
 
 cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int k, int metric, const int64_t* ids,
-                         float* D, int64_t* I, cudaStream_t s, int64_t* rows) {
+                         float* D, int64_t* I, cudaStream_t s, int64_t* rows, const int32_t* nq_dev) {
     const size_t smem = nparts > 1 ? static_cast<size_t>(next_pow2(nparts * kp)) * 8 : 0;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured = true;
-    }
-    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I, rows);
+    cudaError_t e = cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I, rows, nq_dev);
     return cudaGetLastError();
 }
 
@@ -930,6 +929,13 @@ __global__ void stop_labels_kernel(const int64_t* __restrict__ rows, int n, int 
     label[q] = static_cast<float>(worst + 1);
 }
 
+__global__ void cut_probes_kernel(int64_t* __restrict__ probes, int n, int P, const int32_t* __restrict__ np) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int c = max(1, min(P, np[q]));
+    for (int j = c; j < P; ++j) probes[static_cast<int64_t>(q) * P + j] = -1;
+}
+
 // Per-query nprobe = clamp(ceil(2^(y + margin)), 1, P); probes beyond it
 // become -1.  Adds the chosen counts to *total.
 __global__ void apply_nprobe_kernel(const float* __restrict__ y, int n, float margin, int P,
@@ -944,6 +950,11 @@ __global__ void apply_nprobe_kernel(const float* __restrict__ y, int n, float ma
 }
 
 }  // namespace
+
+cudaError_t launch_cut_probes(int64_t* probes, int n, int P, const int32_t* np, cudaStream_t s) {
+    cut_probes_kernel<<<grid_for(n, 128), 128, 0, s>>>(probes, n, P, np);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_probe_features(const float* scores, int n, int P, const float* mu, const float* sd, float* X,
                                   cudaStream_t s) {

@@ -49,6 +49,7 @@ struct ScanParams {
     unsigned long long* counters;  // [2]: tile blocks loaded, tile blocks possible
     int* err;
     int nq, nprobe, nsplit, k, metric, prune;
+    const int32_t* nq_dev = nullptr;  // optional device count: queries at or past it are skipped
 };
 
 cudaError_t launch_coarse_scores(const float* q, int nq, const float* cent, int nlist, int d, int metric, float* out,
@@ -62,8 +63,13 @@ cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_
                           int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s);
 cudaError_t launch_scan_plain(const ScanParams& p, int* smem_bytes_out, cudaStream_t s);
 // rows (optional): the arena row of every result (-1 when unfilled).
+// nq_dev (optional): device count; queries at or past it are skipped.
 cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int k, int metric, const int64_t* ids,
-                         float* D, int64_t* I, cudaStream_t s, int64_t* rows = nullptr);
+                         float* D, int64_t* I, cudaStream_t s, int64_t* rows = nullptr,
+                         const int32_t* nq_dev = nullptr);
+
+// Per-query nprobe: probes at or beyond np[q] (clamped to [1, P]) become -1.
+cudaError_t launch_cut_probes(int64_t* probes, int n, int P, const int32_t* np, cudaStream_t s);
 
 // Learned probe predictor helpers (see hy_kernels.cu).
 cudaError_t launch_probe_features(const float* scores, int n, int P, const float* mu, const float* sd, float* X,

@@ -136,6 +136,22 @@ class Index:
         check(self._L.hy_index_search(self._h, n, _p(q), int(k), _p(D), _p(I)))
         return D, I
 
+    def search_nprobes(self, queries, k, nprobes):
+        """Search with a per-query nprobe (int array, one per query)."""
+        q = _f32(queries, self.d)
+        npq = np.ascontiguousarray(nprobes, dtype=np.int32)
+        if npq.shape != (q.shape[0],):
+            raise ValueError("nprobes must hold one value per query")
+        D = np.empty((q.shape[0], k), np.float32)
+        I = np.empty((q.shape[0], k), np.int64)
+        check(self._L.hy_index_search_nprobes(self._h, q.shape[0], _p(q), int(k), _p(npq), _p(D), _p(I)))
+        return D, I
+
+    def search_nprobes_device(self, n, q_ptr, k, nprobes_ptr, max_nprobe, d_ptr, i_ptr, stream=0):
+        check(self._L.hy_index_search_nprobes_device(self._h, int(n), C.c_void_p(q_ptr), int(k),
+                                                     C.c_void_p(nprobes_ptr), int(max_nprobe), C.c_void_p(d_ptr),
+                                                     C.c_void_p(i_ptr), C.c_void_p(stream)))
+
     def search_preassigned(self, queries, k, probes):
         q = _f32(queries, self.d)
         P = np.ascontiguousarray(probes, np.int64)

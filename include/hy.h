@@ -93,6 +93,9 @@ typedef struct {
     double kernel_ms;         /* device time of the scan kernel's launches (plain: scan_plain_kernel;
                                  bf16: batched_scan_kernel, both passes) in the last query chunk */
     uint64_t kernel_launches; /* launches kernel_ms covers */
+    uint64_t unresolved_queries; /* bf16 device-pointer search: overflowed queries beyond the device
+                                    fallback's capacity (296 per chunk), left with the bf16 re-rank's
+                                    answer; the host-pointer search re-runs such batches exactly */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -129,11 +132,12 @@ HY_API int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* str
 HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
 
 /* Scan form (no counterpart in the reference, whose only scan is the exact
- * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16 (d <= 192).  The bf16 form batches queries
- * per list on the tensor cores and re-ranks candidates with exact FP32
- * distances; on integer-valued data below 256 its results equal the plain
- * form's.  Queries whose candidates overflow are answered by the plain form
- * (host-pointer search only). */
+ * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16 (d <= 128).  The bf16 form batches
+ * queries per list on the tensor cores and re-ranks candidates with exact FP32
+ * distances chosen by rigorous error bounds, so its results equal the plain
+ * form's.  Queries whose candidates overflow their buffers are answered again
+ * by the plain scan on the device (up to 296 per chunk of queries; the
+ * host-pointer search re-runs a batch with more in the plain form). */
 HY_API int hy_index_set_form(hy_index* h, int form);
 
 /* bf16 form parameters (0 keeps the current value): candidate slots per
@@ -157,6 +161,15 @@ HY_API int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_lis
 HY_API int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I);
 HY_API int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI,
                                   void* stream);
+
+/* Search with a per-query nprobe (no counterpart in the reference, whose
+ * nprobe is one value per call): query i probes its nprobes[i] nearest lists
+ * (clamped to nlist).  The device variant takes the per-query values on the
+ * device and their maximum from the caller. */
+HY_API int hy_index_search_nprobes(hy_index* h, size_t n, const float* q, size_t k, const int32_t* nprobes, float* D,
+                                   int64_t* I);
+HY_API int hy_index_search_nprobes_device(hy_index* h, size_t n, const float* dq, size_t k, const int32_t* dnprobes,
+                                          size_t max_nprobe, float* dD, int64_t* dI, void* stream);
 
 /* Search with caller-given probe lists (n x nprobe list ids, best first; -1
  * entries are skipped).  This is the list-scan half of the search
