@@ -141,22 +141,21 @@ def cpu_baseline_ref(x, q, cent, nprobe, k, budget_s):
             "sample": f"{m2} of {q.shape[0]} queries, reference Index::search ORIGINAL mode, OpenMP x{nt}"}
 
 
-def _time_device(idx, dq, dD, dI, k, steps, stream, dist, dev):
+def _time_device(idx, dq, dD, dI, k, steps, ts, dist, dev):
     """Device-timed loop of `steps` batch searches (CUDA events on the
-    launching stream, max over ranks); the last step's stats come back."""
+    launching stream `ts`, max over ranks); the last step's stats come back."""
     import torch
     n = dq.shape[0]
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
     with Clocks(dev) as clk:
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("timed")  # profilers select the timed launches by this range
-        e0.record()
+        e0.record(ts)
         for _ in range(steps):
-            idx.search_device(n, dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
-        e1.record()
+            idx.search_device(n, dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), ts.cuda_stream)
+        e1.record(ts)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
     st = idx.last_stats()
@@ -167,14 +166,14 @@ def _time_device(idx, dq, dD, dI, k, steps, stream, dist, dev):
     return float(t.item()), st, clk.summary()
 
 
-def _kernel_ms(idx, dq, dD, dI, k, reps, stream):
+def _kernel_ms(idx, dq, dD, dI, k, reps, ts):
     """Average duration of the dominant scan kernel's launches: every
     launch is bracketed by CUDA events on its own stream inside the library;
     `reps` further searches, each read back."""
     import torch
     tot, launches = 0.0, 0
     for _ in range(reps):
-        idx.search_device(dq.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        idx.search_device(dq.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), ts.cuda_stream)
         st = idx.last_stats()
         tot += st["kernel_ms"]
         launches += st["kernel_launches"]
@@ -221,13 +220,18 @@ def run_ours(args, rank, world, dist):
         train_s = time.perf_counter() - t0
         idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
     idx.set_form("plain" if args.form == "plain" else "bf16")
+    tune = None
+    if args.form != "plain" and args.autotune:
+        # Work shape picked on this batch (every shape gives the same answer).
+        tune = idx.autotune(q, k, reps=2)
 
-    stream = torch.cuda.current_stream().cuda_stream
+    stream = torch.cuda.Stream()  # the launching stream of every timed search
     dq = torch.from_numpy(q).cuda()
     dD = torch.empty((q.shape[0], k), dtype=torch.float32, device="cuda")
     dI = torch.empty((q.shape[0], k), dtype=torch.int64, device="cuda")
+    idx.set_graph(args.graph)
     for _ in range(args.warmup):
-        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     ms_max, st_dev, clocks = _time_device(idx, dq, dD, dI, k, args.steps, stream, dist, dev)
     value = world * q.shape[0] * args.steps / (ms_max / 1e3)
@@ -275,7 +279,7 @@ def run_ours(args, rank, world, dist):
         if learned:
             idx.set_learned(False)
         idx.set_form("plain")
-        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream)
+        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream.cuda_stream)
         pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev)
         pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream)
         plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "clocks": pclk}
@@ -381,6 +385,8 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(st_dev["launches"]) * args.steps,
+        "graph": {"enabled": bool(args.graph), "replayed": bool(st_dev["graph_replayed"])},
+        "work_shape": {**idx.batch_params(), "autotune": tune},
         "plain_fp32": plain_line,
         "warmup_list": args.warmup_list,
         "fallback_queries": fallback,
@@ -453,6 +459,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--coverage", type=float, default=0.97)
     ap.add_argument("--judge-fraction", type=float, default=0.01)
+    ap.add_argument("--no-graph", dest="graph", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--nb", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--recall-sample", type=int, default=200)

@@ -25,7 +25,8 @@ class HyError(RuntimeError):
 class IndexInfo(C.Structure):
     _fields_ = [("d", C.c_size_t), ("nlist", C.c_size_t), ("nprobe", C.c_size_t), ("metric", C.c_int),
                 ("opt_level", C.c_int), ("dim_blocks", C.c_size_t), ("ntotal", C.c_size_t),
-                ("arena_rows", C.c_size_t), ("trained", C.c_int), ("device", C.c_int)]
+                ("arena_rows", C.c_size_t), ("trained", C.c_int), ("device", C.c_int), ("form", C.c_int),
+                ("learned", C.c_int), ("capq", C.c_size_t), ("row_slice", C.c_size_t)]
 
 
 class SearchStats(C.Structure):
@@ -33,7 +34,8 @@ class SearchStats(C.Structure):
                 ("tile_blocks_max", C.c_uint64), ("coarse_ms", C.c_double), ("scan_ms", C.c_double),
                 ("merge_ms", C.c_double), ("launches", C.c_uint64), ("fallback_queries", C.c_uint64),
                 ("mean_nprobe", C.c_double), ("judge_recall", C.c_double), ("learned_fallback", C.c_uint64),
-                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("unresolved_queries", C.c_uint64)]
+                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("graph_replayed", C.c_uint64),
+                ("unresolved_queries", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -87,6 +89,8 @@ def load():
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
     L.hy_index_search_preassigned_noalloc.argtypes = [H, sz, vp, sz, sz, vp, vp, vp, vp]
+    L.hy_index_set_graph.argtypes = [H, i]
+    L.hy_index_autotune.argtypes = [H, sz, vp, sz, i, vp]
     L.hy_index_search_nprobes.argtypes = [H, sz, vp, sz, vp, vp, vp]
     L.hy_index_search_nprobes_device.argtypes = [H, sz, vp, sz, vp, sz, vp, vp, vp]
     L.hy_index_train_probe_model.argtypes = [H, sz, vp, sz, sz, i, C.c_float, C.c_float, vp]

@@ -63,6 +63,10 @@ struct Status {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
     int ensure(size_t n) {
         if (n <= bytes) return HY_OK;
         if (p) cudaFree(p);
@@ -133,10 +137,34 @@ struct hy_index {
     DevBuf w_x, w_lab, w_dist, w_keys, w_keys2, w_vals, w_vals2, w_sort, w_start, w_sums, w_cnt, w_rows, w_xn;
 
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[10] = {};  // 0-4: phases; 6-9: the batched scan launches
+    // Timing events (0-4: phases; 6-9: the batched scan launches).  A search
+    // captured in a graph records its own set: an event recorded during a
+    // capture cannot be waited on outside the graph.
+    cudaEvent_t ev_direct[10] = {};
+    cudaEvent_t ev_graph[10] = {};
+    cudaEvent_t* ev = ev_direct;
     int kev = 0;              // batched scan launches timed by ev[6..9]
     const int32_t* q_nprobe = nullptr;  // per-query nprobe (device) during a search_nprobes call
     DevBuf w_np;
+    // CUDA graph of the device-pointer search (graph mode): the captured
+    // launch sequence and the call it was captured for.
+    uint64_t epoch = 0;  // bumped by every call that changes what a search does
+    bool graph_on = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    struct GraphKey {
+        uint64_t epoch;
+        size_t n, k, nprobe;
+        const void *dq, *dD, *dI, *np;
+        cudaStream_t s;
+        bool operator==(const GraphKey& o) const {
+            return epoch == o.epoch && n == o.n && k == o.k && nprobe == o.nprobe && dq == o.dq && dD == o.dD &&
+                   dI == o.dI && np == o.np && s == o.s;
+        }
+    } gkey{};
+    uint64_t graph_kernels = 0;
+    int graph_kev = 0;
+    cudaEvent_t gev[2] = {};
     bool times_pending = false;  // a device-API search recorded events not yet read
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
@@ -165,6 +193,16 @@ struct hy_index {
 };
 
 namespace {
+
+// Timing events are recorded as external event nodes when the stream is
+// being captured, so a replayed graph records them too.
+inline cudaError_t ev_record(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    const cudaError_t ce = cudaStreamIsCapturing(s, &st);
+    if (ce != cudaSuccess) return ce;
+    return st == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, s);
+}
 
 int set_device(hy_index* h) {
     HY_CUDA(cudaSetDevice(h->device));
@@ -417,16 +455,16 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
     p.metric = h->metric;
     p.prune = 1;
     p.nq_dev = nq_dev;
-    if (timed) HY_CUDA(cudaEventRecord(h->ev[2], s));
+    if (timed) HY_CUDA(ev_record(h->ev[2], s));
     h->launches += 2 + (nsplit > 1 ? 1 : 0);
     int smem = 0;
     cudaError_t e = hy::launch_scan_plain(p, &smem, s);
     if (e != cudaSuccess)
         return fail(HY_ERR_CUDA, std::string("scan launch (") + std::to_string(smem) + " B shared): " + cudaGetErrorString(e));
-    if (timed) HY_CUDA(cudaEventRecord(h->ev[3], s));
+    if (timed) HY_CUDA(ev_record(h->ev[3], s));
     HY_CUDA(hy::launch_merge(h->w_parts.as<uint64_t>(), (int)n, nsplit, kp, (int)k, h->metric, h->ids.as<int64_t>(),
                              dD, dI, s, drows, nq_dev));
-    if (timed) HY_CUDA(cudaEventRecord(h->ev[4], s));
+    if (timed) HY_CUDA(ev_record(h->ev[4], s));
     return HY_OK;
 }
 
@@ -484,7 +522,7 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
-        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[0], s));
+        if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
@@ -506,7 +544,7 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
                                       (int)wls, 1, h->w_thr.as<uint32_t>(), nullptr, h->w_err.as<int>(), s));
             thr = h->w_thr.as<uint32_t>();
         }
-        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[1], s));
+        if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[1], s));
         HY_RET(scan_and_merge(h, m, qq, k, nprobe, h->w_probes.as<int64_t>(), thr, dD + q0 * k, dI + q0 * k, s,
                               timed && q0 + qc >= n));
     }
@@ -600,7 +638,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         const float* qq = dq + q0 * h->d;
         w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then chunk-local query ids
         HY_CUDA(cudaMemsetAsync(w.overflow, 0, sizeof(int32_t), s));
-        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[0], s));
+        if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
@@ -620,9 +658,9 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
             HY_CUDA(hy::launch_fill_f32(h->b_thr.as<float>(), (int64_t)m, INFINITY, s));
         }
         HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(), s));
-        if (timed && q0 == 0) HY_CUDA(cudaEventRecord(h->ev[1], s));
+        if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[1], s));
         HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
-        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[2], s));
+        if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[2], s));
         hy::BatchedLaunch b;
         b.abf = h->abf.p;
         b.list_off = h->list_off.as<int64_t>();
@@ -644,25 +682,25 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         const bool last = timed && q0 + qc >= n;
         HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
                                          h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
-        if (last) HY_CUDA(cudaEventRecord(h->ev[6], s));
+        if (last) HY_CUDA(ev_record(h->ev[6], s));
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
-        if (last) HY_CUDA(cudaEventRecord(h->ev[7], s));
+        if (last) HY_CUDA(ev_record(h->ev[7], s));
         if (last) h->kev = 1;
         if (nprobe > 1) {
             HY_CUDA(hy::launch_tighten(h->norms.as<float>(), h->xaux.as<float2>(), h->b_qn.as<float4>(), (int)m, w,
                                        (int)capq, (int)k, h->metric, (int)h->d, h->b_thr.as<float>(), s));
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
                                              (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
-            if (last) HY_CUDA(cudaEventRecord(h->ev[8], s));
+            if (last) HY_CUDA(ev_record(h->ev[8], s));
             HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
-            if (last) HY_CUDA(cudaEventRecord(h->ev[9], s));
+            if (last) HY_CUDA(ev_record(h->ev[9], s));
             if (last) h->kev = 2;
         }
-        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[3], s));
+        if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[3], s));
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
                                   h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, 0, (int)capq, (int)k,
                                   h->metric, dD + q0 * k, dI + q0 * k, s));
-        if (timed && q0 + qc >= n) HY_CUDA(cudaEventRecord(h->ev[4], s));
+        if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[4], s));
         const int fb = (int)std::min<size_t>(m, fbcap);
         HY_CUDA(hy::launch_fb_gather(w.overflow, qq, h->w_probes.as<int64_t>(), (int)nprobe, (int)h->d, fb,
                                      h->b_fq.as<float>(), h->b_fpr.as<int64_t>(), h->b_fcnt.as<int32_t>(), s));
@@ -733,6 +771,74 @@ int reset_counters(hy_index* h, cudaStream_t s) {
     return HY_OK;
 }
 
+void drop_graph(hy_index* h) {
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+}
+
+// The device-pointer search, through a CUDA graph in graph mode: the first
+// call with a new (buffers, sizes, stream, index state) runs normally (every
+// buffer reaches its size), then captures the same launch sequence; later
+// identical calls replay it with one cudaGraphLaunch.  The legacy default
+// stream cannot be captured: such calls run the graph on the handle's stream,
+// ordered after and before the default stream's work by events.
+int run_device_search(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s) {
+    h->stats.graph_replayed = 0;
+    h->ev = h->ev_direct;
+    if (!h->graph_on) return search_device_impl(h, n, dq, k, dD, dI, s, true);
+    const hy_index::GraphKey key{h->epoch, n, k, h->nprobe, dq, dD, dI, h->q_nprobe, s};
+    cudaStream_t run = s ? s : h->stream;
+    if (h->gexec && key == h->gkey) {
+        if (!s) {
+            HY_CUDA(cudaEventRecord(h->gev[0], nullptr));
+            HY_CUDA(cudaStreamWaitEvent(h->stream, h->gev[0], 0));
+        }
+        HY_CUDA(cudaGraphLaunch(h->gexec, run));
+        h->ev = h->ev_graph;  // the replay recorded the graph's timing events
+        if (!s) {
+            HY_CUDA(cudaEventRecord(h->gev[1], h->stream));
+            HY_CUDA(cudaStreamWaitEvent(nullptr, h->gev[1], 0));
+        }
+        h->launches = h->graph_kernels;
+        h->kev = h->graph_kev;
+        h->stats.graph_replayed = 1;
+        return HY_OK;
+    }
+    HY_RET(search_device_impl(h, n, dq, k, dD, dI, s, true));
+    const uint64_t launches = h->launches;
+    const int kev = h->kev;
+    drop_graph(h);
+    HY_CUDA(cudaStreamBeginCapture(run, cudaStreamCaptureModeThreadLocal));
+    h->launches = 0;
+    h->ev = h->ev_graph;
+    const int rc = search_device_impl(h, n, dq, k, dD, dI, run, true);
+    h->ev = h->ev_direct;  // this call's times come from the direct run
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(run, &g);
+    if (rc != HY_OK || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        h->launches = launches;
+        h->kev = kev;
+        if (rc != HY_OK) return rc;
+        return fail(HY_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        h->gexec = nullptr;
+        return fail(HY_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    h->graph = g;
+    h->gkey = key;
+    h->graph_kernels = h->launches;
+    h->graph_kev = h->kev;
+    h->launches = launches;
+    h->kev = kev;
+    return HY_OK;
+}
+
 // Fallback accounting of a bf16 host-pointer search.  Overflowed queries were
 // answered again on the device by the plain scan (up to FB_CAP per chunk);
 // if more overflowed in some chunk, the whole batch is searched again here
@@ -792,7 +898,8 @@ int hy_index_create(size_t d, size_t nlist, size_t nprobe, int metric, int opt_l
     int rc = set_device(h);
     if (rc == HY_OK) {
         e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-        for (int i = 0; e == cudaSuccess && i < 10; ++i) e = cudaEventCreate(&h->ev[i]);
+        for (int i = 0; e == cudaSuccess && i < 10; ++i) e = cudaEventCreate(&h->ev_direct[i]);
+        for (int i = 0; e == cudaSuccess && i < 10; ++i) e = cudaEventCreate(&h->ev_graph[i]);
         if (e != cudaSuccess) rc = fail(HY_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
     }
     if (rc == HY_OK) rc = ensure_common(h);
@@ -817,7 +924,12 @@ int hy_index_destroy(hy_index* h) {
                       &h->w_keys2, &h->w_vals,  &h->w_vals2,   &h->w_sort, &h->w_start, &h->w_sums, &h->w_cnt,
                       &h->w_rows, &h->w_xn};
     for (DevBuf* b : bufs) b->release();
-    for (auto& ev : h->ev)
+    drop_graph(h);
+    for (auto& ev : h->ev_direct)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : h->ev_graph)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : h->gev)
         if (ev) cudaEventDestroy(ev);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -836,11 +948,16 @@ int hy_index_info(const hy_index* h, hy_index_info_t* out) {
     out->arena_rows = h->arena_rows;
     out->trained = h->trained ? 1 : 0;
     out->device = h->device;
+    out->form = h->form;
+    out->learned = learned_on(h) ? 1 : 0;
+    out->capq = h->capq;
+    out->row_slice = h->row_slice;
     return HY_OK;
 }
 
 int hy_index_train(hy_index* h, size_t n, const float* x, int lite) {
     HY_CHECK(h && (x || n == 0), HY_ERR_ARG, "train: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     return train_impl(h, n, x, false, lite, h->stream);
@@ -848,6 +965,7 @@ int hy_index_train(hy_index* h, size_t n, const float* x, int lite) {
 
 int hy_index_train_device(hy_index* h, size_t n, const float* dx, int lite, void* stream) {
     HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "train: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     return train_impl(h, n, dx, true, lite, static_cast<cudaStream_t>(stream));
@@ -855,6 +973,7 @@ int hy_index_train_device(hy_index* h, size_t n, const float* dx, int lite, void
 
 int hy_index_set_centroids(hy_index* h, const float* c) {
     HY_CHECK(h && c, HY_ERR_ARG, "set_centroids: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     const size_t bytes = h->nlist * h->d * sizeof(float);
@@ -874,6 +993,7 @@ int hy_index_get_centroids(const hy_index* h, float* c) {
 
 int hy_index_add(hy_index* h, size_t n, const float* x) {
     HY_CHECK(h && (x || n == 0), HY_ERR_ARG, "add: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     return add_impl(h, n, x, false, h->stream);
@@ -881,6 +1001,7 @@ int hy_index_add(hy_index* h, size_t n, const float* x) {
 
 int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream) {
     HY_CHECK(h && (dx || n == 0), HY_ERR_ARG, "add: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     return add_impl(h, n, dx, true, static_cast<cudaStream_t>(stream));
@@ -888,6 +1009,7 @@ int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream) {
 
 int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
     HY_CHECK(h, HY_ERR_ARG, "set_nprobe: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
     HY_CHECK(nprobe >= 1, HY_ERR_ARG, "set_nprobe: nprobe must be >= 1");
     h->nprobe = nprobe;
     return HY_OK;
@@ -895,6 +1017,7 @@ int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
 
 int hy_index_set_form(hy_index* h, int form) {
     HY_CHECK(h, HY_ERR_ARG, "set_form: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
     HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16, HY_ERR_ARG, "set_form: unknown form");
     HY_CHECK(form != HY_FORM_BF16 || h->d <= 128, HY_ERR_ARG, "set_form: the bf16 form supports d <= 128");
     h->form = form;
@@ -903,6 +1026,7 @@ int hy_index_set_form(hy_index* h, int form) {
 
 int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice) {
     HY_CHECK(h, HY_ERR_ARG, "set_batch_params: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
     if (capq) {
         HY_CHECK(capq >= 64 && capq <= 12288, HY_ERR_ARG, "set_batch_params: capq must be in [64, 12288]");
         h->capq = capq;
@@ -918,6 +1042,7 @@ int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_
 
 int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_list_size) {
     HY_CHECK(h, HY_ERR_ARG, "presearch: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
     h->warmup_list = warmup_list;
     h->warmup_list_size = warmup_list_size;
     return HY_OK;
@@ -933,10 +1058,91 @@ int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, flo
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     HY_RET(ensure_common(h));
     h->launches = 0;
-    HY_RET(search_device_impl(h, n, dq, k, dD, dI, s, true));
+    HY_RET(run_device_search(h, n, dq, k, dD, dI, s));
     h->stats.launches = h->launches;
     h->stats.nq = n;
     h->times_pending = true;
+    return HY_OK;
+}
+
+int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps, float* report) {
+    HY_CHECK(h && q && n >= 1 && reps >= 1, HY_ERR_ARG, "autotune: need a handle, queries and reps >= 1");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(check_search_args(h, n, k));
+    HY_CHECK(h->form == HY_FORM_BF16, HY_ERR_STATE, "autotune: select the bf16 form first");
+    HY_RET(set_device(h));
+    h->ev = h->ev_direct;
+    h->epoch++;
+    cudaStream_t s = h->stream;
+    HY_RET(ensure_common(h));
+    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
+    HY_RET(h->w_D.ensure(n * k * sizeof(float)));
+    HY_RET(h->w_I.ensure(n * k * sizeof(int64_t)));
+    HY_CUDA(cudaMemcpy(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice));
+    // Candidate work shapes: rows per work item (the list-side tile extent
+    // of an item) x candidate slots per query.  Every shape returns the same
+    // exact answer; the fastest is kept.
+    const size_t slices[3] = {512, 1024, 2048};
+    const size_t capqs[2] = {4096, 8192};
+    const size_t keep_rs = h->row_slice, keep_capq = h->capq;
+    std::vector<int64_t> ref_I;
+    std::vector<int64_t> got_I(n * k);
+    double best = 1e30;
+    size_t best_rs = keep_rs, best_capq = keep_capq;
+    int c = 0;
+    for (size_t rs : slices)
+        for (size_t cq : capqs) {
+            h->row_slice = rs;
+            h->capq = cq;
+            int rc = search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, false);
+            if (rc == HY_OK) {
+                HY_CUDA(ev_record(h->ev[6], s));
+                for (int r = 0; r < reps && rc == HY_OK; ++r)
+                    rc = search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s,
+                                            false);
+                HY_CUDA(ev_record(h->ev[7], s));
+            }
+            if (rc != HY_OK) {
+                h->row_slice = keep_rs;
+                h->capq = keep_capq;
+                return rc;
+            }
+            HY_CUDA(cudaStreamSynchronize(s));
+            float ms = 0.0f;
+            HY_CUDA(cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]));
+            ms /= (float)reps;
+            HY_CUDA(cudaMemcpy(got_I.data(), h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost));
+            if (ref_I.empty()) ref_I = got_I;
+            const bool same = got_I == ref_I;
+            if (report) {
+                report[3 * c] = (float)rs;
+                report[3 * c + 1] = (float)cq;
+                report[3 * c + 2] = same ? ms : -ms;
+            }
+            if (same && ms < best) {
+                best = ms;
+                best_rs = rs;
+                best_capq = cq;
+            }
+            ++c;
+        }
+    h->row_slice = best_rs;
+    h->capq = best_capq;
+    h->launches = 0;
+    h->kev = 0;
+    return HY_OK;
+}
+
+int hy_index_set_graph(hy_index* h, int enabled) {
+    HY_CHECK(h, HY_ERR_ARG, "set_graph: NULL handle");
+    std::lock_guard<std::mutex> g(h->mu);
+    HY_RET(set_device(h));
+    if (enabled && !h->gev[0]) {
+        HY_CUDA(cudaEventCreateWithFlags(&h->gev[0], cudaEventDisableTiming));
+        HY_CUDA(cudaEventCreateWithFlags(&h->gev[1], cudaEventDisableTiming));
+    }
+    if (!enabled) drop_graph(h);
+    h->graph_on = enabled != 0;
     return HY_OK;
 }
 
@@ -948,6 +1154,7 @@ namespace {
 // bf16 overflow fallback, statistics.
 int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
     cudaStream_t s = h->stream;
+    h->ev = h->ev_direct;
     HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
     HY_RET(h->w_D.ensure(n * k * sizeof(float)));
     HY_RET(h->w_I.ensure(n * k * sizeof(int64_t)));
@@ -1117,7 +1324,7 @@ int hy_index_search_nprobes_device(hy_index* h, size_t n, const float* dq, size_
     const size_t keep = h->nprobe;
     h->nprobe = std::min(max_nprobe, h->nlist);
     h->q_nprobe = dnprobes;
-    const int rc = search_device_impl(h, n, dq, k, dD, dI, s, true);
+    const int rc = run_device_search(h, n, dq, k, dD, dI, s);
     h->q_nprobe = nullptr;
     h->nprobe = keep;
     HY_RET(rc);
@@ -1130,6 +1337,7 @@ int hy_index_search_nprobes_device(hy_index* h, size_t n, const float* dq, size_
 int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max_nprobe, size_t k_label, int epochs,
                                float lr, float coverage, float* report) {
     HY_CHECK(h && q && n >= 100, HY_ERR_ARG, "train_probe_model: need a handle and at least 100 queries");
+    h->epoch++;  // a captured search graph no longer matches
     HY_CHECK(k_label >= 1 && k_label <= HY_MAX_K && epochs >= 1 && lr > 0 && coverage > 0 && coverage < 1, HY_ERR_ARG,
              "train_probe_model: bad k_label / epochs / lr / coverage");
     std::lock_guard<std::mutex> g(h->mu);
@@ -1264,6 +1472,7 @@ int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max
 
 int hy_index_set_learned(hy_index* h, int enabled, float judge_fraction, float judge_recall) {
     HY_CHECK(h, HY_ERR_ARG, "set_learned: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
     HY_CHECK(!enabled || h->model_ready, HY_ERR_STATE, "set_learned: no probe model (train or set one first)");
     HY_CHECK(judge_fraction >= 0 && judge_fraction <= 1 && judge_recall >= 0 && judge_recall <= 1, HY_ERR_ARG,
              "set_learned: judge_fraction and judge_recall must be in [0, 1]");
@@ -1290,6 +1499,7 @@ int hy_index_get_probe_model(const hy_index* hc, float* out) {
 
 int hy_index_set_probe_model(hy_index* h, const float* in) {
     HY_CHECK(h && in, HY_ERR_ARG, "set_probe_model: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     HY_RET(set_device(h));
     HY_RET(h->m_params.ensure(hy::MLP_NPARAM * sizeof(float)));
     HY_RET(h->m_mu.ensure(hy::MLP_IN * sizeof(float)));
@@ -1333,8 +1543,9 @@ int hy_index_search_preassigned(hy_index* h, size_t n, const float* q, size_t k,
                                   h->w_err.as<int>(), s));
         thr = h->w_thr.as<uint32_t>();
     }
-    HY_CUDA(cudaEventRecord(h->ev[0], s));
-    HY_CUDA(cudaEventRecord(h->ev[1], s));
+    h->ev = h->ev_direct;
+    HY_CUDA(ev_record(h->ev[0], s));
+    HY_CUDA(ev_record(h->ev[1], s));
     HY_RET(scan_and_merge(h, n, h->w_q.as<float>(), k, nprobe, h->w_probes.as<int64_t>(), thr, h->w_D.as<float>(),
                           h->w_I.as<int64_t>(), s, true));
     HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -1629,6 +1840,7 @@ int hy_index_save(const hy_index* hc, const char* path) {
 
 int hy_index_load(hy_index* h, const char* path) {
     HY_CHECK(h && path, HY_ERR_ARG, "load: NULL argument");
+    h->epoch++;  // a captured search graph no longer matches
     FileIndex f;
     HY_RET(read_index_file(path, &f, true));
     std::lock_guard<std::mutex> g(h->mu);

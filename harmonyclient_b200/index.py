@@ -136,6 +136,23 @@ class Index:
         check(self._L.hy_index_search(self._h, n, _p(q), int(k), _p(D), _p(I)))
         return D, I
 
+    def autotune(self, queries, k, reps=3):
+        """Pick the bf16 form's work shape on sample queries; returns the
+        timings as a list of (row_slice, capq, ms, same_answer)."""
+        q = _f32(queries, self.d)
+        rep = np.zeros(18, np.float32)
+        check(self._L.hy_index_autotune(self._h, q.shape[0], _p(q), int(k), int(reps), _p(rep)))
+        return [(int(rep[3 * i]), int(rep[3 * i + 1]), abs(float(rep[3 * i + 2])), bool(rep[3 * i + 2] >= 0))
+                for i in range(6)]
+
+    def batch_params(self):
+        inf = self.info()
+        return {"capq": int(inf.capq), "row_slice": int(inf.row_slice)}
+
+    def set_graph(self, enabled=True):
+        """Graph mode for the device-pointer searches (CUDA graph replay)."""
+        check(self._L.hy_index_set_graph(self._h, int(bool(enabled))))
+
     def search_nprobes(self, queries, k, nprobes):
         """Search with a per-query nprobe (int array, one per query)."""
         q = _f32(queries, self.d)

@@ -71,6 +71,10 @@ typedef struct {
     size_t arena_rows;  /* rows in the device arena, padding included */
     int trained;        /* centroids are set */
     int device;         /* CUDA device ordinal */
+    int form;           /* HY_FORM_* */
+    int learned;        /* the probe network picks each query's nprobe */
+    size_t capq;        /* bf16 form: candidate slots per query */
+    size_t row_slice;   /* bf16 form: rows per work item */
 } hy_index_info_t;
 
 /* Counters of the last search on a handle (the reference returns a Stats
@@ -93,6 +97,7 @@ typedef struct {
     double kernel_ms;         /* device time of the scan kernel's launches (plain: scan_plain_kernel;
                                  bf16: batched_scan_kernel, both passes) in the last query chunk */
     uint64_t kernel_launches; /* launches kernel_ms covers */
+    uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
     uint64_t unresolved_queries; /* bf16 device-pointer search: overflowed queries beyond the device
                                     fallback's capacity (296 per chunk), left with the bf16 re-rank's
                                     answer; the host-pointer search re-runs such batches exactly */
@@ -161,6 +166,23 @@ HY_API int hy_index_presearch(hy_index* h, size_t warmup_list, size_t warmup_lis
 HY_API int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I);
 HY_API int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI,
                                   void* stream);
+
+/* Autotuner of the bf16 form (no counterpart in the reference): times the
+ * search of n sample queries (host pointer) at k for every candidate work
+ * shape (rows per work item 512 / 1024 / 2048 x candidate slots per query
+ * 4096 / 8192; reps timed searches each, after one untimed) and keeps the
+ * fastest whose results equal the first shape's.  report (may be NULL)
+ * receives 6 x {row_slice, capq, ms} (ms negated for a shape whose results
+ * differed). */
+HY_API int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps, float* report);
+
+/* Graph mode for the device-pointer searches (no counterpart in the
+ * reference): the first call with given buffers, sizes, stream and index
+ * state runs normally and captures its launch sequence (coarse quantisation,
+ * probe network, warm-up, the persistent batched scan, re-rank, fallback) in
+ * a CUDA graph; identical later calls replay it with one launch.  Any call
+ * that changes the index or its parameters retires the graph. */
+HY_API int hy_index_set_graph(hy_index* h, int enabled);
 
 /* Search with a per-query nprobe (no counterpart in the reference, whose
  * nprobe is one value per call): query i probes its nprobes[i] nearest lists
