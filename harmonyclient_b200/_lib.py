@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(HERE, "libhy.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "hy.h")
 
 HY_OK, HY_ERR_ARG, HY_ERR_OOM, HY_ERR_CUDA, HY_ERR_TIMEOUT, HY_ERR_STATE, HY_ERR_IO, HY_ERR_UNSUPPORTED = range(8)
-HY_FORM_PLAIN, HY_FORM_BF16 = 0, 1
+HY_FORM_PLAIN, HY_FORM_BF16, HY_FORM_FP8 = 0, 1, 2
 HY_MAX_K = 256
 
 
@@ -90,6 +90,7 @@ def load():
     L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
     L.hy_index_search_preassigned_noalloc.argtypes = [H, sz, vp, sz, sz, vp, vp, vp, vp]
     L.hy_index_set_graph.argtypes = [H, i]
+    L.hy_selftest_tcgen05_e4m3.argtypes = [vp, vp, vp]
     L.hy_index_autotune.argtypes = [H, sz, vp, sz, i, vp]
     L.hy_index_search_nprobes.argtypes = [H, sz, vp, sz, vp, vp, vp]
     L.hy_index_search_nprobes_device.argtypes = [H, sz, vp, sz, vp, sz, vp, vp, vp]

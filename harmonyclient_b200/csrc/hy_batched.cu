@@ -22,6 +22,7 @@
 // distances are exact.  A query whose candidates overflow its buffer is
 // reported so the caller can answer it with the plain scan.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include <cfloat>
 #include <cstddef>
@@ -33,11 +34,9 @@
 namespace hy {
 namespace {
 
-constexpr int QG = 128;      // queries per group (MMA N)
 constexpr int TM = 128;      // rows per tile (MMA M)
 constexpr int NS = 4;        // A stages (one 16 KiB k-block each)
 constexpr int KB_BYTES = 16384;
-constexpr int TMEM_COLS = 256;  // two accumulators of QG columns
 
 // ---------------------------------------------------------------------------
 // Conversion of the FP32 arena into the bf16 tensor-core image.
@@ -56,18 +55,83 @@ __global__ void to_bf16_arena_kernel(ArenaLayout L, const float* __restrict__ co
     *reinterpret_cast<__nv_bfloat16*>(dst) = __float2bfloat16_rn(v);
 }
 
-// Per-row quantities for the bf16 error bound: |x~| (norm of the bf16-rounded
-// row) and |x - x~| (its rounding error), one warp per arena row.
-__global__ void row_aux_kernel(ArenaLayout L, const float* __restrict__ codes, int64_t rows, float2* __restrict__ aux) {
+// e4m3 code of v / scale and its decoded value times scale (saturating at
+// the largest finite e4m3 magnitude, 448).
+__device__ inline unsigned char e4m3_code(float v, float scale) {
+    return static_cast<unsigned char>(__nv_cvt_float_to_fp8(v / scale, __NV_SATFINITE, __NV_E4M3));
+}
+__device__ inline float e4m3_value(unsigned char c, float scale) {
+    const __half_raw h = __nv_cvt_fp8_to_halfraw(static_cast<__nv_fp8_storage_t>(c), __NV_E4M3);
+    return __half2float(__half(h)) * scale;
+}
+
+// e4m3 image of the arena: per 128-row tile, ceil(d/128) k-blocks of 128 rows
+// x 128 bytes in the same swizzled K-major layout as the bf16 image; every
+// value is coded relative to its list's scale (tscale of its tile).
+__global__ void to_f8_arena_kernel(ArenaLayout L, const float* __restrict__ codes, int64_t rows, int nkb,
+                                   const float* __restrict__ tscale, unsigned char* __restrict__ out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= rows * L.d) return;
+    const int64_t r = i / L.d;
+    const int j = static_cast<int>(i % L.d);
+    int b = 0;
+    while (b + 1 < L.nb && j >= L.bstart[b + 1]) ++b;
+    const float v = codes[arena_offset(L, r, b, j - L.bstart[b])];
+    const int64_t tile = r >> 7;
+    const uint32_t row = static_cast<uint32_t>(r & 127), by = static_cast<uint32_t>(j & 127);
+    out[(tile * nkb + (j >> 7)) * KB_BYTES + row * 128u + ((((by >> 4) ^ (row & 7u)) & 7u) << 4) + (by & 15u)] =
+        e4m3_code(v, tscale[tile]);
+}
+
+// Largest |value| of each 128-row tile (one warp per tile).
+__global__ void tile_absmax_kernel(ArenaLayout L, const float* __restrict__ codes, int64_t tiles,
+                                   float* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (t >= tiles) return;
+    float m = 0.0f;
+    for (int r = 0; r < TM; ++r)
+        for (int j = lane; j < L.d; j += 32) {
+            int b = 0;
+            while (b + 1 < L.nb && j >= L.bstart[b + 1]) ++b;
+            m = fmaxf(m, fabsf(codes[arena_offset(L, t * TM + r, b, j - L.bstart[b])]));
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if (lane == 0) out[t] = m;
+}
+
+// Per list: scale = (largest |value| over its tiles) / 448, 1 for an all-zero
+// list; the list's tiles get the same scale.
+__global__ void list_scale_kernel(const int64_t* __restrict__ list_off, const int32_t* __restrict__ list_size,
+                                  int nlist, const float* __restrict__ tile_max, float* __restrict__ lscale,
+                                  float* __restrict__ tscale) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlist) return;
+    const int64_t t0 = list_off[l] / TM;
+    const int nt = (list_size[l] + TM - 1) / TM;
+    float m = 0.0f;
+    for (int t = 0; t < nt; ++t) m = fmaxf(m, tile_max[t0 + t]);
+    const float sc = m > 0.0f ? m / 448.0f : 1.0f;
+    lscale[l] = sc;
+    for (int t = 0; t < nt; ++t) tscale[t0 + t] = sc;
+}
+
+// Per-row quantities for the error bound: |x~| (norm of the row as the tensor
+// cores see it: bf16-rounded, or e4m3-coded times its tile's scale when
+// tscale is given) and |x - x~| (its rounding error), one warp per arena row.
+__global__ void row_aux_kernel(ArenaLayout L, const float* __restrict__ codes, int64_t rows,
+                               const float* __restrict__ tscale, float2* __restrict__ aux) {
     const int lane = threadIdx.x & 31;
     const int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (r >= rows) return;
     float nn = 0.0f, ee = 0.0f;
+    const float ts = tscale ? tscale[r >> 7] : 1.0f;
     for (int j = lane; j < L.d; j += 32) {
         int b = 0;
         while (b + 1 < L.nb && j >= L.bstart[b + 1]) ++b;
         const float v = codes[arena_offset(L, r, b, j - L.bstart[b])];
-        const float vb = __bfloat162float(__float2bfloat16_rn(v));
+        const float vb = tscale ? e4m3_value(e4m3_code(v, ts), ts) : __bfloat162float(__float2bfloat16_rn(v));
         nn = fmaf(vb, vb, nn);
         ee = fmaf(v - vb, v - vb, ee);
     }
@@ -97,6 +161,63 @@ __global__ void tile_aux_kernel(const float2* __restrict__ row_aux, int64_t tile
         e = fmaxf(e, __shfl_xor_sync(FULL, e, o));
     }
     if (lane == 0) out[t] = make_float2(a, e);
+}
+
+// Queries in e4m3: per query scale t = max|q_j| / 448 (1 for a zero query),
+// codes of q_j / t padded to nkb*128 bytes, and {|q|^2, |q|, |q~|, |q - q~|}
+// with q~ = t * decoded code.
+__global__ void prep_queries_f8_kernel(const float* __restrict__ q, int nq, int d, int nkb,
+                                       unsigned char* __restrict__ qb, float4* __restrict__ qaux,
+                                       float* __restrict__ qscale) {
+    const int i = blockIdx.x;
+    if (i >= nq) return;
+    const float* src = q + static_cast<size_t>(i) * d;
+    __shared__ float red[2][4];
+    __shared__ float s_t;
+    float m = 0.0f;
+    for (int j = threadIdx.x; j < d; j += blockDim.x) m = fmaxf(m, fabsf(src[j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float mm = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mm = fmaxf(mm, red[0][w]);
+        s_t = mm > 0.0f ? mm / 448.0f : 1.0f;
+    }
+    __syncthreads();
+    const float t = s_t;
+    float nn = 0.0f, ee = 0.0f;
+    for (int j = threadIdx.x; j < nkb * 128; j += blockDim.x) {
+        const float v = j < d ? src[j] : 0.0f;
+        const unsigned char c = e4m3_code(v, t);
+        qb[static_cast<size_t>(i) * nkb * 128 + j] = c;
+        const float vb = e4m3_value(c, t);
+        nn = fmaf(vb, vb, nn);
+        ee = fmaf(v - vb, v - vb, ee);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nn += __shfl_xor_sync(FULL, nn, o);
+        ee += __shfl_xor_sync(FULL, ee, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = nn;
+        red[1][threadIdx.x >> 5] = ee;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.0f;
+        for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(src[j], src[j]));
+        float tn = 0.0f, te = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            tn += red[0][w];
+            te += red[1][w];
+        }
+        qaux[i] = make_float4(s, sqrtf(s), sqrtf(tn), sqrtf(te));
+        qscale[i] = t;
+    }
 }
 
 // Queries: bf16 rows padded to nkb*64, and per query {|q|^2 (sequential f32,
@@ -219,11 +340,11 @@ __global__ void probe_fill_kernel(const int64_t* __restrict__ probes, int nq, in
 
 // Items of a list = query groups x row slices (none for an empty list).
 __global__ void item_count_kernel(const int32_t* __restrict__ cnt, const int32_t* __restrict__ list_size, int nlist,
-                                  int rs, int32_t* __restrict__ items) {
+                                  int rs, int qg, int32_t* __restrict__ items) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nlist) return;
     const int c = cnt[l], s = list_size[l];
-    items[l] = (c > 0 && s > 0) ? ((c + QG - 1) / QG) * ((s + rs - 1) / rs) : 0;
+    items[l] = (c > 0 && s > 0) ? ((c + qg - 1) / qg) * ((s + rs - 1) / rs) : 0;
 }
 
 // Item descriptors {list, query group, row slice} for the first `cap` items,
@@ -243,7 +364,7 @@ __global__ void item_fill_kernel(const int64_t* __restrict__ item_off, const int
 
 // ---------------------------------------------------------------------------
 struct BatchedParams {
-    const unsigned char* abf;       // bf16 arena image
+    const unsigned char* abf;       // tensor-core image of the arena (bf16 or e4m3)
     const int64_t* list_off;        // [nlist+1]
     const int32_t* list_size;       // [nlist]
     const int64_t* item_off;        // [nlist+1]
@@ -254,8 +375,10 @@ struct BatchedParams {
     const int32_t* pair_cnt;        // [nlist]
     const float* xn;                // [arena rows] squared norms (f32)
     const float2* tile_aux;         // [arena tiles] {max |x~|, max |x - x~|} over the tile's rows
-    const __nv_bfloat16* qb;        // [nq][nkb*64]
+    const unsigned char* qb;        // [nq][nkb*128 bytes] queries in the operand type
     const float4* qaux;             // [nq] {|q|^2, |q|, |q~|, |q - q~|}
+    const float* lscale;            // e4m3 form: [nlist] list scales (x~ = lscale * code), else null
+    const float* qscale;            // e4m3 form: [nq] query scales, else null
     const float* thr;               // [nq] distance thresholds (score units)
     uint64_t* cand;                 // [nq][capq]
     int32_t* cand_cnt;              // [nq]
@@ -278,6 +401,7 @@ constexpr int CB = 256;         // per-epilogue-warp candidate staging
 // Item metadata of one query slot (two slots: the item being scanned and the
 // next one being gathered).
 constexpr int RS_MAX = 2048;  // largest row slice (rows staged per slot)
+template <int QG>
 struct ItemSlot {
     int ntiles;  // -1 = no more items
     int nqv;
@@ -290,7 +414,18 @@ struct ItemSlot {
     float V[QG];     // threshold + bound constant - |q|^2 (score units)
     float aq[QG];    // bound coefficient of |x~|
     float bq[QG];    // bound coefficient of |x - x~|
+    alignas(16) float sc[QG];    // accumulator -> inner product scale (1, or list scale x query scale)
 };
+
+// Dynamic shared memory of the batched kernel for query groups of QG and nkb
+// 128-byte k-blocks per row.
+template <int QG>
+constexpr size_t batched_smem(int nkb) {
+    constexpr int CW = QG / 2, CC = CW < 32 ? CW : 32;
+    return 1024 + 2 * static_cast<size_t>(nkb) * QG * 128 + static_cast<size_t>(NS) * KB_BYTES +
+           2 * sizeof(ItemSlot<QG>) + N_EPI * CW * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
+           N_EPI * 32 * CC * sizeof(float);
+}
 
 __device__ inline bool wait_or_abort(uint64_t* bar, uint32_t parity, int* err, volatile int* abort) {
     for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
@@ -307,18 +442,29 @@ __device__ inline void named_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// QG: queries per group (MMA N: 128, 64 or 32); F8: e4m3 operands
+// (kind::f8f6f4, K = 32 per instruction) instead of bf16 (kind::f16, K = 16).
+// Either way a k-block row is 128 bytes and one instruction covers 32 bytes
+// of it, so the descriptors and the stage ring are the same.
+template <int QG, bool F8>
 __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __grid_constant__ BatchedParams p) {
+    constexpr int CW = QG / 2;            // accumulator columns per epilogue warp
+    constexpr int CC = CW < 32 ? CW : 32;  // columns per candidate-test chunk
+    constexpr int TMEM_COLS = 2 * QG;      // two accumulators
+    constexpr int BKB = QG * 128;          // bytes of one B (query) k-block
+    using Slot = ItemSlot<QG>;
     extern __shared__ unsigned char sm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
     const int nkb = p.nkb;
-    unsigned char* sB = base;                                        // 2 slots x nkb x 16 KiB (queries)
-    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * KB_BYTES;  // NS x 16 KiB (list k-blocks)
-    ItemSlot* slot = reinterpret_cast<ItemSlot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2], 1024-aligned
-    static_assert(offsetof(ItemSlot, xn) % 16 == 0 && sizeof(ItemSlot) % 16 == 0, "ItemSlot alignment");
-    float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][64] per-tile test bounds
-    int* s_cq = reinterpret_cast<int*>(sR + N_EPI * 64);             // [N_EPI][CB]
+    unsigned char* sB = base;                                        // 2 slots x nkb x BKB (queries)
+    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * BKB;     // NS x 16 KiB (list k-blocks)
+    Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2], 1024-aligned
+    static_assert(offsetof(Slot, xn) % 16 == 0 && offsetof(Slot, sc) % 16 == 0 && sizeof(Slot) % 16 == 0,
+                  "ItemSlot alignment");
+    float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][CW] per-tile test bounds
+    int* s_cq = reinterpret_cast<int*>(sR + N_EPI * CW);             // [N_EPI][CB]
     uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
-    float* s_ip = reinterpret_cast<float*>(s_ck + N_EPI * CB);       // [N_EPI][32 lanes][32] candidate chunks
+    float* s_ip = reinterpret_cast<float*>(s_ck + N_EPI * CB);       // [N_EPI][32 lanes][CC] candidate chunks
 
     __shared__ uint64_t full[NS], empty[NS], accf[2], acce[2], sfull[2], sfree[2];
     __shared__ uint32_t tbase;
@@ -357,7 +503,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         for (uint32_t it = 0;; ++it) {
             const int b = it & 1;
             if (!wait_or_abort(&sfree[b], ((it >> 1) & 1u) ^ 1u, p.err, vabort)) break;
-            ItemSlot& S = slot[b];
+            Slot& S = slot[b];
             // One index per slot: a gather thread may still be reading this
             // item's index while thread 0 already fetches the next one.
             if (gt == 0) s_g[b] = atomicAdd(p.work, 1u);
@@ -396,6 +542,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             const int nrows = min(p.rs, sz - rsl * p.rs);
             const int32_t* grp = p.pairs + p.pair_off[l] + static_cast<int64_t>(qg) * QG;
             const long long row0 = p.list_off[l] + static_cast<long long>(rsl) * p.rs;
+            const float ls = F8 ? p.lscale[l] : 1.0f;
             if (gt == 0) {
                 S.nqv = nqv;
                 S.nrows = nrows;
@@ -417,29 +564,32 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     S.V[i] = p.thr[qid] + ec.cq - (l2 ? qa.x : 0.0f);
                     S.aq[i] = ec.aq;
                     S.bq[i] = ec.bq;
+                    S.sc[i] = F8 ? ls * p.qscale[qid] : 1.0f;
                 } else {
                     S.qn[i] = 0.0f;
                     S.V[i] = -INFINITY;
                     S.aq[i] = 0.0f;
                     S.bq[i] = 0.0f;
+                    S.sc[i] = 0.0f;
                 }
             }
-            // The group's bf16 queries into the swizzled B operand: every
-            // 16-byte chunk is its own asynchronous copy, all in flight at
-            // once; empty query slots are zero-filled.
-            unsigned char* dst = sB + static_cast<size_t>(b) * nkb * KB_BYTES;
+            // The group's queries into the swizzled B operand: every 16-byte
+            // chunk is its own asynchronous copy, all in flight at once;
+            // empty query slots are zero-filled.
+            unsigned char* dst = sB + static_cast<size_t>(b) * nkb * BKB;
+            const size_t qstride = static_cast<size_t>(nkb) * 128;
             for (int i = gt; i < QG; i += 32 * N_GATHER) {
                 if (i < nqv) {
-                    const __nv_bfloat16* src = p.qb + static_cast<size_t>(grp[i]) * nkb * 64;
+                    const unsigned char* src = p.qb + static_cast<size_t>(grp[i]) * qstride;
                     for (int kb = 0; kb < nkb; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            cp_async16(dst + kb * KB_BYTES + i * 128 + (((c ^ (i & 7)) & 7) << 4), src + kb * 64 + c * 8);
+                            cp_async16(dst + kb * BKB + i * 128 + (((c ^ (i & 7)) & 7) << 4), src + kb * 128 + c * 16);
                 } else {
                     for (int kb = 0; kb < nkb; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            *reinterpret_cast<uint4*>(dst + kb * KB_BYTES + i * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
+                            *reinterpret_cast<uint4*>(dst + kb * BKB + i * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
                 }
             }
             cp_async_wait_all();
@@ -476,7 +626,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     } else if (warp == W_MMA) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16_f32(TM, QG);
+            const uint32_t idesc = F8 ? tc::idesc_e4m3_f32(TM, QG) : tc::idesc_bf16_f32(TM, QG);
             uint32_t mma_it = 0, tile_it = 0;
             bool ok = true;
             for (uint32_t it = 0; ok; ++it) {
@@ -485,7 +635,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const int ntiles = slot[b].ntiles;
                 if (ntiles < 0) break;
                 tc::fence_after_sync();
-                const uint32_t b0 = smem_u32(sB + static_cast<size_t>(b) * nkb * KB_BYTES);
+                const uint32_t b0 = smem_u32(sB + static_cast<size_t>(b) * nkb * BKB);
                 for (int t = 0; t < ntiles && ok; ++t, ++tile_it) {
                     const int buf = tile_it & 1;
                     if (!wait_or_abort(&acce[buf], ((tile_it >> 1) & 1u) ^ 1u, p.err, vabort)) {
@@ -503,10 +653,14 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                         tc::fence_after_sync();
                         const uint32_t a0 = smem_u32(sA + static_cast<size_t>(s) * KB_BYTES);
 #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk)
-                            tc::mma_bf16(dcol, tc::sdesc_sw128(a0 + kk * 32),
-                                         tc::sdesc_sw128(b0 + kb * KB_BYTES + kk * 32), idesc,
-                                         (kb | kk) != 0 ? 1u : 0u);
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint64_t ad = tc::sdesc_sw128(a0 + kk * 32);
+                            const uint64_t bd = tc::sdesc_sw128(b0 + kb * BKB + kk * 32);
+                            if constexpr (F8)
+                                tc::mma_e4m3(dcol, ad, bd, idesc, (kb | kk) != 0 ? 1u : 0u);
+                            else
+                                tc::mma_bf16(dcol, ad, bd, idesc, (kb | kk) != 0 ? 1u : 0u);
+                        }
                         tc::mma_commit(&empty[s]);
                     }
                     if (ok) tc::mma_commit(&accf[buf]);
@@ -516,10 +670,10 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         }
     } else if (warp >= W_EPI0) {
         // ---------------- epilogue: thread = row of the tile; each warp of a
-        // TMEM lane quadrant handles half of the 128 query columns.
+        // TMEM lane quadrant handles half of the QG query columns.
         const int e = warp - W_EPI0;       // 0..7
         const int quad = warp & 3;         // TMEM lanes [32*quad, 32*quad+32)
-        const int half = e >> 2;           // columns [64*half, 64*half+64)
+        const int half = e >> 2;           // columns [CW*half, CW*half+CW)
         int* wq = s_cq + e * CB;
         uint64_t* wk = s_ck + e * CB;
         int* wcount = &s_wcount[e];
@@ -542,21 +696,21 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         for (uint32_t it = 0;; ++it) {
             const int b = it & 1;
             if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
-            const ItemSlot& S = slot[b];
+            const Slot& S = slot[b];
             const int ntiles = S.ntiles;
             if (ntiles < 0) break;
             const int nqv = S.nqv, nrows = S.nrows;
             const long long row0 = S.row0;
             bool ok = true;
-            float* R = sR + e * 64;  // this warp's 64 columns
+            float* R = sR + e * CW;  // this warp's CW columns
             for (int t = 0; t < ntiles; ++t, ++tile_it) {
                 const int buf = tile_it & 1;
                 // Per-tile test bound of this warp's queries:
                 // V + max|x~| aq + max|x - x~| bq over the tile's rows.
                 const float2 ta = S.taux[t];
                 __syncwarp();
-                for (int cc = lane; cc < 64; cc += 32) {
-                    const int q = half * 64 + cc;
+                for (int cc = lane; cc < CW; cc += 32) {
+                    const int q = half * CW + cc;
                     R[cc] = S.V[q] + fmaf(ta.x, S.aq[q], ta.y * S.bq[q]);
                 }
                 __syncwarp();
@@ -571,44 +725,53 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const float xnv = rvalid ? S.xn[rs_row] : 0.0f;
                 // Rows past the slice end compare as NaN: never candidates.
                 const float ax = rvalid ? (l2 ? xnv - err_row_const(xnv, l2, p.cN) : 0.0f) : __int_as_float(0x7fffffff);
-                // This warp's 64 columns in one TMEM load.
-                uint32_t u[64];
-                tc::tmem_ld64(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * 64), u);
+                // This warp's CW columns in one TMEM load.
+                uint32_t u[CW];
+                tc::tmem_ld_cols<CW>(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * CW), u);
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const int col0 = half * 64 + c * 32;
+                for (int c = 0; c < CW / CC; ++c) {
+                    const int col0 = half * CW + c * CC;
                     if (col0 >= nqv) continue;
-                    // The chunk's 32 test bounds, in registers (no memory
-                    // access inside the test loop).
-                    float r[32];
+                    // The chunk's test bounds (and, for e4m3, the
+                    // accumulator scales) in registers.
+                    float r[CC], m[CC];
 #pragma unroll
-                    for (int j = 0; j < 32; j += 4) {
-                        const float4 t4 = *reinterpret_cast<const float4*>(R + c * 32 + j);
+                    for (int j = 0; j < CC; j += 4) {
+                        const float4 t4 = *reinterpret_cast<const float4*>(R + c * CC + j);
                         r[j] = t4.x;
                         r[j + 1] = t4.y;
                         r[j + 2] = t4.z;
                         r[j + 3] = t4.w;
+                        if constexpr (F8) {
+                            const float4 m4 = *reinterpret_cast<const float4*>(S.sc + col0 + j);
+                            m[j] = cf * m4.x;
+                            m[j + 1] = cf * m4.y;
+                            m[j + 2] = cf * m4.z;
+                            m[j + 3] = cf * m4.w;
+                        } else {
+                            m[j] = m[j + 1] = m[j + 2] = m[j + 3] = cf;
+                        }
                     }
                     // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef)
                     uint32_t mask = 0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        mask |= (fmaf(cf, __uint_as_float(u[c * 32 + j]), ax) <= r[j]) ? (1u << j) : 0u;
+                    for (int j = 0; j < CC; ++j)
+                        mask |= (fmaf(m[j], __uint_as_float(u[c * CC + j]), ax) <= r[j]) ? (1u << j) : 0u;
                     if (mask) {
-                        // Rare: this lane has candidates in the chunk.  Its 32
-                        // inner products go to a private shared-memory row so
-                        // the set bits can be visited with a compact loop.
-                        float* sip = s_ip + (e * 32 + lane) * 32;
+                        // Rare: this lane has candidates in the chunk.  Its
+                        // accumulators go to a private shared-memory row so the
+                        // set bits can be visited with a compact loop.
+                        float* sip = s_ip + (e * 32 + lane) * CC;
 #pragma unroll
-                        for (int j = 0; j < 32; j += 4)
+                        for (int j = 0; j < CC; j += 4)
                             *reinterpret_cast<float4*>(sip + j) =
-                                make_float4(__uint_as_float(u[c * 32 + j]), __uint_as_float(u[c * 32 + j + 1]),
-                                            __uint_as_float(u[c * 32 + j + 2]), __uint_as_float(u[c * 32 + j + 3]));
+                                make_float4(__uint_as_float(u[c * CC + j]), __uint_as_float(u[c * CC + j + 1]),
+                                            __uint_as_float(u[c * CC + j + 2]), __uint_as_float(u[c * CC + j + 3]));
                         while (mask) {
                             const int j = __ffs(mask) - 1;
                             mask &= mask - 1u;
                             const int q = col0 + j;
-                            const float ip = sip[j];
+                            const float ip = F8 ? sip[j] * S.sc[q] : sip[j];
                             const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
                             const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
                             const int slotpos = atomicAdd(wcount, 1);
@@ -714,8 +877,8 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
                                                      const int64_t* __restrict__ ids, const float* __restrict__ xn,
                                                      const float2* __restrict__ xaux, const float4* __restrict__ qaux,
                                                      const float* __restrict__ q, BatchWork w, int qbase, int capq,
-                                                     int k, int metric, float cK, float cN, float* __restrict__ D,
-                                                     int64_t* __restrict__ I) {
+                                                     int k, int rmax, int metric, float cK, float cN,
+                                                     float* __restrict__ D, int64_t* __restrict__ I) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t* sel = reinterpret_cast<uint64_t*>(sm);                  // [RERANK_MAX]
     float* qs = reinterpret_cast<float*>(sel + RERANK_MAX);           // [row_pitch]
@@ -751,8 +914,19 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
         int need;
         U = o2f(cta_radix_select(hi, n, k, &need, hist, sh));
     }
+    // Oversampled re-rank (rmax > 0): of the candidates whose bound can reach
+    // the top-k, only the rmax with the smallest tensor-core distance.
+    uint32_t Sr = 0xffffffffu;
+    if (rmax > 0 && n > rmax) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            hi[i] = lo[i] <= U ? static_cast<uint32_t>(cq[i] >> 32) : 0xffffffffu;
+        __syncthreads();
+        int need;
+        Sr = cta_radix_select(hi, n, rmax, &need, hist, sh);
+    }
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        if (lo[i] <= U) {
+        if (lo[i] <= U && static_cast<uint32_t>(cq[i] >> 32) <= Sr) {
             const int pos = atomicAdd(&s_nsel, 1);
             if (pos < RERANK_MAX)
                 sel[pos] = cq[i];
@@ -848,21 +1022,21 @@ cudaError_t launch_to_bf16_arena(const ArenaLayout& L, const float* codes, int64
 }
 
 // Error-bound constants for dimension d (see err_coef).
-static void err_consts(int d, float* cK, float* cN) {
-    const int K = (d + 63) / 64 * 64;
+static void err_consts(int d, bool f8, float* cK, float* cN) {
+    const int K = f8 ? (d + 127) / 128 * 128 : (d + 63) / 64 * 64;
     const double u = 1.0 / 16777216.0, inflate = 1.0 + 1.0 / 128.0;
     *cK = static_cast<float>((K + 8) * u * inflate);
     *cN = static_cast<float>((3.0 * d + 16) * u * inflate);
 }
 
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, float* thr, cudaStream_t s) {
+                           int capq, int k, int metric, int d, bool f8, float* thr, cudaStream_t s) {
     const size_t smem = static_cast<size_t>(capq) * 8;
     cudaError_t e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     float cK, cN;
-    err_consts(d, &cK, &cN);
+    err_consts(d, f8, &cK, &cN);
     tighten_kernel<<<nq, 256, smem, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
     return cudaGetLastError();
 }
@@ -884,22 +1058,40 @@ cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, cudaStream_t s) {
-    const int nkb = (d + 63) / 64;
-    prep_queries_kernel<<<nq, 128, 0, s>>>(q, nq, d, nkb, static_cast<__nv_bfloat16*>(qb), qaux);
+cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s) {
+    if (qscale) {
+        prep_queries_f8_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 127) / 128, static_cast<unsigned char*>(qb), qaux,
+                                                  qscale);
+    } else {
+        prep_queries_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 63) / 64, static_cast<__nv_bfloat16*>(qb), qaux);
+    }
     return cudaGetLastError();
 }
 
-cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, float2* tile_aux,
-                           cudaStream_t s) {
-    row_aux_kernel<<<grid_for(rows * 32, 256), 256, 0, s>>>(L, codes, rows, aux);
+cudaError_t launch_to_f8_arena(const ArenaLayout& L, const float* codes, int64_t rows, const int64_t* list_off,
+                               const int32_t* list_size, int nlist, float* tile_max, float* lscale, float* tscale,
+                               void* out, cudaStream_t s) {
+    const int64_t tiles = rows / TM;
+    cudaError_t e = cudaMemsetAsync(out, 0, f8_image_bytes(rows, L.d), s);
+    if (e != cudaSuccess) return e;
+    fill_f32_kernel<<<grid_for(tiles, 256), 256, 0, s>>>(tscale, tiles, 1.0f);
+    tile_absmax_kernel<<<grid_for(tiles * 32, 256), 256, 0, s>>>(L, codes, tiles, tile_max);
+    list_scale_kernel<<<grid_for(nlist, 128), 128, 0, s>>>(list_off, list_size, nlist, tile_max, lscale, tscale);
+    to_f8_arena_kernel<<<grid_for(rows * L.d, 256), 256, 0, s>>>(L, codes, rows, (L.d + 127) / 128, tscale,
+                                                                  static_cast<unsigned char*>(out));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, const float* tscale, float2* aux,
+                           float2* tile_aux, cudaStream_t s) {
+    row_aux_kernel<<<grid_for(rows * 32, 256), 256, 0, s>>>(L, codes, rows, tscale, aux);
     const int64_t tiles = rows / TM;
     tile_aux_kernel<<<grid_for(tiles * 32, 256), 256, 0, s>>>(aux, tiles, tile_aux);
     return cudaGetLastError();
 }
 
 cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
-                                 const int32_t* list_size, int rs, const BatchWork& w, cudaStream_t s) {
+                                 const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s) {
     const int64_t n = static_cast<int64_t>(nq) * (j1 - j0);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.pair_cnt, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
@@ -908,10 +1100,30 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
     scan_kernel<<<1, 1024, 0, s>>>(w.pair_cnt, nlist, w.pair_off);
     probe_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_off, w.pair_fill,
                                                        w.pairs);
-    item_count_kernel<<<grid_for(nlist, 256), 256, 0, s>>>(w.pair_cnt, list_size, nlist, rs, w.item_cnt);
+    item_count_kernel<<<grid_for(nlist, 256), 256, 0, s>>>(w.pair_cnt, list_size, nlist, rs, qg, w.item_cnt);
     scan_kernel<<<1, 1024, 0, s>>>(w.item_cnt, nlist, w.item_off);
     item_fill_kernel<<<grid_for(static_cast<int64_t>(nlist) * 32, 256), 256, 0, s>>>(w.item_off, list_size, nlist, rs,
                                                                                      w.item_cap, w.items);
+    return cudaGetLastError();
+}
+
+int batched_group_size(int d, bool f8) {
+    const int nkb = f8 ? (d + 127) / 128 : (d + 63) / 64;
+    constexpr size_t cap = 227 * 1024;
+    if (batched_smem<128>(nkb) <= cap) return 128;
+    if (batched_smem<64>(nkb) <= cap) return 64;
+    if (batched_smem<32>(nkb) <= cap) return 32;
+    return 0;
+}
+
+template <int QG, bool F8>
+static cudaError_t launch_batched_t(const BatchedParams& p, int nsm, cudaStream_t s) {
+    const size_t smem = batched_smem<QG>(p.nkb);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(batched_scan_kernel<QG, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    batched_scan_kernel<QG, F8><<<nsm, BATCH_THREADS, smem, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -928,35 +1140,37 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.pair_cnt = w.pair_cnt;
     p.xn = b.xn;
     p.tile_aux = b.tile_aux;
-    p.qb = static_cast<const __nv_bfloat16*>(b.qb);
+    p.qb = static_cast<const unsigned char*>(b.qb);
     p.qaux = b.qaux;
+    p.lscale = b.lscale;
+    p.qscale = b.qscale;
     p.thr = b.thr;
     p.cand = w.cand;
     p.cand_cnt = w.cand_cnt;
     p.work = w.work;
     p.err = err;
     p.nlist = b.nlist;
-    p.nkb = (b.d + 63) / 64;
+    p.nkb = b.f8 ? (b.d + 127) / 128 : (b.d + 63) / 64;
     p.rs = b.rs;
     p.capq = b.capq;
     p.metric = b.metric;
-    err_consts(b.d, &p.cK, &p.cN);
-    const size_t smem = 1024 + 2 * static_cast<size_t>(p.nkb) * KB_BYTES + static_cast<size_t>(NS) * KB_BYTES +
-                        2 * sizeof(ItemSlot) + N_EPI * 64 * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
-                        N_EPI * 32 * 32 * sizeof(float);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    err_consts(b.d, b.f8, &p.cK, &p.cN);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(batched_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem))) != cudaSuccess)
-        return e;
-    batched_scan_kernel<<<b.nsm, BATCH_THREADS, smem, s>>>(p);
-    return cudaGetLastError();
+    switch (b.qg * 2 + (b.f8 ? 1 : 0)) {
+        case 256: return launch_batched_t<128, false>(p, b.nsm, s);
+        case 257: return launch_batched_t<128, true>(p, b.nsm, s);
+        case 128: return launch_batched_t<64, false>(p, b.nsm, s);
+        case 129: return launch_batched_t<64, true>(p, b.nsm, s);
+        case 64: return launch_batched_t<32, false>(p, b.nsm, s);
+        case 65: return launch_batched_t<32, true>(p, b.nsm, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
-                          int capq, int k, int metric, float* D, int64_t* I, cudaStream_t s) {
+                          int capq, int k, int rmax, int metric, bool f8, float* D, int64_t* I, cudaStream_t s) {
     const size_t smem = static_cast<size_t>(RERANK_MAX) * 8 + static_cast<size_t>(L.row_pitch) * 4 +
                         static_cast<size_t>(capq) * 8;
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
@@ -964,8 +1178,9 @@ cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     float cK, cN;
-    err_consts(L.d, &cK, &cN);
-    rerank_kernel<<<nq, 256, smem, s>>>(L, codes, ids, xn, xaux, qaux, q, w, qbase, capq, k, metric, cK, cN, D, I);
+    err_consts(L.d, f8, &cK, &cN);
+    rerank_kernel<<<nq, 256, smem, s>>>(L, codes, ids, xn, xaux, qaux, q, w, qbase, capq, k, rmax, metric, cK, cN, D,
+                                        I);
     return cudaGetLastError();
 }
 

@@ -17,12 +17,29 @@ inline size_t bf16_image_bytes(int64_t rows, int d) {
     return static_cast<size_t>(rows / BATCH_ROW_ALIGN) * nkb * BATCH_KB_BYTES;
 }
 
+// Bytes of the e4m3 image (128-byte k-blocks of 128 dimensions).
+inline size_t f8_image_bytes(int64_t rows, int d) {
+    const int nkb = (d + 127) / 128;
+    return static_cast<size_t>(rows / BATCH_ROW_ALIGN) * nkb * BATCH_KB_BYTES;
+}
+
+// Queries per group of the batched kernel for dimension d (128, 64 or 32:
+// the largest whose shared-memory footprint fits), 0 if none fits.
+int batched_group_size(int d, bool f8);
+
 cudaError_t launch_to_bf16_arena(const ArenaLayout& L, const float* codes, int64_t rows, void* out, cudaStream_t s);
-cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, cudaStream_t s);
-// Per arena row {|x~|, |x - x~|} for the bf16 error bound, and per 128-row
+// e4m3 image with per-list scales: tile_max [rows/128] scratch, lscale
+// [nlist] and tscale [rows/128] outputs.
+cudaError_t launch_to_f8_arena(const ArenaLayout& L, const float* codes, int64_t rows, const int64_t* list_off,
+                               const int32_t* list_size, int nlist, float* tile_max, float* lscale, float* tscale,
+                               void* out, cudaStream_t s);
+// qscale == nullptr: bf16 queries; else e4m3 queries with per-query scales.
+cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s);
+// Per arena row {|x~|, |x - x~|} for the error bound (tscale == nullptr: the
+// bf16 image, else the e4m3 image with those tile scales), and per 128-row
 // tile the maxima of both.
-cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, float2* aux, float2* tile_aux,
-                           cudaStream_t s);
+cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, const float* tscale, float2* aux,
+                           float2* tile_aux, cudaStream_t s);
 
 // Work buffers of one batched search.
 struct BatchWork {
@@ -43,10 +60,10 @@ struct BatchWork {
 // Inverts probe columns [j0, j1) of every query into per-list query groups
 // and builds the work items.
 cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
-                                 const int32_t* list_size, int rs, const BatchWork& w, cudaStream_t s);
+                                 const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s);
 // thr := min(thr, k-th smallest upper bound over each query's candidates).
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, float* thr, cudaStream_t s);
+                           int capq, int k, int metric, int d, bool f8, float* thr, cudaStream_t s);
 
 struct BatchedLaunch {
     const void* abf;
@@ -57,15 +74,22 @@ struct BatchedLaunch {
     const void* qb;
     const float4* qaux;
     const float* thr;
+    const float* lscale = nullptr;  // e4m3 form: per-list scales
+    const float* qscale = nullptr;  // e4m3 form: per-query scales
     int nlist, d, rs, capq, metric, nsm;
+    int qg = 128;     // queries per group (batched_group_size)
+    bool f8 = false;  // e4m3 operands
 };
 
 cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int* err, cudaStream_t s);
 
-// qbase: global index of the chunk's first query (overflow ids are global).
+// qbase: added to the query ids listed in w.overflow.  rmax > 0: at most the
+// rmax candidates with the smallest tensor-core distance are re-ranked (the
+// e4m3 form's oversampled re-rank); 0 re-ranks every candidate whose bound
+// can reach the top-k.
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
-                          int capq, int k, int metric, float* D, int64_t* I, cudaStream_t s);
+                          int capq, int k, int rmax, int metric, bool f8, float* D, int64_t* I, cudaStream_t s);
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s);
 
 // Device-side exact fallback for queries whose candidates overflowed

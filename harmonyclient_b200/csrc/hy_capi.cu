@@ -169,16 +169,20 @@ struct hy_index {
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
 
-    // bf16 (batched tensor-core) form
+    // batched tensor-core forms (bf16, e4m3)
     int form = HY_FORM_PLAIN;
     size_t capq = 8192;       // candidate slots per query
-    size_t oversample = 4;    // exact re-rank of oversample * k candidates
+    size_t oversample = 4;    // e4m3 form: exact re-rank of at most oversample * k candidates
     size_t row_slice = 2048;  // rows per work item
     int nsm = 0;
     DevBuf abf;               // bf16 tensor-core image of the arena
     DevBuf xaux;              // per arena row {|x~|, |x - x~|}
     DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
+    DevBuf a8, x8aux, t8aux;  // the same for the e4m3 image
+    DevBuf lscale, tscale, tmax;  // e4m3 per-list and per-tile scales, tile maxima
+    bool a8_valid = false;
+    DevBuf b_qs;              // e4m3 per-query scales
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
     DevBuf b_fq, b_fpr, b_fD, b_fI, b_fcnt, b_fbtot;  // device-side exact fallback
 
@@ -340,6 +344,7 @@ int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, con
     h->arena_rows = (size_t)h->h_list_off[nlist];
     const size_t rows_alloc = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
     h->abf_valid = false;
+    h->a8_valid = false;
     HY_RET(h->codes.ensure(rows_alloc * h->L.row_pitch * sizeof(float)));
     HY_RET(h->ids.ensure(rows_alloc * sizeof(int64_t)));
     HY_RET(h->norms.ensure(rows_alloc * sizeof(float)));
@@ -478,6 +483,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
                      bool timed);
 
 bool learned_on(const hy_index* h) { return h->learned && h->model_ready; }
+bool batched_form(const hy_index* h) { return h->form == HY_FORM_BF16 || h->form == HY_FORM_FP8; }
 
 // Chunk of queries whose probes (m x nprobe, best first) and their coarse
 // scores (h->m_pscore) are on the device: the probe network predicts each
@@ -508,7 +514,7 @@ int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, i
 // merge, in query chunks.
 int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
                        bool timed) {
-    if (h->form == HY_FORM_BF16 && h->arena_rows > 0) return search_bf16_impl(h, n, dq, k, dD, dI, s, timed);
+    if (batched_form(h) && h->arena_rows > 0) return search_bf16_impl(h, n, dq, k, dD, dI, s, timed);
     const size_t nprobe = std::min(h->nprobe, h->nlist);
     HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search: nprobe must be >= 1");
     HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "search: nlist above 40000 is not supported by the coarse selector");
@@ -553,13 +559,31 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
 
 // The bf16 tensor-core image of the arena, built on first use after add/load.
 int ensure_bf16_image(hy_index* h, cudaStream_t s) {
+    if (h->form == HY_FORM_FP8) {
+        if (h->a8_valid) return HY_OK;
+        const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
+        const size_t tiles = rows / hy::BATCH_ROW_ALIGN;
+        HY_RET(h->a8.ensure(hy::f8_image_bytes((int64_t)rows, (int)h->d)));
+        HY_RET(h->x8aux.ensure(rows * sizeof(float2)));
+        HY_RET(h->t8aux.ensure(tiles * sizeof(float2)));
+        HY_RET(h->lscale.ensure(h->nlist * sizeof(float)));
+        HY_RET(h->tscale.ensure(tiles * sizeof(float)));
+        HY_RET(h->tmax.ensure(tiles * sizeof(float)));
+        HY_CUDA(hy::launch_to_f8_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->list_off.as<int64_t>(),
+                                       h->list_size.as<int32_t>(), (int)h->nlist, h->tmax.as<float>(),
+                                       h->lscale.as<float>(), h->tscale.as<float>(), h->a8.p, s));
+        HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->tscale.as<float>(),
+                                   h->x8aux.as<float2>(), h->t8aux.as<float2>(), s));
+        h->a8_valid = true;
+        return HY_OK;
+    }
     if (h->abf_valid) return HY_OK;
     const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
     HY_RET(h->abf.ensure(hy::bf16_image_bytes((int64_t)rows, (int)h->d)));
     HY_RET(h->xaux.ensure(rows * sizeof(float2)));
     HY_RET(h->taux.ensure(rows / hy::BATCH_ROW_ALIGN * sizeof(float2)));
     HY_CUDA(hy::launch_to_bf16_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->abf.p, s));
-    HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->xaux.as<float2>(), h->taux.as<float2>(),
+    HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, nullptr, h->xaux.as<float2>(), h->taux.as<float2>(),
                                s));
     h->abf_valid = true;
     return HY_OK;
@@ -579,14 +603,18 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     const size_t capq = h->capq;
     size_t qc = std::min(query_chunk(h->nlist, n), std::max<size_t>(1, (size_t(2) << 30) / (capq * 8)));
     qc = std::min(qc, n);
-    const size_t nkb = (h->d + 63) / 64;
+    const bool f8 = h->form == HY_FORM_FP8;
+    const size_t nkb = f8 ? (h->d + 127) / 128 : (h->d + 63) / 64;  // 128-byte k-blocks per row
+    const int qg = hy::batched_group_size((int)h->d, f8);
+    HY_CHECK(qg > 0, HY_ERR_ARG, "search: d too large for the tensor-core form");
     const size_t nlist = h->nlist;
     HY_RET(h->w_scores.ensure(qc * nlist * sizeof(float)));
     HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
     if (learned_on(h)) HY_RET(h->m_pscore.ensure(qc * nprobe * sizeof(float)));
     HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
     HY_RET(h->b_thr.ensure(qc * sizeof(float)));
-    HY_RET(h->b_qb.ensure(qc * nkb * 64 * 2));
+    HY_RET(h->b_qb.ensure(qc * nkb * 128));
+    if (f8) HY_RET(h->b_qs.ensure(qc * sizeof(float)));
     HY_RET(h->b_qn.ensure(qc * sizeof(float4)));
     HY_RET(h->b_pcnt.ensure(nlist * sizeof(int32_t)));
     HY_RET(h->b_pfill.ensure(nlist * sizeof(int32_t)));
@@ -657,16 +685,21 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
             // candidate buffers then hold every probed row.
             HY_CUDA(hy::launch_fill_f32(h->b_thr.as<float>(), (int64_t)m, INFINITY, s));
         }
-        HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(), s));
+        HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(),
+                                        f8 ? h->b_qs.as<float>() : nullptr, s));
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[1], s));
         HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[2], s));
         hy::BatchedLaunch b;
-        b.abf = h->abf.p;
+        b.abf = f8 ? h->a8.p : h->abf.p;
         b.list_off = h->list_off.as<int64_t>();
         b.list_size = h->list_size.as<int32_t>();
         b.xn = h->norms.as<float>();
-        b.tile_aux = h->taux.as<float2>();
+        b.tile_aux = f8 ? h->t8aux.as<float2>() : h->taux.as<float2>();
+        b.lscale = f8 ? h->lscale.as<float>() : nullptr;
+        b.qscale = f8 ? h->b_qs.as<float>() : nullptr;
+        b.f8 = f8;
+        b.qg = qg;
         b.qb = h->b_qb.p;
         b.qaux = h->b_qn.as<float4>();
         b.thr = h->b_thr.as<float>();
@@ -681,25 +714,27 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         // bound; pass 2: the remaining probed lists under the tight threshold.
         const bool last = timed && q0 + qc >= n;
         HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
-                                         h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+                                         h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
         if (last) HY_CUDA(ev_record(h->ev[6], s));
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
         if (last) HY_CUDA(ev_record(h->ev[7], s));
         if (last) h->kev = 1;
         if (nprobe > 1) {
-            HY_CUDA(hy::launch_tighten(h->norms.as<float>(), h->xaux.as<float2>(), h->b_qn.as<float4>(), (int)m, w,
-                                       (int)capq, (int)k, h->metric, (int)h->d, h->b_thr.as<float>(), s));
+            HY_CUDA(hy::launch_tighten(h->norms.as<float>(), f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(),
+                                       h->b_qn.as<float4>(), (int)m, w, (int)capq, (int)k, h->metric, (int)h->d, f8,
+                                       h->b_thr.as<float>(), s));
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
-                                             (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, w, s));
+                                             (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
             if (last) HY_CUDA(ev_record(h->ev[8], s));
             HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
             if (last) HY_CUDA(ev_record(h->ev[9], s));
             if (last) h->kev = 2;
         }
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[3], s));
+        const int rmax = f8 ? (int)std::min<size_t>(h->oversample * k, 4096) : 0;
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
-                                  h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m, w, 0, (int)capq, (int)k,
-                                  h->metric, dD + q0 * k, dI + q0 * k, s));
+                                  f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m,
+                                  w, 0, (int)capq, (int)k, rmax, h->metric, f8, dD + q0 * k, dI + q0 * k, s));
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[4], s));
         const int fb = (int)std::min<size_t>(m, fbcap);
         HY_CUDA(hy::launch_fb_gather(w.overflow, qq, h->w_probes.as<int64_t>(), (int)nprobe, (int)h->d, fb,
@@ -1018,8 +1053,10 @@ int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
 int hy_index_set_form(hy_index* h, int form) {
     HY_CHECK(h, HY_ERR_ARG, "set_form: NULL handle");
     h->epoch++;  // a captured search graph no longer matches
-    HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16, HY_ERR_ARG, "set_form: unknown form");
-    HY_CHECK(form != HY_FORM_BF16 || h->d <= 128, HY_ERR_ARG, "set_form: the bf16 form supports d <= 128");
+    HY_CHECK(form == HY_FORM_PLAIN || form == HY_FORM_BF16 || form == HY_FORM_FP8, HY_ERR_ARG,
+             "set_form: unknown form");
+    HY_CHECK(form == HY_FORM_PLAIN || hy::batched_group_size((int)h->d, form == HY_FORM_FP8) > 0, HY_ERR_ARG,
+             "set_form: d too large for the tensor-core forms (bf16: d <= 768, e4m3: d <= 1536)");
     h->form = form;
     return HY_OK;
 }
@@ -1069,7 +1106,7 @@ int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps,
     HY_CHECK(h && q && n >= 1 && reps >= 1, HY_ERR_ARG, "autotune: need a handle, queries and reps >= 1");
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(check_search_args(h, n, k));
-    HY_CHECK(h->form == HY_FORM_BF16, HY_ERR_STATE, "autotune: select the bf16 form first");
+    HY_CHECK(batched_form(h), HY_ERR_STATE, "autotune: select the bf16 or e4m3 form first");
     HY_RET(set_device(h));
     h->ev = h->ev_direct;
     h->epoch++;
@@ -1171,7 +1208,7 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
         HY_CUDA(cudaMemcpy(&tot, h->m_total.p, sizeof(tot), cudaMemcpyDeviceToHost));
         h->stats.mean_nprobe = (double)tot / (double)n;
     }
-    if (h->form == HY_FORM_BF16 && h->arena_rows > 0) {
+    if (batched_form(h) && h->arena_rows > 0) {
         const hy_search_stats_t keep = h->stats;
         HY_RET(bf16_fallback(h, n, k, D, I, s));
         const uint64_t fb = h->stats.fallback_queries;
@@ -1631,7 +1668,7 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
         HY_RET(set_device(h));
         HY_CUDA(cudaEventSynchronize(h->ev[4]));
         collect_times(h);
-        if (h->form == HY_FORM_BF16 && h->b_fbtot.p) {
+        if (batched_form(h) && h->b_fbtot.p) {
             unsigned long long c[2] = {0, 0};
             HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
             h->stats.fallback_queries = c[0];

@@ -3,6 +3,7 @@
 // TMEM, commit to an mbarrier, 32x32b loads), so the tests can check the
 // tensor-core plumbing against an exact integer product on its own.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include <string>
 
@@ -12,6 +13,8 @@
 namespace hy {
 namespace {
 
+// F8: operands are e4m3 (K = 256 in two 128-byte k-blocks), else bf16 (K = 128).
+template <bool F8>
 __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* __restrict__ A, const float* __restrict__ B,
                                                           float* __restrict__ D, int* err) {
     extern __shared__ unsigned char sm_raw[];
@@ -22,11 +25,21 @@ __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* __restric
     __shared__ uint32_t tbase;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    for (int i = threadIdx.x; i < 128 * 128; i += blockDim.x) {
-        const int r = i >> 7, k = i & 127;
-        const int kb = k >> 6, kk = k & 63;
-        *reinterpret_cast<__nv_bfloat16*>(sA + kb * 16384 + tc::kblock_offset(r, kk)) = __float2bfloat16_rn(A[i]);
-        *reinterpret_cast<__nv_bfloat16*>(sB + kb * 16384 + tc::kblock_offset(r, kk)) = __float2bfloat16_rn(B[i]);
+    if constexpr (F8) {
+        for (int i = threadIdx.x; i < 128 * 256; i += blockDim.x) {
+            const int r = i >> 8, k = i & 255;
+            const int kb = k >> 7, by = k & 127;
+            const uint32_t off = kb * 16384 + r * 128 + ((((by >> 4) ^ (r & 7)) & 7) << 4) + (by & 15);
+            sA[off] = __nv_cvt_float_to_fp8(A[i], __NV_SATFINITE, __NV_E4M3);
+            sB[off] = __nv_cvt_float_to_fp8(B[i], __NV_SATFINITE, __NV_E4M3);
+        }
+    } else {
+        for (int i = threadIdx.x; i < 128 * 128; i += blockDim.x) {
+            const int r = i >> 7, k = i & 127;
+            const int kb = k >> 6, kk = k & 63;
+            *reinterpret_cast<__nv_bfloat16*>(sA + kb * 16384 + tc::kblock_offset(r, kk)) = __float2bfloat16_rn(A[i]);
+            *reinterpret_cast<__nv_bfloat16*>(sB + kb * 16384 + tc::kblock_offset(r, kk)) = __float2bfloat16_rn(B[i]);
+        }
     }
     fence_proxy_async();
     if (threadIdx.x == 0) {
@@ -40,12 +53,15 @@ __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* __restric
     tc::fence_after_sync();
     const uint32_t t = tbase;
     if (threadIdx.x == 0) {
-        const uint32_t idesc = tc::idesc_bf16_f32(128, 128);
+        const uint32_t idesc = F8 ? tc::idesc_e4m3_f32(128, 128) : tc::idesc_bf16_f32(128, 128);
         for (int kb = 0; kb < 2; ++kb)
             for (int kk = 0; kk < 4; ++kk) {
                 const uint64_t a = tc::sdesc_sw128(smem_u32(sA + kb * 16384 + kk * 32));
                 const uint64_t b = tc::sdesc_sw128(smem_u32(sB + kb * 16384 + kk * 32));
-                tc::mma_bf16(t, a, b, idesc, (kb | kk) != 0 ? 1u : 0u);
+                if constexpr (F8)
+                    tc::mma_e4m3(t, a, b, idesc, (kb | kk) != 0 ? 1u : 0u);
+                else
+                    tc::mma_bf16(t, a, b, idesc, (kb | kk) != 0 ? 1u : 0u);
             }
         tc::mma_commit(&bar);
     }
@@ -67,28 +83,32 @@ __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* __restric
 }  // namespace
 }  // namespace hy
 
-extern "C" int hy_selftest_tcgen05(const float* A, const float* B, float* D) {
+namespace {
+
+template <bool F8>
+int run_selftest(const float* A, const float* B, float* D) {
     if (!A || !B || !D) return HY_ERR_ARG;
     float *dA = nullptr, *dB = nullptr, *dD = nullptr;
     int* derr = nullptr;
-    const size_t bytes = 128 * 128 * sizeof(float);
+    const size_t in_bytes = (F8 ? 128 * 256 : 128 * 128) * sizeof(float);
+    const size_t out_bytes = 128 * 128 * sizeof(float);
     int rc = HY_OK;
-    if (cudaMalloc(&dA, bytes) != cudaSuccess || cudaMalloc(&dB, bytes) != cudaSuccess ||
-        cudaMalloc(&dD, bytes) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+    if (cudaMalloc(&dA, in_bytes) != cudaSuccess || cudaMalloc(&dB, in_bytes) != cudaSuccess ||
+        cudaMalloc(&dD, out_bytes) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
         rc = HY_ERR_CUDA;
     }
     if (rc == HY_OK) {
-        cudaMemcpy(dA, A, bytes, cudaMemcpyHostToDevice);
-        cudaMemcpy(dB, B, bytes, cudaMemcpyHostToDevice);
-        cudaMemset(dD, 0, bytes);
+        cudaMemcpy(dA, A, in_bytes, cudaMemcpyHostToDevice);
+        cudaMemcpy(dB, B, in_bytes, cudaMemcpyHostToDevice);
+        cudaMemset(dD, 0, out_bytes);
         cudaMemset(derr, 0, sizeof(int));
         const int smem = 65536 + 1024;
-        cudaFuncSetAttribute(hy::tc_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        hy::tc_selftest_kernel<<<1, 128, smem>>>(dA, dB, dD, derr);
+        cudaFuncSetAttribute(hy::tc_selftest_kernel<F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        hy::tc_selftest_kernel<F8><<<1, 128, smem>>>(dA, dB, dD, derr);
         cudaError_t e = cudaDeviceSynchronize();
         int herr = 0;
         if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(D, dD, bytes, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(D, dD, out_bytes, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = HY_ERR_CUDA;
         else if (herr) rc = HY_ERR_TIMEOUT;
     }
@@ -98,3 +118,9 @@ extern "C" int hy_selftest_tcgen05(const float* A, const float* B, float* D) {
     cudaFree(derr);
     return rc;
 }
+
+}  // namespace
+
+extern "C" int hy_selftest_tcgen05(const float* A, const float* B, float* D) { return run_selftest<false>(A, B, D); }
+
+extern "C" int hy_selftest_tcgen05_e4m3(const float* A, const float* B, float* D) { return run_selftest<true>(A, B, D); }

@@ -120,9 +120,10 @@ class Index:
         check(self._L.hy_index_presearch(self._h, int(warmUpSearchList), int(warmUpSearchListSize)))
 
     def set_form(self, form):
-        """'plain' (exact FP32 scan) or 'bf16' (batched tensor-core scan with
-        exact FP32 re-rank)."""
-        f = {"plain": _lib.HY_FORM_PLAIN, "bf16": _lib.HY_FORM_BF16}.get(form, form)
+        """'plain' (exact FP32 scan), 'bf16' (batched tensor-core scan with
+        exact FP32 re-rank) or 'fp8' (the same on e4m3 codes with per-list
+        scales and an oversampled exact re-rank)."""
+        f = {"plain": _lib.HY_FORM_PLAIN, "bf16": _lib.HY_FORM_BF16, "fp8": _lib.HY_FORM_FP8}.get(form, form)
         check(self._L.hy_index_set_form(self._h, int(f)))
 
     def set_batch_params(self, capq=0, oversample=0, row_slice=0):

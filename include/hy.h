@@ -51,7 +51,8 @@ enum { HY_METRIC_IP = 0, HY_METRIC_L2 = 1 };
 /* Scan forms selectable with hy_index_set_form. */
 enum {
     HY_FORM_PLAIN = 0, /* exact FP32 query-major scan with dim-block pruning */
-    HY_FORM_BF16 = 1   /* batched list-major bf16 tensor-core scan + exact FP32 re-rank */
+    HY_FORM_BF16 = 1,  /* batched list-major bf16 tensor-core scan + exact FP32 re-rank */
+    HY_FORM_FP8 = 2    /* the same on e4m3 codes with per-list / per-query scales, oversampled re-rank */
 };
 
 /* Largest k the scan kernels keep per query. The reference's distributed
@@ -282,6 +283,9 @@ HY_API int hy_mlp_loss_grad(const float* params, int B, const float* X, const fl
  * (D = A * B^T, A and B row-major 128 x 128 float32 rounded to bf16, D
  * float32).  Returns HY_OK or an error status. */
 HY_API int hy_selftest_tcgen05(const float* A, const float* B, float* D);
+/* The same on e4m3 operands: A and B are 128 x 256 (values rounded to e4m3
+ * with saturation), D = A B^T is 128 x 128, accumulated by kind::f8f6f4. */
+HY_API int hy_selftest_tcgen05_e4m3(const float* A, const float* B, float* D);
 
 #ifdef __cplusplus
 }
