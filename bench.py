@@ -38,14 +38,15 @@ METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu
 # captures of this script (dram__bytes_read.sum + dram__bytes_write.sum; the
-# capture commands are listed in profiles/), keyed by (form, nb, nq, nprobe).
+# capture commands are listed in profiles/), keyed by (workload, form, nb, nq,
+# nprobe).
 # The plain entry is a 1,000-query capture scaled by 10 to the 10,000-query
 # launch (traffic grows with the query count: every query streams its own
 # probed lists).
 KNOWN_TRAFFIC = {
-    ("plain", 1_000_000, 10_000, 64): 218_703_690_000,
-    ("learned", 1_000_000, 10_000, 64): 250_758_000,
-    ("bf16", 1_000_000, 10_000, 64): 279_463_000,
+    ("c2", "plain", 1_000_000, 10_000, 64): 218_703_690_000,
+    ("c2", "learned", 1_000_000, 10_000, 64): 250_758_000,
+    ("c2", "bf16", 1_000_000, 10_000, 64): 279_463_000,
 }
 
 
@@ -109,12 +110,29 @@ class Clocks:
                 "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml"}
 
 
+# The measured workloads (seeded synthetic stand-ins of the named shapes).
+WORKLOADS = {
+    "c2": dict(gen="gmm_uint8", d=128, nlist=1024, k=100,
+               desc="{nb} x 128 uint8-valued gmm (4096 components, sigma 20)",
+               data="synthetic (seeded Gaussian mixture, integer-valued in [0,255])"),
+    "c3": dict(gen="gmm_dense", d=420, nlist=2048, k=10,
+               desc="{nb} x 420 float gmm (2048 components, per-dim mean U[-1,1], sigma 0.3)",
+               data="synthetic (seeded Gaussian mixture, float32)"),
+}
+
+
+def queries(args, n, query_seed):
+    """Another query set from the workload's mixture."""
+    from harmonyclient_b200 import datasets
+    return getattr(datasets, WORKLOADS[args.workload]["gen"])(0, n, seed=0, query_seed=query_seed)[1]
+
+
 def workload(args, rank):
     from harmonyclient_b200 import datasets
-    x, q = datasets.gmm_uint8(args.nb, args.nq, seed=0)
+    x, q = getattr(datasets, WORKLOADS[args.workload]["gen"])(args.nb, args.nq, seed=0)
     if rank:
         # Other ranks search their own queries from the same mixture.
-        _, q = datasets.gmm_uint8(0, args.nq, seed=0, query_seed=1000 + rank)
+        q = queries(args, args.nq, 1000 + rank)
     return x, q
 
 
@@ -181,11 +199,14 @@ def _kernel_ms(idx, dq, dD, dI, k, reps, ts):
     return tot / max(launches, 1), launches / max(reps, 1)
 
 
-def _recall10(x, q, I, ns):
-    from oracle import port
-    ns = min(ns, q.shape[0])
-    _, It = port.bruteforce_f64(x, q[:ns], 10)
-    return float(np.mean([len(set(a) & set(b)) / 10 for a, b in zip(I[:ns, :10].tolist(), It.tolist())])), ns
+def _score(x, q, D, I, ns, truth):
+    """recall@10 and distance errors against the float64 GPU brute force on
+    the first ns queries (0: all); the exact top-10 is computed once."""
+    from oracle import gpu_bruteforce as gb
+    ns = q.shape[0] if ns <= 0 else min(ns, q.shape[0])
+    if "It" not in truth:
+        truth["Dt"], truth["It"] = gb.topk(x, q[:ns], 10)
+    return gb.score(D[:ns], I[:ns], truth["Dt"], truth["It"], x, q[:ns], at=10), ns
 
 
 def run_ours(args, rank, world, dist):
@@ -199,7 +220,8 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     x, q = workload(args, rank)
-    nlist, k, d = 1024, 100, 128
+    W = WORKLOADS[args.workload]
+    nlist, k, d = W["nlist"], W["k"], W["d"]
     idx = hb.Index(d, nlist, args.nprobe, hb.METRIC_L2, device=dev)
     t0 = time.perf_counter()
     idx.train(x)
@@ -213,15 +235,18 @@ def run_ours(args, rank, world, dist):
     if learned:
         # The probe network is trained on its own query sample from the same
         # mixture (labels from the exact scan at the index's nprobe).
-        _, tq = datasets.gmm_uint8(0, args.train_queries, seed=0, query_seed=777)
+        tq = queries(args, args.train_queries, 777)
         t0 = time.perf_counter()
         probe_report = idx.train_probe_model(tq, max_nprobe=args.nprobe, k_label=10, epochs=args.epochs,
                                              lr=1e-3, coverage=args.coverage)
         train_s = time.perf_counter() - t0
         idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
-    idx.set_form("plain" if args.form == "plain" else "bf16")
+    base = args.base if learned else args.form
+    idx.set_form(base)
     tune = None
-    if args.form != "plain" and args.autotune:
+    if base == "fp8":
+        idx.set_batch_params(oversample=args.oversample)
+    if base != "plain" and args.autotune:
         # Work shape picked on this batch (every shape gives the same answer).
         tune = idx.autotune(q, k, reps=2)
 
@@ -236,6 +261,7 @@ def run_ours(args, rank, world, dist):
     ms_max, st_dev, clocks = _time_device(idx, dq, dD, dI, k, args.steps, stream, dist, dev)
     value = world * q.shape[0] * args.steps / (ms_max / 1e3)
     I_main = dI.cpu().numpy()
+    D_main = dD.cpu().numpy()
     kern_ms, kern_per_search = _kernel_ms(idx, dq, dD, dI, k, 3, stream)
 
     # End to end through the public host API: pinned host queries in, results
@@ -275,15 +301,15 @@ def run_ours(args, rank, world, dist):
     # fraction.
     plain = None
     P_main = idx.probes(q)
-    if args.form != "plain" and args.plain_steps > 0:
+    if base != "plain" and args.plain_steps > 0:
         if learned:
             idx.set_learned(False)
         idx.set_form("plain")
         idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream.cuda_stream)
         pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev)
         pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream)
-        plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "clocks": pclk}
-        idx.set_form("bf16")
+        plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "D": dD.cpu().numpy(), "clocks": pclk}
+        idx.set_form(base)
         if learned:
             idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
 
@@ -298,14 +324,14 @@ def run_ours(args, rank, world, dist):
     hbm_peak, tc_peak, peak_kind = peaks()
     learned_probes = int((P_main >= 0).sum())
     rows_main = pair_rows(P_main)
-    if args.form == "plain":
+    if base == "plain":
         # Algorithmic bytes of one scan launch: every (query, probed row)
         # pair's row, d x 4 bytes, plus the queries and the results.
         alg = rows_main * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
         ach = alg / (kern_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "traffic": KNOWN_TRAFFIC.get(("plain", args.nb, args.nq,
-                                                                               args.nprobe)),
+                "frac": round(ach / hbm_peak, 4), "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb,
+                                                                               args.nq, args.nprobe)),
                 "peak_kind": peak_kind, "kernel": "scan_plain_kernel", "kernel_ms": round(kern_ms, 4),
                 "algorithmic_bytes": alg}
     else:
@@ -319,7 +345,7 @@ def run_ours(args, rank, world, dist):
             cols = P_main[:, j0:j1]
             used = np.unique(cols[cols >= 0])
             distinct += int(sizes[used].sum())
-        lbytes = distinct * d * 2 / kern_per_search
+        lbytes = distinct * d * (1 if base == "fp8" else 2) / kern_per_search
         t_tc, t_hbm = flops / (tc_peak * 1e12), lbytes / (hbm_peak * 1e9)
         if t_tc >= t_hbm:
             ach = flops / (kern_ms / 1e3) / 1e12
@@ -329,12 +355,13 @@ def run_ours(args, rank, world, dist):
             ach = lbytes / (kern_ms / 1e3) / 1e9
             roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
                     "frac": round(ach / hbm_peak, 4)}
-        roof.update({"traffic": KNOWN_TRAFFIC.get((args.form, args.nb, args.nq, args.nprobe)),
+        roof.update({"traffic": KNOWN_TRAFFIC.get((args.workload, args.form, args.nb, args.nq, args.nprobe)),
                      "peak_kind": peak_kind, "kernel": "batched_scan_kernel", "kernel_ms": round(kern_ms, 4),
                      "algorithmic_flops": int(flops), "algorithmic_bytes": int(lbytes),
                      "launches_per_search": kern_per_search})
 
-    recall10, ns = _recall10(x, q, I_main, args.recall_sample)
+    truth = {}
+    sc_main, ns = _score(x, q, D_main, I_main, args.recall_sample, truth)
     plain_line = None
     if plain is not None:
         if learned:
@@ -343,14 +370,16 @@ def run_ours(args, rank, world, dist):
         prow = pair_rows(P_plain)
         palg = prow * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
         pach = palg / (plain["kernel_ms"] / 1e3) / 1e9
-        prec, _ = _recall10(x, q, plain["I"], args.recall_sample)
+        sc_plain, _ = _score(x, q, plain["D"], plain["I"], args.recall_sample, truth)
         pv = world * q.shape[0] * args.plain_steps / (plain["ms"] / 1e3)
         plain_line = {"value": round(pv, 1), "unit": "queries/s", "steps": args.plain_steps,
-                      "ms_per_step": round(plain["ms"] / args.plain_steps, 3), "recall_at_10": round(prec, 4),
+                      "ms_per_step": round(plain["ms"] / args.plain_steps, 3),
+                      "recall_at_10": round(sc_plain["recall"], 4),
+                      "dist_rel_err_max": sc_plain["dist_rel_err_max"],
                       "nprobe": args.nprobe, "speedup_of_headline": round(value / pv, 2),
                       "roofline": {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
                                    "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
-                                   "traffic": KNOWN_TRAFFIC.get(("plain", args.nb, args.nq, args.nprobe)),
+                                   "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb, args.nq, args.nprobe)),
                                    "kernel": "scan_plain_kernel", "kernel_ms": round(plain["kernel_ms"], 4),
                                    "algorithmic_bytes": palg},
                       "clocks": plain["clocks"]}
@@ -358,8 +387,10 @@ def run_ours(args, rank, world, dist):
     cpu = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
     h2d = q.nbytes
     d2h = q.shape[0] * k * 12
-    form_name = {"learned": "learned probes + bf16 tcgen05 scan + exact FP32 re-rank",
-                 "bf16": "bf16 tcgen05 scan + exact FP32 re-rank", "plain": "plain FP32 scan"}[args.form]
+    scan_name = {"bf16": "bf16 tcgen05 scan + exact FP32 re-rank",
+                 "fp8": f"e4m3 tcgen05 scan (per-list scales) + exact FP32 re-rank of <= {args.oversample} x k",
+                 "plain": "plain FP32 scan"}[base]
+    form_name = f"learned probes + {scan_name}" if learned else scan_name
     line = {
         "metric": METRIC,
         "value": round(value, 1),
@@ -371,15 +402,17 @@ def run_ours(args, rank, world, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" if args.form == "plain" else "bf16",
-        "data": "synthetic (seeded Gaussian mixture, integer-valued in [0,255])",
+        "dtype": {"plain": "f32", "bf16": "bf16", "fp8": "e4m3"}[base],
+        "data": W["data"],
         "form": form_name,
-        "config": {"workload": f"{args.nb} x {d} uint8-valued gmm (4096 components, sigma 20), nlist {nlist}, "
-                               f"nprobe {args.nprobe}, k {k}, {q.shape[0]} queries per step per GPU",
+        "config": {"workload": W["desc"].format(nb=args.nb) + f", nlist {nlist}, nprobe {args.nprobe}, k {k}, "
+                               f"{q.shape[0]} queries per step per GPU",
+                   "name": args.workload,
                    "nb": args.nb, "d": d, "nlist": nlist, "nprobe": args.nprobe, "k": k, "nq": q.shape[0],
                    "l2_flush": "not needed: list arena larger than L2", "parallelism": f"replicas x{world}"},
-        "recall_at_10": round(recall10, 4),
-        "recall_vs": f"FP64 brute force, first {ns} queries",
+        "recall_at_10": round(sc_main["recall"], 4),
+        "recall_vs": f"FP64 brute force on the GPU, {ns} queries",
+        "dist_rel_err": {"max": sc_main["dist_rel_err_max"], "mean": sc_main["dist_rel_err_mean"]},
         "mean_nprobe": round(learned_probes / q.shape[0], 3),
         "roofline": roof,
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d,
@@ -416,8 +449,9 @@ def run_reference(args, rank):
     x, q = workload(args, 0)
     nt = os.cpu_count() or 1
     ref.set_threads(nt)
-    nlist, k = 1024, 100
-    R = ref.RefIndex(128, nlist, args.nprobe)
+    W = WORKLOADS[args.workload]
+    nlist, k = W["nlist"], W["k"]
+    R = ref.RefIndex(W["d"], nlist, args.nprobe)
     R.train(x)
     R.add(x)
     m = max(nt, 64)
@@ -437,8 +471,8 @@ def run_reference(args, rank):
         "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"{args.nb} x 128 uint8-valued gmm, nlist {nlist}, nprobe {args.nprobe}, k {k}",
-                   "queries_per_step": per_step},
+        "config": {"workload": W["desc"].format(nb=args.nb) + f", nlist {nlist}, nprobe {args.nprobe}, k {k}",
+                   "name": args.workload, "queries_per_step": per_step},
         "cpu_baseline": {"value": round(v, 2), "unit": "queries/s", "cores": nt, "kind": "reference",
                          "sample": f"{per_step} queries per step of the {q.shape[0]}-query batch"},
         "e2e": {"value": round(v, 2), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -453,7 +487,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nprobe", type=int, default=64)
     ap.add_argument("--warmup-list", type=int, default=10)
-    ap.add_argument("--form", default="learned", choices=["learned", "bf16", "plain"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--form", default="learned", choices=["learned", "bf16", "fp8", "plain"])
+    ap.add_argument("--base", default="bf16", choices=["bf16", "fp8", "plain"],
+                    help="scan form under the learned probes")
+    ap.add_argument("--oversample", type=int, default=4, help="e4m3 form: re-rank at most oversample x k")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--train-queries", type=int, default=20000)
     ap.add_argument("--epochs", type=int, default=30)
@@ -463,7 +501,7 @@ def main():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--nb", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
-    ap.add_argument("--recall-sample", type=int, default=200)
+    ap.add_argument("--recall-sample", type=int, default=0, help="queries scored for recall (0: all)")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=5.0)
     args = ap.parse_args()

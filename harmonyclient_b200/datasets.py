@@ -70,11 +70,14 @@ def gmm_uint8(n, nq, d=128, ncomp=4096, sigma=20.0, seed=0, zipf=None, query_see
     return x, q
 
 
-def gmm_dense(n, nq, d=420, ncomp=2048, sigma=0.3, seed=0):
-    """Mixture with per-dimension means U[-1,1] (config c3)."""
+def gmm_dense(n, nq, d=420, ncomp=2048, sigma=0.3, seed=0, query_seed=None):
+    """Mixture with per-dimension means U[-1,1] (config c3); query_seed as
+    in gmm_uint8."""
     rng = np.random.default_rng(seed)
     centres = rng.uniform(-1.0, 1.0, size=(ncomp, d)).astype(np.float32)
-    return _mixture(rng, n, centres, sigma), _mixture(rng, nq, centres, sigma)
+    x = _mixture(rng, n, centres, sigma)
+    q = _mixture(rng if query_seed is None else np.random.default_rng(query_seed), nq, centres, sigma)
+    return x, q
 
 
 def sparse_nonneg(n, nq, d=500, ncomp=2048, density=0.1, seed=0, chunk=1 << 17):

@@ -7,6 +7,8 @@ Two libraries live here, both used only as checkers (by ``tests/``,
   compiled unmodified from the reference sources into ``oracle/_ref``.
 * ``oracle.port`` — this project's sequential C++ restatement of the same
   algorithm (``oracle/hy_oracle.cpp``), built into ``oracle/_build``.
+* ``oracle.gpu_bruteforce`` — float64 brute force on the GPU (torch), the
+  recall and distance-error oracle of the full-size measurement.
 * ``oracle.mlp``  — numpy restatement of the learned probe predictor
   (features, stop labels, network forward/backward) for checking its kernels.
 
