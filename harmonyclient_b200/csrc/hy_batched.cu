@@ -873,6 +873,141 @@ __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ 
 // in w.overflow for the caller.
 constexpr int RERANK_MAX = 4096;
 
+// Warp re-rank of one query with at most KR*32 candidates, all in registers
+// (element e = r*32 + lane): U = the k-th smallest upper bound s + e (warp
+// bitonic sort), the selected set = candidates with s - e <= U (for rmax > 0
+// only the rmax with the smallest s), their exact FP32 distances (the plain
+// scan's arithmetic, spread over the lanes through the warp's shared list
+// sl), a final sort, the top k written out.
+template <int KR>
+__device__ void rerank_warp_query(const ArenaLayout& L, const float* __restrict__ codes,
+                                  const int64_t* __restrict__ ids, const float* __restrict__ xn,
+                                  const float2* __restrict__ xaux, const ErrCoef& ec, const uint64_t* cq, int n, int k,
+                                  int rmax, bool l2, float cN, const float* qs, uint64_t* sl, float* __restrict__ Dq,
+                                  int64_t* __restrict__ Iq, int lane) {
+    uint64_t key[KR], srt[KR];
+    float lo[KR];
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        const int e = r * 32 + lane;
+        key[r] = KEY_MAX;
+        srt[r] = KEY_MAX;
+        lo[r] = INFINITY;
+        if (e < n) {
+            const uint64_t kk = cq[e];
+            const int64_t row = static_cast<int64_t>(kk & 0xffffffffu);
+            const float sc = o2f(static_cast<uint32_t>(kk >> 32));
+            const float2 xa = xaux[row];
+            const float eb = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+            key[r] = kk;
+            lo[r] = sc - eb;
+            srt[r] = static_cast<uint64_t>(f2o(sc + eb)) << 32;
+        }
+    }
+    float U = INFINITY;
+    if (n > k) {
+        warp_sort<KR>(srt, lane);
+        U = o2f(static_cast<uint32_t>(warp_get<KR>(srt, k - 1) >> 32));
+    }
+    bool sel[KR];
+    int nsel = 0;
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        sel[r] = key[r] != KEY_MAX && lo[r] <= U;
+        nsel += sel[r] ? 1 : 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nsel += __shfl_xor_sync(FULL, nsel, o);
+    if (rmax > 0 && nsel > rmax) {
+#pragma unroll
+        for (int r = 0; r < KR; ++r) srt[r] = sel[r] ? key[r] : KEY_MAX;
+        warp_sort<KR>(srt, lane);
+        const uint32_t Sr = static_cast<uint32_t>(warp_get<KR>(srt, rmax - 1) >> 32);
+#pragma unroll
+        for (int r = 0; r < KR; ++r) sel[r] = sel[r] && static_cast<uint32_t>(key[r] >> 32) <= Sr;
+    }
+    int m = 0;
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        const unsigned b = __ballot_sync(FULL, sel[r]);
+        if (sel[r]) sl[m + __popc(b & ((1u << lane) - 1u))] = key[r] & 0xffffffffu;
+        m += __popc(b);
+    }
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+        const int64_t row = static_cast<int64_t>(sl[i]);
+        const float sc = l2 ? row_l2_global(L, codes, row, qs, true) : -row_ip_global(L, codes, row, qs);
+        sl[i] = (static_cast<uint64_t>(f2o(sc)) << 32) | static_cast<uint32_t>(row);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        const int e = r * 32 + lane;
+        srt[r] = e < m ? sl[e] : KEY_MAX;
+    }
+    warp_sort<KR>(srt, lane);
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        const int e = r * 32 + lane;
+        if (e < k) {
+            const uint64_t kk = srt[r];
+            if (kk == KEY_MAX) {
+                Dq[e] = l2 ? FLT_MAX : -FLT_MAX;
+                Iq[e] = -1;
+            } else {
+                const float sc = o2f(static_cast<uint32_t>(kk >> 32));
+                Dq[e] = l2 ? sc : -sc;
+                Iq[e] = ids[kk & 0xffffffffu];
+            }
+        }
+    }
+}
+
+// One warp per query; a query with more than 512 candidates (or k > 512, or
+// an overflowed buffer) is listed in w.big for the CTA kernel.
+__global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant__ ArenaLayout L,
+                                                          const float* __restrict__ codes,
+                                                          const int64_t* __restrict__ ids, const float* __restrict__ xn,
+                                                          const float2* __restrict__ xaux,
+                                                          const float4* __restrict__ qaux, const float* __restrict__ q,
+                                                          int nq, BatchWork w, int capq, int k, int rmax, int metric,
+                                                          float cK, float cN, float* __restrict__ D,
+                                                          int64_t* __restrict__ I) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t* sl = reinterpret_cast<uint64_t*>(sm) + static_cast<size_t>(warp) * 512;  // [8][512] selected keys
+    float* qs = reinterpret_cast<float*>(reinterpret_cast<uint64_t*>(sm) + 8 * 512) +
+                static_cast<size_t>(warp) * L.row_pitch;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    const int cnt = w.cand_cnt[qi];
+    const int n = min(cnt, capq);
+    if (cnt > capq || n > 512 || k > 512) {
+        if (lane == 0) w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
+        return;
+    }
+    const float* src = q + static_cast<size_t>(qi) * L.d;
+    for (int i = lane; i < L.row_pitch; i += 32) {
+        int b = 0;
+        while (b + 1 < L.nb && i >= L.boff[b + 1]) ++b;
+        const int j = i - L.boff[b];
+        qs[i] = j < L.bstart[b + 1] - L.bstart[b] ? src[L.bstart[b] + j] : 0.0f;
+    }
+    __syncwarp();
+    const bool l2 = metric == 1;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    const uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
+    float* Dq = D + static_cast<size_t>(qi) * k;
+    int64_t* Iq = I + static_cast<size_t>(qi) * k;
+    const int need = max(n, k);
+    if (need <= 128)
+        rerank_warp_query<4>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+    else if (need <= 256)
+        rerank_warp_query<8>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+    else
+        rerank_warp_query<16>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+}
+
 __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float* __restrict__ codes,
                                                      const int64_t* __restrict__ ids, const float* __restrict__ xn,
                                                      const float2* __restrict__ xaux, const float4* __restrict__ qaux,
@@ -888,7 +1023,11 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
     __shared__ uint32_t sh[2];
     __shared__ int s_nsel, s_over;
     const bool l2 = metric == 1;
-    const int qi = blockIdx.x;
+    // Queries left by the warp re-rank (w.big: count, then ids), a CTA each.
+    const int nbig = w.big[0];
+    for (int li = blockIdx.x; li < nbig; li += gridDim.x) {
+    const int qi = w.big[1 + li];
+    __syncthreads();  // the previous query's shared state is no longer read
     const int cnt = w.cand_cnt[qi];
     const int n = min(cnt, capq);
     const uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
@@ -963,6 +1102,7 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
         }
         D[static_cast<size_t>(qi) * k + i] = dv;
         I[static_cast<size_t>(qi) * k + i] = iv;
+    }
     }
 }
 
@@ -1170,17 +1310,27 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
 
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
-                          int capq, int k, int rmax, int metric, bool f8, float* D, int64_t* I, cudaStream_t s) {
+                          int capq, int k, int rmax, int metric, bool f8, int nsm, float* D, int64_t* I,
+                          cudaStream_t s) {
+    float cK, cN;
+    err_consts(L.d, f8, &cK, &cN);
+    cudaError_t e = cudaMemsetAsync(w.big, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    const size_t wsmem = static_cast<size_t>(8) * (512 * sizeof(uint64_t) + L.row_pitch * sizeof(float));
+    if ((e = cudaFuncSetAttribute(rerank_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(wsmem))) != cudaSuccess)
+        return e;
+    rerank_warp_kernel<<<(nq + 7) / 8, 256, wsmem, s>>>(L, codes, ids, xn, xaux, qaux, q, nq, w, capq, k, rmax, metric,
+                                                        cK, cN, D, I);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t smem = static_cast<size_t>(RERANK_MAX) * 8 + static_cast<size_t>(L.row_pitch) * 4 +
                         static_cast<size_t>(capq) * 8;
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    float cK, cN;
-    err_consts(L.d, f8, &cK, &cN);
-    rerank_kernel<<<nq, 256, smem, s>>>(L, codes, ids, xn, xaux, qaux, q, w, qbase, capq, k, rmax, metric, cK, cN, D,
-                                        I);
+    if ((e = cudaFuncSetAttribute(rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem))) != cudaSuccess)
+        return e;
+    rerank_kernel<<<2 * nsm, 256, smem, s>>>(L, codes, ids, xn, xaux, qaux, q, w, qbase, capq, k, rmax, metric, cK, cN,
+                                             D, I);
     return cudaGetLastError();
 }
 

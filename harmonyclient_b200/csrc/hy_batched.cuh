@@ -55,6 +55,7 @@ struct BatchWork {
     uint64_t* cand;      // [nq*capq]
     int32_t* cand_cnt;   // [nq]
     int32_t* overflow;   // [1 + nq]: count, then query ids
+    int32_t* big;        // [1 + nq]: queries re-ranked by the CTA kernel (count, then ids)
 };
 
 // Inverts probe columns [j0, j1) of every query into per-list query groups
@@ -89,7 +90,8 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
 // can reach the top-k.
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
-                          int capq, int k, int rmax, int metric, bool f8, float* D, int64_t* I, cudaStream_t s);
+                          int capq, int k, int rmax, int metric, bool f8, int nsm, float* D, int64_t* I,
+                          cudaStream_t s);
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s);
 
 // Device-side exact fallback for queries whose candidates overflowed

@@ -183,6 +183,7 @@ struct hy_index {
     DevBuf lscale, tscale, tmax;  // e4m3 per-list and per-tile scales, tile maxima
     bool a8_valid = false;
     DevBuf b_qs;              // e4m3 per-query scales
+    DevBuf b_big;             // queries re-ranked by the CTA kernel
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
     DevBuf b_fq, b_fpr, b_fD, b_fI, b_fcnt, b_fbtot;  // device-side exact fallback
 
@@ -626,6 +627,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
+    HY_RET(h->b_big.ensure((qc + 1) * sizeof(int32_t)));
     // Exact fallback on the device: up to FB_CAP overflowed queries per chunk
     // are searched again by the plain scan over the same probe lists.
     const size_t fbcap = std::min<size_t>(qc, FB_CAP);
@@ -661,6 +663,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     w.work = h->b_work.as<unsigned int>();
     w.cand = h->b_cand.as<uint64_t>();
     w.cand_cnt = h->b_ccnt.as<int32_t>();
+    w.big = h->b_big.as<int32_t>();
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
@@ -734,7 +737,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         const int rmax = f8 ? (int)std::min<size_t>(h->oversample * k, 4096) : 0;
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
                                   f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m,
-                                  w, 0, (int)capq, (int)k, rmax, h->metric, f8, dD + q0 * k, dI + q0 * k, s));
+                                  w, 0, (int)capq, (int)k, rmax, h->metric, f8, h->nsm, dD + q0 * k, dI + q0 * k, s));
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[4], s));
         const int fb = (int)std::min<size_t>(m, fbcap);
         HY_CUDA(hy::launch_fb_gather(w.overflow, qq, h->w_probes.as<int64_t>(), (int)nprobe, (int)h->d, fb,

@@ -162,13 +162,17 @@ __device__ inline void warp_merge(uint64_t (&t)[KR], uint64_t (&c)[KR], int lane
 }
 
 // Key at element index e (warp-uniform e), broadcast to every lane.
+// (Each register is broadcast by its own shuffle and the wanted one kept: a
+// select on e >> 5 would become an indexed access and put t in local memory.)
 template <int KR>
 __device__ inline uint64_t warp_get(const uint64_t (&t)[KR], int e) {
     uint64_t x = 0;
 #pragma unroll
-    for (int r = 0; r < KR; ++r)
-        if (r == (e >> 5)) x = t[r];
-    return __shfl_sync(FULL, x, e & 31);
+    for (int r = 0; r < KR; ++r) {
+        const uint64_t v = __shfl_sync(FULL, t[r], e & 31);
+        if (r == (e >> 5)) x = v;
+    }
+    return x;
 }
 
 }  // namespace hy
