@@ -194,6 +194,7 @@ struct hy_index {
     float margin = 0.0f;
     int model_P = 0;
     DevBuf m_params, m_mu, m_sd, m_X, m_y, m_work, m_pscore, m_total;
+    DevBuf m_wimg;  // the weights' tensor-core operand image (mlp_pack)
     DevBuf t_X, t_t, t_Xb, t_tb, t_dy, t_loss, t_grads, t_am, t_av, t_perm, t_rows, t_D, t_I;
 };
 
@@ -491,23 +492,11 @@ bool batched_form(const hy_index* h) { return h->form == HY_FORM_BF16 || h->form
 // query's nprobe and the probes beyond it become -1.
 int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, int64_t* probes = nullptr) {
     if (!probes) probes = h->w_probes.as<int64_t>();
-    const int B = 8192;
     HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
-    HY_RET(h->m_X.ensure((size_t)B * hy::MLP_IN * sizeof(float)));
-    HY_RET(h->m_y.ensure((size_t)B * sizeof(float)));
-    HY_RET(h->m_work.ensure(hy::mlp_work_floats(B) * sizeof(float)));
-    hy::MlpWork w;
-    hy::mlp_work_bind(w, h->m_work.as<float>(), B);
-    for (size_t r0 = 0; r0 < m; r0 += B) {
-        const int b = (int)std::min<size_t>(B, m - r0);
-        HY_CUDA(hy::launch_probe_features(h->m_pscore.as<float>() + r0 * nprobe, b, (int)nprobe, h->m_mu.as<float>(),
-                                          h->m_sd.as<float>(), h->m_X.as<float>(), s));
-        HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), b, h->m_X.as<float>(), w, h->m_y.as<float>(), s));
-        HY_CUDA(hy::launch_apply_nprobe(h->m_y.as<float>(), b, h->margin, (int)nprobe,
-                                        probes + r0 * nprobe, h->m_total.as<unsigned long long>(),
-                                        s));
-        h->launches += 9;
-    }
+    HY_CUDA(hy::mlp_infer(h->m_pscore.as<float>(), (int)m, (int)nprobe, h->m_mu.as<float>(), h->m_sd.as<float>(),
+                          h->m_wimg.as<unsigned char>(), h->m_params.as<float>(), h->margin, probes,
+                          h->m_total.as<unsigned long long>(), nullptr, h->w_err.as<int>(), s));
+    h->launches += 1;
     return HY_OK;
 }
 
@@ -1270,7 +1259,7 @@ int judge_learned(hy_index* h, size_t n, const float* q, size_t k, float* D, int
 
 // Chunked exact labelling for the probe network: for every query, coarse
 // scores of its P best lists (features) and its stop label.
-int probe_training_data(hy_index* h, size_t n, const float* q, size_t P, size_t kl, float* X, float* lab,
+int probe_training_data(hy_index* h, size_t n, const float* q, size_t P, size_t kl, float* X, float* lab, float* S,
                         cudaStream_t s) {
     const size_t qc = std::min<size_t>(query_chunk(h->nlist, n), 8192);
     HY_RET(ensure_common(h));
@@ -1298,6 +1287,7 @@ int probe_training_data(hy_index* h, size_t n, const float* q, size_t P, size_t 
                                        h->list_off.as<int64_t>(), (int)h->nlist, h->t_t.as<float>(), s));
         HY_CUDA(cudaMemcpyAsync(X + q0 * hy::MLP_IN, h->m_X.p, m * hy::MLP_IN * sizeof(float), cudaMemcpyDeviceToHost, s));
         HY_CUDA(cudaMemcpyAsync(lab + q0, h->t_t.p, m * sizeof(float), cudaMemcpyDeviceToHost, s));
+        HY_CUDA(cudaMemcpyAsync(S + q0 * P, h->m_pscore.p, m * P * sizeof(float), cudaMemcpyDeviceToHost, s));
         HY_CUDA(cudaStreamSynchronize(s));
     }
     return HY_OK;
@@ -1386,8 +1376,8 @@ int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max
     cudaStream_t s = h->stream;
     const size_t P = std::max<size_t>(1, std::min(max_nprobe, h->nlist));
     // 1. features and exact stop labels
-    std::vector<float> X(n * hy::MLP_IN), lab(n);
-    HY_RET(probe_training_data(h, n, q, P, k_label, X.data(), lab.data(), s));
+    std::vector<float> X(n * hy::MLP_IN), lab(n), S(n * P);
+    HY_RET(probe_training_data(h, n, q, P, k_label, X.data(), lab.data(), S.data(), s));
     const size_t ntr = std::max<size_t>(1, n * 9 / 10), nva = n - ntr;
     std::vector<float> t(n);
     for (size_t i = 0; i < n; ++i) t[i] = std::log2(std::max(1.0f, lab[i]));
@@ -1471,16 +1461,22 @@ int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max
     // queries, so that fraction of them gets at least its stop point.
     const size_t nv = nva ? nva : ntr;
     const size_t v0 = nva ? ntr : 0;
+    // Held-out predictions come from the inference kernel the search uses.
     std::vector<float> yv(nv);
-    hy::MlpWork wv;
-    hy::mlp_work_bind(wv, h->m_work.as<float>(), 8192);
-    for (size_t r0 = 0; r0 < nv; r0 += 8192) {
-        const int b = (int)std::min<size_t>(8192, nv - r0);
-        HY_CUDA(hy::mlp_forward(h->m_params.as<float>(), b, h->t_X.as<float>() + (v0 + r0) * hy::MLP_IN, wv,
-                                h->m_y.as<float>(), s));
-        HY_CUDA(cudaMemcpyAsync(yv.data() + r0, h->m_y.p, b * sizeof(float), cudaMemcpyDeviceToHost, s));
-        HY_CUDA(cudaStreamSynchronize(s));
-    }
+    HY_RET(h->m_mu.ensure(hy::MLP_IN * sizeof(float)));
+    HY_RET(h->m_sd.ensure(hy::MLP_IN * sizeof(float)));
+    HY_CUDA(cudaMemcpy(h->m_mu.p, mu.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    HY_CUDA(cudaMemcpy(h->m_sd.p, sd.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
+    HY_RET(h->m_wimg.ensure(hy::mlp_wimg_bytes()));
+    HY_CUDA(hy::mlp_pack(h->m_params.as<float>(), h->m_wimg.as<unsigned char>(), s));
+    HY_RET(h->m_pscore.ensure(nv * P * sizeof(float)));
+    HY_RET(h->m_y.ensure(nv * sizeof(float)));
+    HY_CUDA(cudaMemcpyAsync(h->m_pscore.p, S.data() + v0 * P, nv * P * sizeof(float), cudaMemcpyHostToDevice, s));
+    HY_CUDA(hy::mlp_infer(h->m_pscore.as<float>(), (int)nv, (int)P, h->m_mu.as<float>(), h->m_sd.as<float>(),
+                          h->m_wimg.as<unsigned char>(), h->m_params.as<float>(), 0.0f, nullptr, nullptr,
+                          h->m_y.as<float>(), h->w_err.as<int>(), s));
+    HY_CUDA(cudaMemcpyAsync(yv.data(), h->m_y.p, nv * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
     std::vector<float> resid(nv);
     for (size_t i = 0; i < nv; ++i) resid[i] = t[v0 + i] - yv[i];
     std::vector<float> sorted = resid;
@@ -1496,10 +1492,6 @@ int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max
     }
     h->margin = margin;
     h->model_P = (int)P;
-    HY_RET(h->m_mu.ensure(hy::MLP_IN * sizeof(float)));
-    HY_RET(h->m_sd.ensure(hy::MLP_IN * sizeof(float)));
-    HY_CUDA(cudaMemcpy(h->m_mu.p, mu.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
-    HY_CUDA(cudaMemcpy(h->m_sd.p, sd.data(), hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
     h->model_ready = true;
     if (report) {
         report[0] = (float)last_loss;
@@ -1549,6 +1541,9 @@ int hy_index_set_probe_model(hy_index* h, const float* in) {
     HY_CUDA(cudaMemcpy(h->m_sd.p, in + hy::MLP_NPARAM + hy::MLP_IN, hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
     h->margin = in[hy::MLP_NPARAM + 2 * hy::MLP_IN];
     h->model_P = (int)in[hy::MLP_NPARAM + 2 * hy::MLP_IN + 1];
+    HY_RET(h->m_wimg.ensure(hy::mlp_wimg_bytes()));
+    HY_CUDA(hy::mlp_pack(h->m_params.as<float>(), h->m_wimg.as<unsigned char>(), nullptr));
+    HY_CUDA(cudaDeviceSynchronize());
     h->model_ready = true;
     return HY_OK;
 }

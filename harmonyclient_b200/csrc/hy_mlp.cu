@@ -17,6 +17,7 @@
 
 #include "../../include/hy.h"
 #include "hy_mlp.cuh"
+#include "hy_tc.cuh"
 
 namespace hy {
 namespace {
@@ -143,6 +144,171 @@ __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __res
     p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the tensor cores.  The weights are packed once (mlp_pack) into
+// the tcgen05 B-operand image: W1 as 256 rows (output features) x 64 inputs,
+// one 128-byte-swizzled K-major k-block of 32 KiB; W2 as 256 rows x 256
+// inputs, four such k-blocks.  One CTA of 128 threads takes 128 queries
+// (thread = query = TMEM lane): features -> bf16 A tile -> MMA (M 128, N 256,
+// K 64) -> bias + GELU -> bf16 A tiles (4 k-blocks) -> MMA (K 256) -> bias +
+// GELU -> dot with W3 -> nprobe, all on chip.
+constexpr int MI_WIMG = 32768 + 4 * 32768;   // packed W1 + W2 bytes
+constexpr int MI_SMEM = 1024 + 65536 + MI_WIMG;  // alignment slack, A tiles, weights
+
+__global__ void mlp_pack_kernel(const float* __restrict__ params, unsigned char* __restrict__ wimg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MLP_IN * MLP_H) {
+        const int k = i / MLP_H, n = i % MLP_H;  // W1[k][n]
+        *reinterpret_cast<__nv_bfloat16*>(wimg + tc::kblock_offset(n, k)) = __float2bfloat16_rn(params[MLP_W1 + i]);
+    } else if (i < MLP_IN * MLP_H + MLP_H * MLP_H) {
+        const int j = i - MLP_IN * MLP_H;
+        const int k = j / MLP_H, n = j % MLP_H;  // W2[k][n]
+        *reinterpret_cast<__nv_bfloat16*>(wimg + 32768 + (k >> 6) * 32768 + tc::kblock_offset(n, k & 63)) =
+            __float2bfloat16_rn(params[MLP_W2 + j]);
+    }
+}
+
+// 8 consecutive values as bf16 into one 16-byte chunk.
+__device__ inline uint4 pack8_bf16(const float* v) {
+    uint4 r;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&r);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        w[i] = *reinterpret_cast<const uint32_t*>(&b);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
+                                                           const float* __restrict__ mu, const float* __restrict__ sd,
+                                                           const unsigned char* __restrict__ wimg,
+                                                           const float* __restrict__ params, float margin,
+                                                           int64_t* __restrict__ probes,
+                                                           unsigned long long* __restrict__ total,
+                                                           float* __restrict__ yout, int* err) {
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = base;             // 4 k-blocks x 128 rows x 128 B: X in k-block 0, then H1
+    unsigned char* sW = base + 65536;     // W1 image (32 KiB) then W2 image (128 KiB)
+    __shared__ uint64_t bar_w, bar_m;
+    __shared__ uint32_t tbase;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = blockIdx.x * 128 + tid;
+    const bool valid = row < m;
+    if (tid == 0) {
+        mbar_init(&bar_w, 1);
+        mbar_init(&bar_m, 1);
+        fence_mbar_init();
+        s_ok = 1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&bar_w, MI_WIMG);
+        for (int c = 0; c < MI_WIMG / 16384; ++c) bulk_g2s(sW + c * 16384, wimg + c * 16384, 16384, &bar_w);
+    }
+    if (warp == 0) tc::tmem_alloc(&tbase, 256);
+    // Features of this thread's query (its P best coarse scores), standardised,
+    // as bf16 row `tid` of the A tile.
+    {
+        const float* sc = pscore + static_cast<size_t>(valid ? row : 0) * P;
+        const float s0 = valid ? sc[0] : 0.0f;
+        const float a0 = fabsf(s0) + 1e-6f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float f[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int i = 8 * c + j;
+                const float v = i == 0 ? logf(a0) : log1pf(fmaxf(sc[min(i, P - 1)] - s0, 0.0f) / a0);
+                f[j] = valid ? (v - mu[i]) / sd[i] : 0.0f;
+            }
+            *reinterpret_cast<uint4*>(sA + tid * 128 + (((c ^ (tid & 7)) & 7) << 4)) = pack8_bf16(f);
+        }
+    }
+    fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tbase;
+    const uint32_t idesc = tc::idesc_bf16_f32(128, 256);
+    if (tid == 0) {
+        if (!mbar_wait_bounded(&bar_w, 0, err)) {
+            s_ok = 0;
+        } else {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+                tc::mma_bf16(tmem, tc::sdesc_sw128(smem_u32(sA) + kk * 32), tc::sdesc_sw128(smem_u32(sW) + kk * 32),
+                             idesc, kk != 0 ? 1u : 0u);
+            tc::mma_commit(&bar_m);
+        }
+    }
+    __syncthreads();
+    bool ok = s_ok != 0 && mbar_wait_bounded(&bar_m, 0, err);
+    tc::fence_after_sync();
+    const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    if (ok) {
+        // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks.
+        for (int cb = 0; cb < 4; ++cb) {
+            uint32_t u[64];
+            tc::tmem_ld64(lane_addr + cb * 64, u);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                float h[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    h[j] = gelu(__uint_as_float(u[8 * c + j]) + __ldg(params + MLP_B1 + cb * 64 + 8 * c + j));
+                *reinterpret_cast<uint4*>(sA + cb * 16384 + tid * 128 + (((c ^ (tid & 7)) & 7) << 4)) = pack8_bf16(h);
+            }
+        }
+    }
+    fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0 && ok) {
+        for (int kb = 0; kb < 4; ++kb)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+                tc::mma_bf16(tmem, tc::sdesc_sw128(smem_u32(sA + kb * 16384) + kk * 32),
+                             tc::sdesc_sw128(smem_u32(sW + 32768 + kb * 32768) + kk * 32), idesc,
+                             (kb | kk) != 0 ? 1u : 0u);
+        tc::mma_commit(&bar_m);
+    }
+    __syncthreads();
+    ok = ok && mbar_wait_bounded(&bar_m, 1, err);
+    tc::fence_after_sync();
+    if (ok) {
+        // Layer 2 epilogue and layer 3: y = bf16(GELU(Z2 + b2)) . bf16(W3) + b3.
+        float acc = 0.0f;
+        for (int cb = 0; cb < 4; ++cb) {
+            uint32_t u[64];
+            tc::tmem_ld64(lane_addr + cb * 64, u);
+#pragma unroll
+            for (int j = 0; j < 64; ++j) {
+                const int n = cb * 64 + j;
+                const float a = gelu(__uint_as_float(u[j]) + __ldg(params + MLP_B2 + n));
+                acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
+            }
+        }
+        const float y = acc + params[MLP_B3];
+        if (valid) {
+            if (yout) yout[row] = y;
+            if (probes) {
+                int np = static_cast<int>(ceilf(exp2f(fminf(y + margin, 30.0f))));
+                np = max(1, min(P, np));
+                for (int j = np; j < P; ++j) probes[static_cast<int64_t>(row) * P + j] = -1;
+                atomicAdd(total, static_cast<unsigned long long>(np));
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
 inline int blocks(int64_t n, int t) { return static_cast<int>((n + t - 1) / t); }
 
 template <bool TA, bool TB>
@@ -211,6 +377,24 @@ cudaError_t mlp_adam(float* params, const float* grads, float* m, float* v, int 
     const float c1 = 1.0f - std::pow(b1, static_cast<float>(step));
     const float c2 = 1.0f - std::pow(b2, static_cast<float>(step));
     adam_kernel<<<blocks(MLP_NPARAM, 256), 256, 0, s>>>(MLP_NPARAM, params, grads, m, v, lr, b1, b2, 1e-8f, c1, c2);
+    return cudaGetLastError();
+}
+
+size_t mlp_wimg_bytes() { return MI_WIMG; }
+
+cudaError_t mlp_pack(const float* params, unsigned char* wimg, cudaStream_t s) {
+    mlp_pack_kernel<<<blocks(MLP_IN * MLP_H + MLP_H * MLP_H, 256), 256, 0, s>>>(params, wimg);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_infer(const float* pscore, int m, int P, const float* mu, const float* sd, const unsigned char* wimg,
+                      const float* params, float margin, int64_t* probes, unsigned long long* total, float* yout,
+                      int* err, cudaStream_t s) {
+    if (m <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MI_SMEM);
+    if (e != cudaSuccess) return e;
+    mlp_infer_kernel<<<blocks(m, 128), 128, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin, probes, total,
+                                                         yout, err);
     return cudaGetLastError();
 }
 

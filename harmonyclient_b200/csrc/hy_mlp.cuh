@@ -29,4 +29,16 @@ cudaError_t mlp_backward(const float* params, int B, const float* X, MlpWork& w,
 cudaError_t mlp_mse(int B, const float* y, const float* t, float* dy, float* loss, cudaStream_t s);
 cudaError_t mlp_adam(float* params, const float* grads, float* m, float* v, int step, float lr, cudaStream_t s);
 
+// Tensor-core inference.  mlp_pack writes the weights' bf16 operand image
+// (mlp_wimg_bytes() bytes) from the parameter vector; mlp_infer computes, for
+// m queries with their P best coarse scores (pscore, m x P, best first), the
+// standardised features, the network output y (into yout when given) and,
+// when probes (m x P) is given, cuts each query's probes past
+// clamp(ceil(2^(y + margin)), 1, P) to -1 and adds the kept counts to *total.
+size_t mlp_wimg_bytes();
+cudaError_t mlp_pack(const float* params, unsigned char* wimg, cudaStream_t s);
+cudaError_t mlp_infer(const float* pscore, int m, int P, const float* mu, const float* sd, const unsigned char* wimg,
+                      const float* params, float margin, int64_t* probes, unsigned long long* total, float* yout,
+                      int* err, cudaStream_t s);
+
 }  // namespace hy
