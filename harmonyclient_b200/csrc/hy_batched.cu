@@ -822,9 +822,13 @@ __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ 
     __shared__ uint32_t sh[2];
     __shared__ int s_m;
     const bool l2 = metric == 1;
-    const int qi = blockIdx.x;
+    // Queries left by the warp kernel (w.big: count, then ids), a CTA each.
+    const int nbig = w.big[0];
+    for (int li = blockIdx.x; li < nbig; li += gridDim.x) {
+    const int qi = w.big[1 + li];
+    __syncthreads();  // the previous query's shared state is no longer read
     const int cnt = w.cand_cnt[qi];
-    if (cnt < k || cnt > capq) return;
+    if (cnt < k || cnt > capq) continue;
     const int n = cnt;
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
@@ -858,6 +862,68 @@ __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ 
     __syncthreads();
     if (threadIdx.x == 0) {
         w.cand_cnt[qi] = s_m;
+        if (U < thr[qi]) thr[qi] = U;
+    }
+    }
+}
+
+// Warp tighten: one warp per query with at most 1024 candidates (32 per
+// lane in registers); larger buffers go to the CTA kernel through w.big.
+constexpr int TIGHTEN_WARP_MAX = 1024;
+
+__global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restrict__ xn,
+                                                           const float2* __restrict__ xaux,
+                                                           const float4* __restrict__ qaux, int nq, BatchWork w,
+                                                           int capq, int k, int metric, float cK, float cN,
+                                                           float* __restrict__ thr) {
+    __shared__ int hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    const int cnt = w.cand_cnt[qi];
+    if (cnt < k) return;
+    if (cnt > capq) return;  // overflowed: left for the re-rank to report
+    if (cnt > TIGHTEN_WARP_MAX) {
+        if (lane == 0) w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
+        return;
+    }
+    constexpr int PER = TIGHTEN_WARP_MAX / 32;
+    const bool l2 = metric == 1;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
+    uint32_t hi[PER];
+    float lo[PER];
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        hi[r] = 0xffffffffu;
+        lo[r] = INFINITY;
+        if (e < cnt) {
+            const uint64_t key = cq[e];
+            const int64_t row = static_cast<int64_t>(key & 0xffffffffu);
+            const float2 xa = xaux[row];
+            const float eb = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+            const float sc = o2f(static_cast<uint32_t>(key >> 32));
+            hi[r] = f2o(sc + eb);
+            lo[r] = sc - eb;
+        }
+    }
+    const float U = o2f(warp_radix_select<PER>(hi, cnt, k, hist[warp], lane));
+    // In-place compaction of the candidates that can still enter the top-k:
+    // every element of a round is read before any of that round's writes.
+    int m = 0;
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        const bool keep = e < cnt && lo[r] <= U;
+        const uint64_t key = e < cnt ? cq[e] : 0;
+        const unsigned b = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep) cq[m + __popc(b & ((1u << lane) - 1u))] = key;
+        m += __popc(b);
+    }
+    if (lane == 0) {
+        w.cand_cnt[qi] = m;
         if (U < thr[qi]) thr[qi] = U;
     }
 }
@@ -1170,14 +1236,18 @@ static void err_consts(int d, bool f8, float* cK, float* cN) {
 }
 
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, bool f8, float* thr, cudaStream_t s) {
-    const size_t smem = static_cast<size_t>(capq) * 8;
-    cudaError_t e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
+                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s) {
     float cK, cN;
     err_consts(d, f8, &cK, &cN);
-    tighten_kernel<<<nq, 256, smem, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
+    cudaError_t e = cudaMemsetAsync(w.big, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const size_t smem = static_cast<size_t>(capq) * 8;
+    if ((e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem))) != cudaSuccess)
+        return e;
+    tighten_kernel<<<2 * nsm, 256, smem, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
     return cudaGetLastError();
 }
 

@@ -64,7 +64,7 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
                                  const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s);
 // thr := min(thr, k-th smallest upper bound over each query's candidates).
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, bool f8, float* thr, cudaStream_t s);
+                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s);
 
 struct BatchedLaunch {
     const void* abf;

@@ -714,7 +714,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         if (nprobe > 1) {
             HY_CUDA(hy::launch_tighten(h->norms.as<float>(), f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(),
                                        h->b_qn.as<float4>(), (int)m, w, (int)capq, (int)k, h->metric, (int)h->d, f8,
-                                       h->b_thr.as<float>(), s));
+                                       h->nsm, h->b_thr.as<float>(), s));
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
                                              (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
             if (last) HY_CUDA(ev_record(h->ev[8], s));

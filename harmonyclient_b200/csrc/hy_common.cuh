@@ -147,6 +147,63 @@ __device__ inline void cta_bitonic_sort(uint64_t* a, int P) {
     }
 }
 
+// k-th smallest of the warp's values v (lane l holds elements r*32 + l, valid
+// below n): four 8-bit radix passes over a per-warp 256-bin histogram.
+template <int PER>
+__device__ inline uint32_t warp_radix_select(const uint32_t (&v)[PER], int n, int k, int* hist, int lane) {
+    uint32_t prefix = 0, mask = 0;
+    int rem = k;
+#pragma unroll 1
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < PER; ++r)
+            if (r * 32 + lane < n && (v[r] & mask) == prefix) atomicAdd(&hist[(v[r] >> shift) & 255u], 1);
+        __syncwarp();
+        int loc[8], sum = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            loc[i] = hist[lane * 8 + i];
+            sum += loc[i];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - sum;
+        const bool mine = excl < rem && incl >= rem;
+        int digit = 0, before = 0;
+        if (mine) {
+            int cum = excl;
+            digit = lane * 8 + 7;
+            before = excl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (cum + loc[i] >= rem) {
+                    digit = lane * 8 + i;
+                    before = cum;
+                    break;
+                }
+                cum += loc[i];
+            }
+        }
+        const unsigned who = __ballot_sync(FULL, mine);
+        const int src = __ffs(who) - 1;
+        digit = __shfl_sync(FULL, digit, src);
+        before = __shfl_sync(FULL, before, src);
+        prefix |= static_cast<uint32_t>(digit) << shift;
+        mask |= 0xffu << shift;
+        rem -= before;
+        __syncwarp();
+    }
+    return prefix;
+}
+
 __host__ __device__ inline int next_pow2(int x) {
     int p = 1;
     while (p < x) p <<= 1;

@@ -104,6 +104,66 @@ __global__ void __launch_bounds__(256) select_kernel(const float* __restrict__ s
     }
 }
 
+// Warp version of select_kernel (one warp per row) for rows of at most
+// 32*SPER values and m <= 256: the m-th smallest ordered key by a warp radix
+// select, every smaller element plus the lowest-column equal ones collected
+// through a per-warp shared list, then a register bitonic sort.  Same result
+// as select_kernel.
+template <int SPER>
+__global__ void __launch_bounds__(256) select_warp_kernel(const float* __restrict__ scores, int nrows, int n, int m,
+                                                          int64_t* __restrict__ out_idx,
+                                                          float* __restrict__ out_score) {
+    __shared__ int hist[8][256];
+    __shared__ uint64_t list[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
+    if (row >= nrows) return;  // whole warp
+    const float* src = scores + row * n;
+    uint32_t v[SPER];
+#pragma unroll
+    for (int r = 0; r < SPER; ++r) {
+        const int e = r * 32 + lane;
+        v[r] = e < n ? f2o(src[e]) : 0xffffffffu;
+    }
+    const uint32_t vstar = warp_radix_select<SPER>(v, n, m, hist[warp], lane);
+    int less = 0;
+#pragma unroll
+    for (int r = 0; r < SPER; ++r) less += (r * 32 + lane < n && v[r] < vstar) ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) less += __shfl_xor_sync(FULL, less, o);
+    int need = m - less;  // equal elements to take, lowest columns first
+    int pos = 0;
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < SPER; ++r) {
+        const int e = r * 32 + lane;
+        const bool lt = e < n && v[r] < vstar;
+        const bool eq = e < n && v[r] == vstar;
+        const unsigned be = __ballot_sync(FULL, eq);
+        const bool take = lt || (eq && __popc(be & below) < need);
+        need -= min(__popc(be), max(need, 0));
+        const unsigned bt = __ballot_sync(FULL, take);
+        if (take) list[warp][pos + __popc(bt & below)] = (static_cast<uint64_t>(v[r]) << 32) | static_cast<uint32_t>(e);
+        pos += __popc(bt);
+    }
+    __syncwarp();
+    uint64_t kk[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = r * 32 + lane;
+        kk[r] = e < m ? list[warp][e] : KEY_MAX;
+    }
+    warp_sort<8>(kk, lane);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = r * 32 + lane;
+        if (e < m) {
+            out_idx[row * m + e] = static_cast<int64_t>(kk[r] & 0xffffffffu);
+            if (out_score) out_score[row * m + e] = o2f(static_cast<uint32_t>(kk[r] >> 32));
+        }
+    }
+}
+
 // Per row: the first minimum (lowest column among equal minima), one warp per
 // row — the reference's nearest-centroid rule (strict < in column order,
 // src/IVFScan.hpp:131, src/Clustering.cpp:107).
@@ -185,6 +245,73 @@ __global__ void __launch_bounds__(256) warmup_kernel(ArenaLayout L, const float*
         thr = o2f(v);
     }
     if (threadIdx.x == 0) {
+        out_thr[qi] = f2o(thr);
+        if (out_f) out_f[qi] = thr;
+    }
+}
+
+// Warp version of warmup_kernel (one warp per query) for at most 32 warm-up
+// lists and 1024 warm-up rows: the same distances (row_l2_global), the k-th
+// by a warp radix select.
+__global__ void __launch_bounds__(256) warmup_warp_kernel(const __grid_constant__ ArenaLayout L,
+                                                          const float* __restrict__ codes,
+                                                          const int64_t* __restrict__ list_off,
+                                                          const int32_t* __restrict__ list_size,
+                                                          const float* __restrict__ q,
+                                                          const int64_t* __restrict__ probes, int nq, int nprobe,
+                                                          int k, int wl, int wls, int blockwise,
+                                                          uint32_t* __restrict__ out_thr, float* __restrict__ out_f) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ int hist[8][256];
+    __shared__ int s_base[8][33];
+    __shared__ int64_t s_r0[8][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    float* qs = reinterpret_cast<float*>(sm) + static_cast<size_t>(warp) * L.row_pitch;
+    const float* src = q + static_cast<size_t>(qi) * L.d;
+    for (int i = lane; i < L.row_pitch; i += 32) {
+        int b = 0;
+        while (b + 1 < L.nb && i >= L.boff[b + 1]) ++b;
+        const int j = i - L.boff[b];
+        qs[i] = j < L.bstart[b + 1] - L.bstart[b] ? src[L.bstart[b] + j] : 0.0f;
+    }
+    const int wle = min(wl, nprobe);
+    int cnt = 0;
+    int64_t r0 = 0;
+    if (lane < wle) {
+        const int64_t l = probes[static_cast<size_t>(qi) * nprobe + lane];
+        if (l >= 0) {
+            cnt = min(wls, static_cast<int>(list_size[l]));
+            r0 = list_off[l];
+        }
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    s_base[warp][lane] = incl - cnt;
+    s_r0[warp][lane] = r0;
+    const int total = __shfl_sync(FULL, incl, 31);
+    if (lane == 0) s_base[warp][32] = total;
+    __syncwarp();
+    uint32_t v[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        const int i = r * 32 + lane;
+        v[r] = 0xffffffffu;
+        if (i < total) {
+            int j = 0;
+            while (s_base[warp][j + 1] <= i) ++j;
+            const int64_t row = s_r0[warp][j] + (i - s_base[warp][j]);
+            v[r] = f2o(row_l2_global(L, codes, row, qs, blockwise != 0));
+        }
+    }
+    float thr = FLT_MAX;
+    if (total >= k) thr = o2f(warp_radix_select<32>(v, total, k, hist[warp], lane));
+    if (lane == 0) {
         out_thr[qi] = f2o(thr);
         if (out_f) out_f[qi] = thr;
     }
@@ -732,12 +859,17 @@ cudaError_t launch_coarse_scores(const float* q, int nq, const float* cent, int 
 
 cudaError_t launch_select(const float* scores, int nq, int n, int m, int64_t* out_idx, float* out_score,
                           cudaStream_t s) {
-    const size_t smem = static_cast<size_t>(next_pow2(m)) * 8 + static_cast<size_t>(n) * 4;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured = true;
+    if (m <= 256 && n <= 1024) {
+        select_warp_kernel<32><<<(nq + 7) / 8, 256, 0, s>>>(scores, nq, n, m, out_idx, out_score);
+        return cudaGetLastError();
     }
+    if (m <= 256 && n <= 2048) {
+        select_warp_kernel<64><<<(nq + 7) / 8, 256, 0, s>>>(scores, nq, n, m, out_idx, out_score);
+        return cudaGetLastError();
+    }
+    const size_t smem = static_cast<size_t>(next_pow2(m)) * 8 + static_cast<size_t>(n) * 4;
+    cudaError_t e = cudaFuncSetAttribute(select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
     select_kernel<<<nq, 256, smem, s>>>(scores, n, m, out_idx, out_score);
     return cudaGetLastError();
 }
@@ -754,13 +886,21 @@ cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_
                           int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s) {
     (void)err;
     const int wle = wl < nprobe ? wl : nprobe;
+    cudaError_t e;
+    if (wle <= 32 && static_cast<int64_t>(wle) * wls <= 1024) {
+        const size_t wsmem = static_cast<size_t>(8) * L.row_pitch * 4;
+        if ((e = cudaFuncSetAttribute(warmup_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(wsmem))) != cudaSuccess)
+            return e;
+        warmup_warp_kernel<<<(nq + 7) / 8, 256, wsmem, s>>>(L, codes, list_off, list_size, q, probes, nq, nprobe, k,
+                                                            wl, wls, blockwise, out_thr, out_f);
+        return cudaGetLastError();
+    }
     const size_t smem = static_cast<size_t>(L.row_pitch) * 4 + static_cast<size_t>((wl + 2) & ~1) * 4 +
                         static_cast<size_t>(wl) * 8 + static_cast<size_t>(wle) * wls * 4;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(warmup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured = true;
-    }
+    if ((e = cudaFuncSetAttribute(warmup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
+        cudaSuccess)
+        return e;
     warmup_kernel<<<nq, 256, smem, s>>>(L, codes, list_off, list_size, q, probes, nprobe, k, wl, wls, blockwise,
                                         out_thr, out_f);
     return cudaGetLastError();
