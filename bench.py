@@ -112,24 +112,43 @@ class Clocks:
 
 # The measured workloads (seeded synthetic stand-ins of the named shapes).
 WORKLOADS = {
-    "c2": dict(gen="gmm_uint8", d=128, nlist=1024, k=100,
+    "c2": dict(gen="gmm_uint8", kw={}, d=128, nlist=1024, k=100, nb=1_000_000, nq=10_000, nprobe=64,
                desc="{nb} x 128 uint8-valued gmm (4096 components, sigma 20)",
                data="synthetic (seeded Gaussian mixture, integer-valued in [0,255])"),
-    "c3": dict(gen="gmm_dense", d=420, nlist=2048, k=10,
+    "c3": dict(gen="gmm_dense", kw={}, d=420, nlist=2048, k=10, nb=1_000_000, nq=10_000, nprobe=64,
                desc="{nb} x 420 float gmm (2048 components, per-dim mean U[-1,1], sigma 0.3)",
                data="synthetic (seeded Gaussian mixture, float32)"),
+    # Zipf(1.1)-weighted components give skewed list sizes; every query has its
+    # own nprobe drawn U[8,128] (seeded), searched through search_nprobes.
+    "c4": dict(gen="gmm_uint8", kw={"ncomp": 16_384, "zipf": 1.1}, d=128, nlist=16_384, k=10, nb=10_000_000,
+               nq=65_536, nprobe=128, per_query=(8, 128), cpu_ref=False,
+               desc="{nb} x 128 uint8-valued gmm (16384 components weighted Zipf(1.1)), per-query nprobe U[8,128]",
+               data="synthetic (seeded Zipf-weighted Gaussian mixture, integer-valued in [0,255])"),
+    "c5": dict(gen="sparse_nonneg", kw={}, d=500, nlist=4096, k=10, nb=2_000_000, nq=20_000, nprobe=256, cpu_ref=False,
+               desc="{nb} x 500 sparse non-negative L2-normalised (2048 components, 10% support, Exp(1))",
+               data="synthetic (seeded sparse non-negative mixture, float32)"),
 }
 
 
 def queries(args, n, query_seed):
     """Another query set from the workload's mixture."""
     from harmonyclient_b200 import datasets
-    return getattr(datasets, WORKLOADS[args.workload]["gen"])(0, n, seed=0, query_seed=query_seed)[1]
+    W = WORKLOADS[args.workload]
+    return getattr(datasets, W["gen"])(0, n, seed=0, query_seed=query_seed, **W["kw"])[1]
+
+
+def per_query_nprobe(args, nq):
+    """The workload's per-query nprobe (None when it uses one nprobe)."""
+    lo_hi = WORKLOADS[args.workload].get("per_query")
+    if lo_hi is None:
+        return None
+    return np.random.default_rng(1).integers(lo_hi[0], lo_hi[1] + 1, size=nq).astype(np.int32)
 
 
 def workload(args, rank):
     from harmonyclient_b200 import datasets
-    x, q = getattr(datasets, WORKLOADS[args.workload]["gen"])(args.nb, args.nq, seed=0)
+    W = WORKLOADS[args.workload]
+    x, q = getattr(datasets, W["gen"])(args.nb, args.nq, seed=0, **W["kw"])
     if rank:
         # Other ranks search their own queries from the same mixture.
         q = queries(args, args.nq, 1000 + rank)
@@ -159,7 +178,17 @@ def cpu_baseline_ref(x, q, cent, nprobe, k, budget_s):
             "sample": f"{m2} of {q.shape[0]} queries, reference Index::search ORIGINAL mode, OpenMP x{nt}"}
 
 
-def _time_device(idx, dq, dD, dI, k, steps, ts, dist, dev):
+def _search(idx, dq, dD, dI, k, ts, npq=None):
+    """One device-pointer search on stream ts; npq = (device per-query
+    nprobe tensor, its maximum) for the per-query workloads."""
+    if npq is None:
+        idx.search_device(dq.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), ts.cuda_stream)
+    else:
+        idx.search_nprobes_device(dq.shape[0], dq.data_ptr(), k, npq[0].data_ptr(), npq[1], dD.data_ptr(),
+                                  dI.data_ptr(), ts.cuda_stream)
+
+
+def _time_device(idx, dq, dD, dI, k, steps, ts, dist, dev, npq=None):
     """Device-timed loop of `steps` batch searches (CUDA events on the
     launching stream `ts`, max over ranks); the last step's stats come back."""
     import torch
@@ -172,7 +201,7 @@ def _time_device(idx, dq, dD, dI, k, steps, ts, dist, dev):
         torch.cuda.nvtx.range_push("timed")  # profilers select the timed launches by this range
         e0.record(ts)
         for _ in range(steps):
-            idx.search_device(n, dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), ts.cuda_stream)
+            _search(idx, dq, dD, dI, k, ts, npq)
         e1.record(ts)
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
@@ -184,14 +213,14 @@ def _time_device(idx, dq, dD, dI, k, steps, ts, dist, dev):
     return float(t.item()), st, clk.summary()
 
 
-def _kernel_ms(idx, dq, dD, dI, k, reps, ts):
+def _kernel_ms(idx, dq, dD, dI, k, reps, ts, npq=None):
     """Average duration of the dominant scan kernel's launches: every
     launch is bracketed by CUDA events on its own stream inside the library;
     `reps` further searches, each read back."""
     import torch
     tot, launches = 0.0, 0
     for _ in range(reps):
-        idx.search_device(dq.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), ts.cuda_stream)
+        _search(idx, dq, dD, dI, k, ts, npq)
         st = idx.last_stats()
         tot += st["kernel_ms"]
         launches += st["kernel_launches"]
@@ -252,17 +281,19 @@ def run_ours(args, rank, world, dist):
 
     stream = torch.cuda.Stream()  # the launching stream of every timed search
     dq = torch.from_numpy(q).cuda()
+    npq_host = per_query_nprobe(args, q.shape[0])
+    npq = None if npq_host is None else (torch.from_numpy(npq_host).cuda(), int(npq_host.max()))
     dD = torch.empty((q.shape[0], k), dtype=torch.float32, device="cuda")
     dI = torch.empty((q.shape[0], k), dtype=torch.int64, device="cuda")
     idx.set_graph(args.graph)
     for _ in range(args.warmup):
-        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream.cuda_stream)
+        _search(idx, dq, dD, dI, k, stream, npq)
     torch.cuda.synchronize()
-    ms_max, st_dev, clocks = _time_device(idx, dq, dD, dI, k, args.steps, stream, dist, dev)
+    ms_max, st_dev, clocks = _time_device(idx, dq, dD, dI, k, args.steps, stream, dist, dev, npq)
     value = world * q.shape[0] * args.steps / (ms_max / 1e3)
     I_main = dI.cpu().numpy()
     D_main = dD.cpu().numpy()
-    kern_ms, kern_per_search = _kernel_ms(idx, dq, dD, dI, k, 3, stream)
+    kern_ms, kern_per_search = _kernel_ms(idx, dq, dD, dI, k, 3, stream, npq)
 
     # End to end through the public host API: pinned host queries in, results
     # back to pinned host memory, every step (with the learned form this
@@ -273,8 +304,13 @@ def run_ours(args, rank, world, dist):
     L = _lib.load()
 
     def e2e_step():
-        _lib.check(L.hy_index_search(idx._h, q.shape[0], C.c_void_p(hq.data_ptr()), k, C.c_void_p(hD.data_ptr()),
-                                     C.c_void_p(hI.data_ptr())))
+        if npq_host is None:
+            _lib.check(L.hy_index_search(idx._h, q.shape[0], C.c_void_p(hq.data_ptr()), k, C.c_void_p(hD.data_ptr()),
+                                         C.c_void_p(hI.data_ptr())))
+        else:
+            _lib.check(L.hy_index_search_nprobes(idx._h, q.shape[0], C.c_void_p(hq.data_ptr()), k,
+                                                 C.c_void_p(npq_host.ctypes.data), C.c_void_p(hD.data_ptr()),
+                                                 C.c_void_p(hI.data_ptr())))
 
     e2e_step()
     if dist:
@@ -301,13 +337,15 @@ def run_ours(args, rank, world, dist):
     # fraction.
     plain = None
     P_main = idx.probes(q)
+    if npq_host is not None:
+        P_main[np.arange(P_main.shape[1])[None, :] >= npq_host[:, None]] = -1
     if base != "plain" and args.plain_steps > 0:
         if learned:
             idx.set_learned(False)
         idx.set_form("plain")
-        idx.search_device(q.shape[0], dq.data_ptr(), k, dD.data_ptr(), dI.data_ptr(), stream.cuda_stream)
-        pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev)
-        pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream)
+        _search(idx, dq, dD, dI, k, stream, npq)
+        pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev, npq)
+        pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream, npq)
         plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "D": dD.cpu().numpy(), "clocks": pclk}
         idx.set_form(base)
         if learned:
@@ -367,6 +405,8 @@ def run_ours(args, rank, world, dist):
         if learned:
             idx.set_learned(False)
         P_plain = idx.probes(q)
+        if npq_host is not None:
+            P_plain[np.arange(P_plain.shape[1])[None, :] >= npq_host[:, None]] = -1
         prow = pair_rows(P_plain)
         palg = prow * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
         pach = palg / (plain["kernel_ms"] / 1e3) / 1e9
@@ -384,7 +424,12 @@ def run_ours(args, rank, world, dist):
                                    "algorithmic_bytes": palg},
                       "clocks": plain["clocks"]}
 
-    cpu = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
+    if W.get("cpu_ref", True):
+        cpu = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
+    else:
+        cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(), "kind": "reference",
+               "unavailable": "the reference's host add() of this base (nearest of nlist centroids for every row) "
+                              "alone takes far longer than the bench's time bound on the host cores"}
     h2d = q.nbytes
     d2h = q.shape[0] * k * 12
     scan_name = {"bf16": "bf16 tcgen05 scan + exact FP32 re-rank",
@@ -446,6 +491,9 @@ def run_reference(args, rank):
     from oracle import ref
     if not ref.available():
         return {"impl": "reference", "unavailable": "reference library oracle/_ref not built"}
+    if not WORKLOADS[args.workload].get("cpu_ref", True):
+        return {"impl": "reference", "unavailable": f"workload {args.workload}: the reference's host add() of this "
+                                                    "base takes far longer than the bench's time bound"}
     x, q = workload(args, 0)
     nt = os.cpu_count() or 1
     ref.set_threads(nt)
@@ -485,7 +533,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nprobe", type=int, default=64)
+    ap.add_argument("--nprobe", type=int, default=None, help="default: the workload's (c4: the per-query maximum)")
     ap.add_argument("--warmup-list", type=int, default=10)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--form", default="learned", choices=["learned", "bf16", "fp8", "plain"])
@@ -499,12 +547,16 @@ def main():
     ap.add_argument("--judge-fraction", type=float, default=0.01)
     ap.add_argument("--no-graph", dest="graph", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
-    ap.add_argument("--nb", type=int, default=1_000_000)
-    ap.add_argument("--nq", type=int, default=10_000)
+    ap.add_argument("--nb", type=int, default=None, help="default: the workload's")
+    ap.add_argument("--nq", type=int, default=None, help="default: the workload's")
     ap.add_argument("--recall-sample", type=int, default=0, help="queries scored for recall (0: all)")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=5.0)
     args = ap.parse_args()
+    W = WORKLOADS[args.workload]
+    args.nb = W["nb"] if args.nb is None else args.nb
+    args.nq = W["nq"] if args.nq is None else args.nq
+    args.nprobe = W["nprobe"] if args.nprobe is None else args.nprobe
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":

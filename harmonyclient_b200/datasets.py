@@ -80,27 +80,28 @@ def gmm_dense(n, nq, d=420, ncomp=2048, sigma=0.3, seed=0, query_seed=None):
     return x, q
 
 
-def sparse_nonneg(n, nq, d=500, ncomp=2048, density=0.1, seed=0, chunk=1 << 17):
+def sparse_nonneg(n, nq, d=500, ncomp=2048, density=0.1, seed=0, chunk=1 << 17, query_seed=None):
     """Sparse non-negative rows, L2-normalised (config c5): each component owns
     a random support of density*d dims; a row draws Exp(1) values on its
-    component's support."""
+    component's support.  query_seed as in gmm_uint8."""
     rng = np.random.default_rng(seed)
     nnz = max(1, int(round(density * d)))
     supports = np.stack([rng.choice(d, size=nnz, replace=False) for _ in range(ncomp)])
 
-    def draw(m):
-        comp = rng.integers(0, ncomp, size=m)
+    def draw(m, g):
+        comp = g.integers(0, ncomp, size=m)
         out = np.zeros((m, d), np.float32)
         for s in range(0, m, chunk):
             e = min(m, s + chunk)
-            vals = rng.exponential(1.0, size=(e - s, nnz)).astype(np.float32)
+            vals = g.exponential(1.0, size=(e - s, nnz)).astype(np.float32)
             rows = np.arange(e - s)[:, None]
             out[s:e][rows, supports[comp[s:e]]] = vals
             nr = np.linalg.norm(out[s:e], axis=1, keepdims=True)
             out[s:e] /= np.maximum(nr, 1e-30)
         return out
 
-    return draw(n), draw(nq)
+    x = draw(n, rng)
+    return x, draw(nq, rng if query_seed is None else np.random.default_rng(query_seed))
 
 
 def c1(seed=0):
