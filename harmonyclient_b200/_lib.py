@@ -90,6 +90,8 @@ def load():
     L.hy_selftest_tcgen05.argtypes = [vp, vp, vp]
     L.hy_index_search_preassigned_noalloc.argtypes = [H, sz, vp, sz, sz, vp, vp, vp, vp]
     L.hy_index_set_graph.argtypes = [H, i]
+    L.hy_index_set_list_range.argtypes = [H, sz, sz]
+    L.hy_merge_topk.argtypes = [vp, vp, sz, sz, sz, i, vp, vp, vp]
     L.hy_selftest_tcgen05_e4m3.argtypes = [vp, vp, vp]
     L.hy_index_autotune.argtypes = [H, sz, vp, sz, i, vp]
     L.hy_index_search_nprobes.argtypes = [H, sz, vp, sz, vp, vp, vp]

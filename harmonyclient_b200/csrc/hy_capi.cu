@@ -144,6 +144,7 @@ struct hy_index {
     cudaEvent_t ev_graph[10] = {};
     cudaEvent_t* ev = ev_direct;
     int kev = 0;              // batched scan launches timed by ev[6..9]
+    size_t list_lo = 0, list_hi = SIZE_MAX;  // lists this index holds (hy_index_set_list_range)
     const int32_t* q_nprobe = nullptr;  // per-query nprobe (device) during a search_nprobes call
     DevBuf w_np;
     // CUDA graph of the device-pointer search (graph mode): the captured
@@ -333,14 +334,24 @@ int train_impl(hy_index* h, size_t n, const float* x, bool x_on_device, int lite
 int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, const int64_t* labels,
                 const std::vector<int32_t>& sizes, cudaStream_t s) {
     const size_t nlist = h->nlist;
-    h->h_list_size = sizes;
+    // An index restricted to lists [list_lo, list_hi) stores only their rows
+    // (the other lists stay empty); `start` follows the sorted order of all rows.
+    const size_t lo = std::min(h->list_lo, nlist), hi = std::min(h->list_hi, nlist);
+    const bool ranged = lo > 0 || hi < nlist;
+    std::vector<int32_t> kept = sizes;
+    if (ranged)
+        for (size_t l = 0; l < nlist; ++l)
+            if (l < lo || l >= hi) kept[l] = 0;
+    h->h_list_size = kept;
     h->h_list_off.assign(nlist + 1, 0);
     std::vector<int64_t> start(nlist + 1, 0);
+    size_t held = 0;
     for (size_t l = 0; l < nlist; ++l) {
         start[l + 1] = start[l] + sizes[l];
+        held += kept[l];
         // Lists start on 128-row boundaries: a 128-row tensor-core tile (and
         // four 32-row scan tiles) never straddles two lists.
-        h->h_list_off[l + 1] = h->h_list_off[l] + (sizes[l] + hy::BATCH_ROW_ALIGN - 1) / hy::BATCH_ROW_ALIGN *
+        h->h_list_off[l + 1] = h->h_list_off[l] + (kept[l] + hy::BATCH_ROW_ALIGN - 1) / hy::BATCH_ROW_ALIGN *
                                                       hy::BATCH_ROW_ALIGN;
     }
     h->arena_rows = (size_t)h->h_list_off[nlist];
@@ -357,14 +368,14 @@ int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, con
     HY_CUDA(cudaMemsetAsync(h->norms.p, 0, rows_alloc * sizeof(float), s));
     HY_CUDA(hy::launch_fill_i64(h->ids.as<int64_t>(), (int64_t)rows_alloc, -1, s));
     HY_CUDA(cudaMemcpyAsync(h->list_off.p, h->h_list_off.data(), (nlist + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    HY_CUDA(cudaMemcpyAsync(h->list_size.p, sizes.data(), nlist * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    HY_CUDA(cudaMemcpyAsync(h->list_size.p, kept.data(), nlist * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     HY_CUDA(cudaMemcpyAsync(h->w_start.p, start.data(), (nlist + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     if (n > 0)
         HY_CUDA(hy::launch_scatter(h->L, x, (int64_t)n, order, labels, h->w_start.as<int64_t>(),
-                                   h->list_off.as<int64_t>(), h->codes.as<float>(), h->ids.as<int64_t>(),
-                                   h->norms.as<float>(), s));
+                                   h->list_off.as<int64_t>(), ranged ? h->list_size.as<int32_t>() : nullptr,
+                                   h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(), s));
     HY_CUDA(cudaStreamSynchronize(s));
-    h->ntotal = n;
+    h->ntotal = held;
     return HY_OK;
 }
 
@@ -1159,6 +1170,28 @@ int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps,
     h->capq = best_capq;
     h->launches = 0;
     h->kev = 0;
+    return HY_OK;
+}
+
+int hy_index_set_list_range(hy_index* h, size_t lo, size_t hi) {
+    HY_CHECK(h, HY_ERR_ARG, "set_list_range: NULL handle");
+    h->epoch++;  // a captured search graph no longer matches
+    HY_CHECK(lo < hi && hi <= h->nlist, HY_ERR_ARG, "set_list_range: need 0 <= lo < hi <= nlist");
+    h->list_lo = lo;
+    h->list_hi = hi;
+    return HY_OK;
+}
+
+int hy_merge_topk(const float* dD, const int64_t* dI, size_t parts, size_t n, size_t k, int metric, float* dDout,
+                  int64_t* dIout, void* stream) {
+    HY_CHECK(n == 0 || (dD && dI && dDout && dIout), HY_ERR_ARG, "merge_topk: NULL argument");
+    HY_CHECK(parts >= 1 && parts <= 64 && k >= 1 && k <= HY_MAX_K && parts * k <= 8192, HY_ERR_ARG,
+             "merge_topk: need 1 <= parts <= 64, 1 <= k <= 256 and parts * k <= 8192");
+    HY_CHECK(metric == HY_METRIC_L2 || metric == HY_METRIC_IP, HY_ERR_ARG, "merge_topk: unknown metric");
+    if (n == 0) return HY_OK;
+    HY_CHECK(n < (size_t(1) << 31), HY_ERR_ARG, "merge_topk: too many queries");
+    HY_CUDA(hy::launch_merge_parts(dD, dI, (int)parts, (int)n, (int)k, metric, dDout, dIout,
+                                   static_cast<cudaStream_t>(stream)));
     return HY_OK;
 }
 

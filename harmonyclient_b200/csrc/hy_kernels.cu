@@ -746,13 +746,14 @@ __global__ void sort_keys_kernel(const int64_t* __restrict__ labels, const float
 // reference's candidate_norms, src/Index.cpp:689-696, sequential float sum).
 __global__ void scatter_kernel(ArenaLayout L, const float* __restrict__ x, int64_t n, const int32_t* __restrict__ order,
                                const int64_t* __restrict__ labels, const int64_t* __restrict__ list_start,
-                               const int64_t* __restrict__ list_off, float* __restrict__ codes,
-                               int64_t* __restrict__ ids, float* __restrict__ norms) {
+                               const int64_t* __restrict__ list_off, const int32_t* __restrict__ keep,
+                               float* __restrict__ codes, int64_t* __restrict__ ids, float* __restrict__ norms) {
     const int lane = threadIdx.x & 31;
     const int64_t p = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (p >= n) return;
     const int64_t src = order[p];
     const int64_t l = labels[src];
+    if (keep && p - list_start[l] >= keep[l]) return;  // a list this index does not hold
     const int64_t r = list_off[l] + (p - list_start[l]);
     const float* xr = x + src * L.d;
     for (int b = 0; b < L.nb; ++b) {
@@ -764,6 +765,48 @@ __global__ void scatter_kernel(ArenaLayout L, const float* __restrict__ x, int64
         for (int j = 0; j < L.d; ++j) s = __fadd_rn(s, __fmul_rn(xr[j], xr[j]));
         ids[r] = src;
         norms[r] = s;
+    }
+}
+
+// Merge of `parts` per-query top-k lists (layout [parts][n][k], each sorted
+// best first) into the best k: key (ordered score, part, rank), so equal
+// distances keep the parts' order and then each part's own order.  One CTA
+// per query.
+__global__ void __launch_bounds__(256) merge_parts_kernel(const float* __restrict__ D, const int64_t* __restrict__ I,
+                                                          int parts, int n, int k, int metric, float* __restrict__ oD,
+                                                          int64_t* __restrict__ oI) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    uint64_t* keys = reinterpret_cast<uint64_t*>(sm);
+    const int q = blockIdx.x;
+    const int total = parts * k;
+    const int P = next_pow2(total);
+    const bool l2 = metric == METRIC_L2;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        uint64_t key = KEY_MAX;
+        if (i < total) {
+            const int p = i / k, r = i % k;
+            const size_t at = (static_cast<size_t>(p) * n + q) * k + r;
+            if (I[at] >= 0) {
+                const float sc = l2 ? D[at] : -D[at];
+                key = (static_cast<uint64_t>(f2o(sc)) << 32) | (static_cast<uint32_t>(p) << 16) | static_cast<uint32_t>(r);
+            }
+        }
+        keys[i] = key;
+    }
+    __syncthreads();
+    cta_bitonic_sort(keys, P);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const uint64_t key = keys[i];
+        const size_t o = static_cast<size_t>(q) * k + i;
+        if (key == KEY_MAX) {
+            oD[o] = l2 ? FLT_MAX : -FLT_MAX;
+            oI[o] = -1;
+        } else {
+            const int p = static_cast<int>((key >> 16) & 0xffffu), r = static_cast<int>(key & 0xffffu);
+            const size_t at = (static_cast<size_t>(p) * n + q) * k + r;
+            oD[o] = D[at];
+            oI[o] = I[at];
+        }
     }
 }
 
@@ -969,10 +1012,20 @@ cudaError_t radix_sort_pairs(void* tmp, size_t* tmp_bytes, const uint64_t* kin, 
 }
 
 cudaError_t launch_scatter(const ArenaLayout& L, const float* x, int64_t n, const int32_t* order,
-                           const int64_t* labels, const int64_t* list_start, const int64_t* list_off, float* codes,
-                           int64_t* ids, float* norms, cudaStream_t s) {
-    scatter_kernel<<<grid_for(n * 32, 256), 256, 0, s>>>(L, x, n, order, labels, list_start, list_off, codes, ids,
-                                                         norms);
+                           const int64_t* labels, const int64_t* list_start, const int64_t* list_off,
+                           const int32_t* keep, float* codes, int64_t* ids, float* norms, cudaStream_t s) {
+    scatter_kernel<<<grid_for(n * 32, 256), 256, 0, s>>>(L, x, n, order, labels, list_start, list_off, keep, codes,
+                                                         ids, norms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_parts(const float* D, const int64_t* I, int parts, int n, int k, int metric, float* oD,
+                               int64_t* oI, cudaStream_t s) {
+    const size_t smem = static_cast<size_t>(next_pow2(parts * k)) * 8;
+    cudaError_t e = cudaFuncSetAttribute(merge_parts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    merge_parts_kernel<<<n, 256, smem, s>>>(D, I, parts, n, k, metric, oD, oI);
     return cudaGetLastError();
 }
 

@@ -85,9 +85,15 @@ cudaError_t launch_make_sort_keys(const int64_t* labels, const float* score, int
                                   int32_t* vals, cudaStream_t s);
 cudaError_t radix_sort_pairs(void* tmp, size_t* tmp_bytes, const uint64_t* kin, uint64_t* kout, const int32_t* vin,
                              int32_t* vout, int64_t n, int end_bit, cudaStream_t s);
+// Merge of parts per-query top-k lists ([parts][n][k], best first) into the
+// best k (ties: part order, then rank).
+cudaError_t launch_merge_parts(const float* D, const int64_t* I, int parts, int n, int k, int metric, float* oD,
+                               int64_t* oI, cudaStream_t s);
+// keep (optional): rows of list l past keep[l] are not stored (lists an index
+// does not hold have keep 0).
 cudaError_t launch_scatter(const ArenaLayout& L, const float* x, int64_t n, const int32_t* order,
-                           const int64_t* labels, const int64_t* list_start, const int64_t* list_off, float* codes,
-                           int64_t* ids, float* norms, cudaStream_t s);
+                           const int64_t* labels, const int64_t* list_start, const int64_t* list_off,
+                           const int32_t* keep, float* codes, int64_t* ids, float* norms, cudaStream_t s);
 cudaError_t launch_fill_i64(int64_t* p, int64_t n, int64_t v, cudaStream_t s);
 cudaError_t launch_gather_rows(const float* x, const int64_t* rows, int64_t n, int d, float* out, cudaStream_t s);
 cudaError_t launch_normalize_rows(const float* x, int64_t n, int d, float* out, cudaStream_t s);

@@ -150,6 +150,11 @@ class Index:
         inf = self.info()
         return {"capq": int(inf.capq), "row_slice": int(inf.row_slice)}
 
+    def set_list_range(self, lo, hi):
+        """Hold only lists [lo, hi) from the next add() on (list partition
+        across GPUs; see harmonyclient_b200.parallel)."""
+        check(self._L.hy_index_set_list_range(self._h, int(lo), int(hi)))
+
     def set_graph(self, enabled=True):
         """Graph mode for the device-pointer searches (CUDA graph replay)."""
         check(self._L.hy_index_set_graph(self._h, int(bool(enabled))))

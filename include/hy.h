@@ -177,6 +177,19 @@ HY_API int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t
  * differed). */
 HY_API int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps, float* report);
 
+/* List partition across GPUs (the reference's vector partition across
+ * teams, src/Index.cpp:288-325, as one index per GPU): after
+ * hy_index_set_list_range(h, lo, hi), add() keeps only the rows of lists
+ * [lo, hi) (the other lists stay empty, ids stay the row indices of the whole
+ * base), so every search scans only this GPU's share of each query's probed
+ * lists.  The per-GPU top-k lists, gathered into one [parts][n][k] device
+ * array (one all-gather), are merged by hy_merge_topk into the top-k of the
+ * whole index; with contiguous ranges in GPU order the merged answer equals
+ * the unpartitioned index's, ties included. */
+HY_API int hy_index_set_list_range(hy_index* h, size_t lo, size_t hi);
+HY_API int hy_merge_topk(const float* dD, const int64_t* dI, size_t parts, size_t n, size_t k, int metric,
+                         float* dDout, int64_t* dIout, void* stream);
+
 /* Graph mode for the device-pointer searches (no counterpart in the
  * reference): the first call with given buffers, sizes, stream and index
  * state runs normally and captures its launch sequence (coarse quantisation,
