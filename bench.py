@@ -482,6 +482,58 @@ def run_ours(args, rank, world, dist):
     return line
 
 
+def run_lists(args, rank, world, dist):
+    """--parallelism lists: one index partitioned by lists over the N ranks
+    (harmonyclient_b200.parallel); every rank searches the same query batch
+    over its own lists, then one all-gather and the device merge.  `value` is
+    the batch's queries/s (strong scaling: the index is fixed, its lists are
+    split), timed with CUDA events on the current stream, max over ranks."""
+    import torch
+
+    from harmonyclient_b200.parallel import ListShardedIndex
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    W = WORKLOADS[args.workload]
+    x, q = workload(args, 0)  # every rank: the same base and queries
+    k = W["k"]
+    sh = ListShardedIndex(W["d"], W["nlist"], args.nprobe, device=dev)
+    sh.train(x)
+    sh.add(x)
+    sh.index.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
+    base = "bf16" if args.form == "learned" else args.form
+    sh.index.set_form(base)
+    dq = torch.from_numpy(q).cuda()
+    for _ in range(args.warmup):
+        sh.search_device(dq, k)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            Dm, Im = sh.search_device(dq, k)
+        e1.record()
+        torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    if rank != 0:
+        return None
+    sc, ns = _score(x, q, Dm.cpu().numpy(), Im.cpu().numpy(), args.recall_sample, {})
+    return {
+        "metric": METRIC, "value": round(q.shape[0] * args.steps / (ms / 1e3), 1), "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": {"plain": "f32", "bf16": "bf16", "fp8": "e4m3"}[base], "data": W["data"],
+        "config": {"workload": W["desc"].format(nb=args.nb) + f", nlist {W['nlist']}, nprobe {args.nprobe}, k {k}, "
+                               f"{q.shape[0]} queries per step, lists split over {world} GPUs",
+                   "name": args.workload, "parallelism": f"lists x{world}"},
+        "recall_at_10": round(sc["recall"], 4), "recall_vs": f"FP64 brute force on the GPU, {ns} queries",
+        "clocks": clk.summary(),
+    }
+
+
 def run_reference(args, rank):
     """The reference's own CPU query path (Index::search, ORIGINAL mode,
     OpenMP over all host cores), compiled from the reference sources into
@@ -536,6 +588,8 @@ def main():
     ap.add_argument("--nprobe", type=int, default=None, help="default: the workload's (c4: the per-query maximum)")
     ap.add_argument("--warmup-list", type=int, default=10)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--parallelism", default="replicas", choices=["replicas", "lists"],
+                    help="N > 1: replicas (each GPU its own query batch) or one index split by lists")
     ap.add_argument("--form", default="learned", choices=["learned", "bf16", "fp8", "plain"])
     ap.add_argument("--base", default="bf16", choices=["bf16", "fp8", "plain"],
                     help="scan form under the learned probes")
@@ -573,7 +627,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    line = run_ours(args, rank, world, dist)
+    if args.parallelism == "lists" and world > 1:
+        line = run_lists(args, rank, world, dist)
+    else:
+        line = run_ours(args, rank, world, dist)
     if line is not None:
         print(json.dumps(line), flush=True)
     if dist:
