@@ -1029,8 +1029,10 @@ __device__ void rerank_warp_query(const ArenaLayout& L, const float* __restrict_
     }
 }
 
-// One warp per query; a query with more than 512 candidates (or k > 512, or
-// an overflowed buffer) is listed in w.big for the CTA kernel.
+// One warp per query; a query with more than 256 candidates (or k > 256, or
+// an overflowed buffer) is listed in w.big for the CTA kernel.  (Capping the
+// register sorts at 256 keys keeps the kernel at 64 registers: four CTAs per
+// SM.)
 __global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant__ ArenaLayout L,
                                                           const float* __restrict__ codes,
                                                           const int64_t* __restrict__ ids, const float* __restrict__ xn,
@@ -1041,14 +1043,14 @@ __global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant_
                                                           int64_t* __restrict__ I) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t* sl = reinterpret_cast<uint64_t*>(sm) + static_cast<size_t>(warp) * 512;  // [8][512] selected keys
-    float* qs = reinterpret_cast<float*>(reinterpret_cast<uint64_t*>(sm) + 8 * 512) +
+    uint64_t* sl = reinterpret_cast<uint64_t*>(sm) + static_cast<size_t>(warp) * 256;  // [8][256] selected keys
+    float* qs = reinterpret_cast<float*>(reinterpret_cast<uint64_t*>(sm) + 8 * 256) +
                 static_cast<size_t>(warp) * L.row_pitch;
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
     const int cnt = w.cand_cnt[qi];
     const int n = min(cnt, capq);
-    if (cnt > capq || n > 512 || k > 512) {
+    if (cnt > capq || n > 256 || k > 256) {
         if (lane == 0) w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
         return;
     }
@@ -1068,10 +1070,8 @@ __global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant_
     const int need = max(n, k);
     if (need <= 128)
         rerank_warp_query<4>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
-    else if (need <= 256)
-        rerank_warp_query<8>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
     else
-        rerank_warp_query<16>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+        rerank_warp_query<8>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
 }
 
 __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float* __restrict__ codes,
@@ -1386,7 +1386,7 @@ cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_
     err_consts(L.d, f8, &cK, &cN);
     cudaError_t e = cudaMemsetAsync(w.big, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
-    const size_t wsmem = static_cast<size_t>(8) * (512 * sizeof(uint64_t) + L.row_pitch * sizeof(float));
+    const size_t wsmem = static_cast<size_t>(8) * (256 * sizeof(uint64_t) + L.row_pitch * sizeof(float));
     if ((e = cudaFuncSetAttribute(rerank_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(wsmem))) != cudaSuccess)
         return e;

@@ -148,8 +148,9 @@ __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __res
 // Inference on the tensor cores.  The weights are packed once (mlp_pack) into
 // the tcgen05 B-operand image: W1 as 256 rows (output features) x 64 inputs,
 // one 128-byte-swizzled K-major k-block of 32 KiB; W2 as 256 rows x 256
-// inputs, four such k-blocks.  One CTA of 128 threads takes 128 queries
-// (thread = query = TMEM lane): features -> bf16 A tile -> MMA (M 128, N 256,
+// inputs, four such k-blocks.  One CTA of 256 threads takes 128 queries
+// (query = TMEM lane; two threads per query split every layer's 256 columns):
+// features -> bf16 A tile -> MMA (M 128, N 256,
 // K 64) -> bias + GELU -> bf16 A tiles (4 k-blocks) -> MMA (K 256) -> bias +
 // GELU -> dot with W3 -> nprobe, all on chip.
 constexpr int MI_WIMG = 32768 + 4 * 32768;   // packed W1 + W2 bytes
@@ -180,7 +181,7 @@ __device__ inline uint4 pack8_bf16(const float* v) {
     return r;
 }
 
-__global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
+__global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
                                                            const float* __restrict__ mu, const float* __restrict__ sd,
                                                            const unsigned char* __restrict__ wimg,
                                                            const float* __restrict__ params, float margin,
@@ -194,17 +195,21 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
     __shared__ uint64_t bar_w, bar_m;
     __shared__ uint32_t tbase;
     __shared__ int s_ok;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ float s_part[128];  // layer-3 partial sums of the upper column half
+    // Two threads per query row: warps w and w + 4 share TMEM lane quadrant
+    // w % 4 and take column halves 0 / 1 of every 256-wide layer.
+    const int warp = threadIdx.x >> 5, half = warp >> 2;
+    const int tid = threadIdx.x & 127;  // the query row within the tile
     const int row = blockIdx.x * 128 + tid;
     const bool valid = row < m;
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         mbar_init(&bar_w, 1);
         mbar_init(&bar_m, 1);
         fence_mbar_init();
         s_ok = 1;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         mbar_expect_tx(&bar_w, MI_WIMG);
         for (int c = 0; c < MI_WIMG / 16384; ++c) bulk_g2s(sW + c * 16384, wimg + c * 16384, 16384, &bar_w);
     }
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
         const float s0 = valid ? sc[0] : 0.0f;
         const float a0 = fabsf(s0) + 1e-6f;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
+        for (int c = 4 * half; c < 4 * half + 4; ++c) {
             float f[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -233,7 +238,7 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
     tc::fence_after_sync();
     const uint32_t tmem = tbase;
     const uint32_t idesc = tc::idesc_bf16_f32(128, 256);
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         if (!mbar_wait_bounded(&bar_w, 0, err)) {
             s_ok = 0;
         } else {
@@ -248,10 +253,11 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
     __syncthreads();
     bool ok = s_ok != 0 && mbar_wait_bounded(&bar_m, 0, err);
     tc::fence_after_sync();
-    const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t lane_addr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
     if (ok) {
-        // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks.
-        for (int cb = 0; cb < 4; ++cb) {
+        // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks
+        // (this thread's column half: k-blocks 2*half, 2*half + 1).
+        for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
             uint32_t u[64];
             tc::tmem_ld64(lane_addr + cb * 64, u);
 #pragma unroll
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (tid == 0 && ok) {
+    if (threadIdx.x == 0 && ok) {
         for (int kb = 0; kb < 4; ++kb)
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk)
@@ -279,11 +285,12 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
     }
     __syncthreads();
     ok = ok && mbar_wait_bounded(&bar_m, 1, err);
+    float acc = 0.0f;
     tc::fence_after_sync();
     if (ok) {
-        // Layer 2 epilogue and layer 3: y = bf16(GELU(Z2 + b2)) . bf16(W3) + b3.
-        float acc = 0.0f;
-        for (int cb = 0; cb < 4; ++cb) {
+        // Layer 2 epilogue and layer 3: y = bf16(GELU(Z2 + b2)) . bf16(W3) + b3,
+        // each thread over its column half.
+        for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
             uint32_t u[64];
             tc::tmem_ld64(lane_addr + cb * 64, u);
 #pragma unroll
@@ -293,7 +300,11 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const float* __restri
                 acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
             }
         }
-        const float y = acc + params[MLP_B3];
+        if (half == 1) s_part[tid] = acc;
+    }
+    __syncthreads();
+    if (ok && half == 0) {
+        const float y = (acc + s_part[tid]) + params[MLP_B3];
         if (valid) {
             if (yout) yout[row] = y;
             if (probes) {
@@ -393,7 +404,7 @@ cudaError_t mlp_infer(const float* pscore, int m, int P, const float* mu, const 
     if (m <= 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MI_SMEM);
     if (e != cudaSuccess) return e;
-    mlp_infer_kernel<<<blocks(m, 128), 128, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin, probes, total,
+    mlp_infer_kernel<<<blocks(m, 128), 256, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin, probes, total,
                                                          yout, err);
     return cudaGetLastError();
 }
