@@ -682,10 +682,19 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         auto flush = [&]() {
             __syncwarp();
             const int n = min(*reinterpret_cast<volatile int*>(wcount), CB);
-            for (int i = lane; i < n; i += 32) {
-                const int qid = wq[i];
-                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
-                if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = wk[i];
+            // All of this lane's counter atomics first (independent, so their
+            // latencies overlap), then the stores that depend on them.
+            int pos[CB / 32], qid[CB / 32];
+#pragma unroll
+            for (int j = 0; j < CB / 32; ++j) {
+                const int i = lane + 32 * j;
+                qid[j] = i < n ? wq[i] : 0;
+                pos[j] = i < n ? atomicAdd(&p.cand_cnt[qid[j]], 1) : p.capq;
+            }
+#pragma unroll
+            for (int j = 0; j < CB / 32; ++j) {
+                const int i = lane + 32 * j;
+                if (pos[j] < p.capq) p.cand[static_cast<int64_t>(qid[j]) * p.capq + pos[j]] = wk[i];
             }
             __syncwarp();
             if (lane == 0) *wcount = 0;
