@@ -145,6 +145,8 @@ struct hy_index {
     cudaEvent_t* ev = ev_direct;
     int kev = 0;              // batched scan launches timed by ev[6..9]
     size_t list_lo = 0, list_hi = SIZE_MAX;  // lists this index holds (hy_index_set_list_range)
+    size_t learned_rows = SIZE_MAX;  // the learned cut applies to batch rows below this
+    DevBuf w_jrows;                  // judged rows of a learned batch
     const int32_t* q_nprobe = nullptr;  // per-query nprobe (device) during a search_nprobes call
     DevBuf w_np;
     // CUDA graph of the device-pointer search (graph mode): the captured
@@ -501,10 +503,14 @@ bool batched_form(const hy_index* h) { return h->form == HY_FORM_BF16 || h->form
 // Chunk of queries whose probes (m x nprobe, best first) and their coarse
 // scores (h->m_pscore) are on the device: the probe network predicts each
 // query's nprobe and the probes beyond it become -1.
-int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, int64_t* probes = nullptr) {
+int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, int64_t* probes = nullptr,
+                         size_t q0 = 0) {
     if (!probes) probes = h->w_probes.as<int64_t>();
     HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
-    HY_CUDA(hy::mlp_infer(h->m_pscore.as<float>(), (int)m, (int)nprobe, h->m_mu.as<float>(), h->m_sd.as<float>(),
+    // Rows at or past learned_rows keep the fixed nprobe (judged rows).
+    const size_t mc = h->learned_rows > q0 ? std::min(m, h->learned_rows - q0) : 0;
+    if (mc == 0) return HY_OK;
+    HY_CUDA(hy::mlp_infer(h->m_pscore.as<float>(), (int)mc, (int)nprobe, h->m_mu.as<float>(), h->m_sd.as<float>(),
                           h->m_wimg.as<unsigned char>(), h->m_params.as<float>(), h->margin, probes,
                           h->m_total.as<unsigned long long>(), nullptr, h->w_err.as<int>(), s));
     h->launches += 1;
@@ -535,7 +541,7 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
                                   h->w_probes.as<int64_t>(), learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
         h->launches += 2;
-        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
+        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s, nullptr, q0));
         if (h->q_nprobe) {
             HY_CUDA(hy::launch_cut_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, h->q_nprobe + q0, s));
             h->launches += 1;
@@ -674,7 +680,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
                                   learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
-        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s));
+        if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s, nullptr, q0));
         if (h->q_nprobe) {
             HY_CUDA(hy::launch_cut_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, h->q_nprobe + q0, s));
             h->launches += 1;
@@ -881,7 +887,7 @@ int run_device_search(hy_index* h, size_t n, const float* dq, size_t k, float* d
 // answered again on the device by the plain scan (up to FB_CAP per chunk);
 // if more overflowed in some chunk, the whole batch is searched again here
 // with the plain form (its queries are still in h->w_q).
-int bf16_fallback(hy_index* h, size_t n, size_t k, float* D, int64_t* I, cudaStream_t s) {
+int bf16_fallback(hy_index* h, size_t n, size_t k, cudaStream_t s) {
     unsigned long long c[2] = {0, 0};
     HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
     h->stats.fallback_queries = c[0];
@@ -892,8 +898,6 @@ int bf16_fallback(hy_index* h, size_t n, size_t k, float* D, int64_t* I, cudaStr
     const int rc = search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, false);
     h->form = form;
     HY_RET(rc);
-    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
-    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
     h->stats.fallback_queries = n;
     return HY_OK;
@@ -1214,18 +1218,32 @@ namespace {
 
 // The host-pointer search of one batch: upload, device search, download,
 // bf16 overflow fallback, statistics.
-int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
+int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I,
+                const std::vector<int64_t>* judge_rows = nullptr, int64_t* jI = nullptr) {
     cudaStream_t s = h->stream;
     h->ev = h->ev_direct;
-    HY_RET(h->w_q.ensure(n * h->d * sizeof(float)));
-    HY_RET(h->w_D.ensure(n * k * sizeof(float)));
-    HY_RET(h->w_I.ensure(n * k * sizeof(int64_t)));
+    // Judged rows (learned form) ride along at the end of the batch: the
+    // same queries again, with the fixed nprobe (the learned cut stops at
+    // row n).
+    const size_t m = judge_rows ? judge_rows->size() : 0;
+    const size_t nt = n + m;
+    HY_RET(h->w_q.ensure(nt * h->d * sizeof(float)));
+    HY_RET(h->w_D.ensure(nt * k * sizeof(float)));
+    HY_RET(h->w_I.ensure(nt * k * sizeof(int64_t)));
     HY_RET(reset_counters(h, s));
     HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
-    HY_RET(search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true));
-    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
-    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    HY_RET(finish_host_call(h, s, true, n, std::min(h->nprobe, h->nlist)));
+    if (m) {
+        HY_RET(h->w_jrows.ensure(m * sizeof(int64_t)));
+        HY_CUDA(cudaMemcpyAsync(h->w_jrows.p, judge_rows->data(), m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        HY_CUDA(hy::launch_gather_rows(h->w_q.as<float>(), h->w_jrows.as<int64_t>(), (int64_t)m, (int)h->d,
+                                       h->w_q.as<float>() + n * h->d, s));
+    }
+    h->learned_rows = n;
+    const int rc = search_device_impl(h, nt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true);
+    h->learned_rows = SIZE_MAX;
+    HY_RET(rc);
+    HY_RET(finish_host_call(h, s, true, nt, std::min(h->nprobe, h->nlist)));
+    h->stats.nq = n;
     h->stats.fallback_queries = 0;
     h->stats.mean_nprobe = (double)std::min(h->nprobe, h->nlist);
     if (learned_on(h)) {
@@ -1235,32 +1253,29 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     }
     if (batched_form(h) && h->arena_rows > 0) {
         const hy_search_stats_t keep = h->stats;
-        HY_RET(bf16_fallback(h, n, k, D, I, s));
+        HY_RET(bf16_fallback(h, nt, k, s));
         const uint64_t fb = h->stats.fallback_queries;
         h->stats = keep;
         h->stats.fallback_queries = fb;
     }
+    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (m) HY_CUDA(cudaMemcpyAsync(jI, h->w_I.as<int64_t>() + n * k, m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
     return HY_OK;
 }
 
-// The learned nprobe is judged on every batch: a sample of the batch is
-// searched again with the fixed nprobe and the learned results' recall@10
-// against those is measured; below the target, the whole batch is searched
-// again with the fixed nprobe.
-int judge_learned(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
+// The learned nprobe is judged on every batch: every (1/judge_fraction)-th
+// query is searched a second time with the fixed nprobe in the same device
+// pass, and the learned results' recall@10 against those is measured; below
+// the target, the whole batch is searched again with the fixed nprobe.
+int search_learned_judged(hy_index* h, size_t n, const float* q, size_t k, float* D, int64_t* I) {
     const size_t step = std::max<size_t>(1, (size_t)std::lround(1.0 / std::max(1e-6f, h->judge_fraction)));
-    std::vector<size_t> rows;
-    for (size_t i = 0; i < n; i += step) rows.push_back(i);
+    std::vector<int64_t> rows;
+    for (size_t i = 0; i < n; i += step) rows.push_back((int64_t)i);
     const size_t m = rows.size();
-    std::vector<float> sq(m * h->d), sD(m * k);
     std::vector<int64_t> sI(m * k);
-    for (size_t i = 0; i < m; ++i) std::memcpy(&sq[i * h->d], q + rows[i] * h->d, h->d * sizeof(float));
-    const hy_search_stats_t keep = h->stats;
-    h->learned = 0;
-    const int rc = search_host(h, m, sq.data(), k, sD.data(), sI.data());
-    h->learned = 1;
-    h->stats = keep;
-    HY_RET(rc);
+    HY_RET(search_host(h, n, q, k, D, I, &rows, sI.data()));
     const size_t kk = std::min<size_t>(10, k);
     size_t hit = 0, tot = 0;
     for (size_t i = 0; i < m; ++i) {
@@ -1336,10 +1351,10 @@ int hy_index_search(hy_index* h, size_t n, const float* q, size_t k, float* D, i
     if (n == 0) return HY_OK;
     HY_RET(check_search_args(h, n, k));
     HY_RET(set_device(h));
+    if (learned_on(h) && h->judge_fraction > 0) return search_learned_judged(h, n, q, k, D, I);
     HY_RET(search_host(h, n, q, k, D, I));
     h->stats.judge_recall = -1.0;
     h->stats.learned_fallback = 0;
-    if (learned_on(h) && h->judge_fraction > 0) HY_RET(judge_learned(h, n, q, k, D, I));
     return HY_OK;
 }
 
