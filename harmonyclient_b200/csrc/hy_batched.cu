@@ -470,7 +470,6 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     __shared__ uint32_t tbase;
     __shared__ int s_abort;
     __shared__ long long s_g[2];
-    __shared__ int s_wcount[N_EPI];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool l2 = p.metric == 1;
@@ -676,12 +675,12 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         const int half = e >> 2;           // columns [CW*half, CW*half+CW)
         int* wq = s_cq + e * CB;
         uint64_t* wk = s_ck + e * CB;
-        int* wcount = &s_wcount[e];
-        if (lane == 0) *wcount = 0;
-        __syncwarp();
+        // Staged candidates of this warp: wc entries (warp-uniform, kept in
+        // a register; only this warp writes its staging rows).
+        int wc = 0;
         auto flush = [&]() {
             __syncwarp();
-            const int n = min(*reinterpret_cast<volatile int*>(wcount), CB);
+            const int n = min(wc, CB);
             // All of this lane's counter atomics first (independent, so their
             // latencies overlap), then the stores that depend on them.
             int pos[CB / 32], qid[CB / 32];
@@ -697,8 +696,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 if (pos[j] < p.capq) p.cand[static_cast<int64_t>(qid[j]) * p.capq + pos[j]] = wk[i];
             }
             __syncwarp();
-            if (lane == 0) *wcount = 0;
-            __syncwarp();
+            wc = 0;
         };
         const float cf = l2 ? -2.0f : -1.0f;
         uint32_t tile_it = 0;
@@ -766,40 +764,44 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
 #pragma unroll
                     for (int j = 0; j < CC; ++j)
                         mask |= (fmaf(m[j], __uint_as_float(u[c * CC + j]), ax) <= r[j]) ? (1u << j) : 0u;
-                    if (mask) {
-                        // Rare: this lane has candidates in the chunk.  Its
-                        // accumulators go to a private shared-memory row so the
-                        // set bits can be visited with a compact loop.
+                    const unsigned cols = __reduce_or_sync(FULL, mask);
+                    if (cols) {
+                        // Some rows of the warp have candidates in the chunk.
+                        // Their accumulators go to private shared-memory rows;
+                        // then, column by column (warp-uniform), the lanes with
+                        // a candidate there write it at their ballot rank.
                         float* sip = s_ip + (e * 32 + lane) * CC;
+                        if (mask) {
 #pragma unroll
-                        for (int j = 0; j < CC; j += 4)
-                            *reinterpret_cast<float4*>(sip + j) =
-                                make_float4(__uint_as_float(u[c * CC + j]), __uint_as_float(u[c * CC + j + 1]),
-                                            __uint_as_float(u[c * CC + j + 2]), __uint_as_float(u[c * CC + j + 3]));
-                        while (mask) {
-                            const int j = __ffs(mask) - 1;
-                            mask &= mask - 1u;
-                            const int q = col0 + j;
-                            const float ip = F8 ? sip[j] * S.sc[q] : sip[j];
-                            const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
-                            const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
-                            const int slotpos = atomicAdd(wcount, 1);
-                            if (slotpos < CB) {
-                                wq[slotpos] = S.qid[q];
-                                wk[slotpos] = key;
-                            } else {
-                                // staging full: emit directly
-                                const int qid = S.qid[q];
-                                const int pos = atomicAdd(&p.cand_cnt[qid], 1);
-                                if (pos < p.capq) p.cand[static_cast<int64_t>(qid) * p.capq + pos] = key;
+                            for (int j = 0; j < CC; j += 4)
+                                *reinterpret_cast<float4*>(sip + j) =
+                                    make_float4(__uint_as_float(u[c * CC + j]), __uint_as_float(u[c * CC + j + 1]),
+                                                __uint_as_float(u[c * CC + j + 2]), __uint_as_float(u[c * CC + j + 3]));
+                        }
+                        unsigned left = cols;
+                        while (left) {
+                            const int j = __ffs(left) - 1;
+                            left &= left - 1u;
+                            const bool mine = (mask >> j) & 1u;
+                            const unsigned bal = __ballot_sync(FULL, mine);
+                            const int cnt = __popc(bal);
+                            if (wc + cnt > CB) flush();  // warp-uniform
+                            if (mine) {
+                                const int q = col0 + j;
+                                const float ip = F8 ? sip[j] * S.sc[q] : sip[j];
+                                const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
+                                const int at = wc + __popc(bal & ((1u << lane) - 1u));
+                                wq[at] = S.qid[q];
+                                wk[at] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
                             }
+                            wc += cnt;
                         }
                     }
                 }
                 tc::fence_before_sync();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cta(&acce[buf]);
-                if (__any_sync(FULL, *reinterpret_cast<volatile int*>(wcount) > CB - 64)) flush();
+                if (wc > CB - 64) flush();
             }
             flush();
             if (lane == 0) mbar_arrive_cta(&sfree[b]);
