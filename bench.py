@@ -44,9 +44,9 @@ METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan 
 # launch (traffic grows with the query count: every query streams its own
 # probed lists).
 KNOWN_TRAFFIC = {
-    ("c2", "plain", 1_000_000, 10_000, 64): 218_703_690_000,
-    ("c2", "learned", 1_000_000, 10_000, 64): 250_758_000,
-    ("c2", "bf16", 1_000_000, 10_000, 64): 279_463_000,
+    ("c2", "plain", 1_000_000, 10_000, 64): 216_530_000_000,
+    ("c2", "learned", 1_000_000, 10_000, 64): 249_000_000,
+    ("c2", "bf16", 1_000_000, 10_000, 64): 279_050_000,
 }
 
 
