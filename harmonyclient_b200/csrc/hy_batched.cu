@@ -427,6 +427,12 @@ constexpr size_t batched_smem(int nkb) {
            N_EPI * 32 * CC * sizeof(float);
 }
 
+// Accumulator column of a group's i-th query (a bijection on [0, QG)).
+template <int QG>
+__device__ __forceinline__ int group_col(int i) {
+    return (i >> 1) + (i & 1) * (QG / 2);
+}
+
 __device__ inline bool wait_or_abort(uint64_t* bar, uint32_t parity, int* err, volatile int* abort) {
     for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
@@ -553,42 +559,50 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             // ranges stay inside it).
             for (int c = gt; c < (nrows + 3) / 4; c += 32 * N_GATHER) cp_async16(&S.xn[4 * c], p.xn + row0 + 4 * c);
             for (int c = gt; c < (nrows + TM - 1) / TM; c += 32 * N_GATHER) S.taux[c] = p.tile_aux[row0 / TM + c];
+            // Query i of the group sits in accumulator column col(i): even
+            // queries in the first half of the columns, odd ones in the
+            // second, so a small group keeps both epilogue warps of every
+            // TMEM lane quadrant busy.
             for (int i = gt; i < QG; i += 32 * N_GATHER) {
+                const int col = group_col<QG>(i);
                 const int qid = i < nqv ? grp[i] : -1;
-                S.qid[i] = qid;
+                S.qid[col] = qid;
                 if (qid >= 0) {
                     const float4 qa = p.qaux[qid];
                     const ErrCoef ec = err_coef(qa, l2, p.cK, p.cN);
-                    S.qn[i] = l2 ? qa.x : 0.0f;
-                    S.V[i] = p.thr[qid] + ec.cq - (l2 ? qa.x : 0.0f);
-                    S.aq[i] = ec.aq;
-                    S.bq[i] = ec.bq;
-                    S.sc[i] = F8 ? ls * p.qscale[qid] : 1.0f;
+                    S.qn[col] = l2 ? qa.x : 0.0f;
+                    S.V[col] = p.thr[qid] + ec.cq - (l2 ? qa.x : 0.0f);
+                    S.aq[col] = ec.aq;
+                    S.bq[col] = ec.bq;
+                    S.sc[col] = F8 ? ls * p.qscale[qid] : 1.0f;
                 } else {
-                    S.qn[i] = 0.0f;
-                    S.V[i] = -INFINITY;
-                    S.aq[i] = 0.0f;
-                    S.bq[i] = 0.0f;
-                    S.sc[i] = 0.0f;
+                    S.qn[col] = 0.0f;
+                    S.V[col] = -INFINITY;
+                    S.aq[col] = 0.0f;
+                    S.bq[col] = 0.0f;
+                    S.sc[col] = 0.0f;
                 }
             }
-            // The group's queries into the swizzled B operand: every 16-byte
-            // chunk is its own asynchronous copy, all in flight at once;
-            // empty query slots are zero-filled.
+            // The group's queries into the swizzled B operand (row = column
+            // of the accumulator): every 16-byte chunk is its own
+            // asynchronous copy, all in flight at once; empty query slots are
+            // zero-filled.
             unsigned char* dst = sB + static_cast<size_t>(b) * nkb * BKB;
             const size_t qstride = static_cast<size_t>(nkb) * 128;
             for (int i = gt; i < QG; i += 32 * N_GATHER) {
+                const int col = group_col<QG>(i);
                 if (i < nqv) {
                     const unsigned char* src = p.qb + static_cast<size_t>(grp[i]) * qstride;
                     for (int kb = 0; kb < nkb; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            cp_async16(dst + kb * BKB + i * 128 + (((c ^ (i & 7)) & 7) << 4), src + kb * 128 + c * 16);
+                            cp_async16(dst + kb * BKB + col * 128 + (((c ^ (col & 7)) & 7) << 4),
+                                       src + kb * 128 + c * 16);
                 } else {
                     for (int kb = 0; kb < nkb; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            *reinterpret_cast<uint4*>(dst + kb * BKB + i * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
+                            *reinterpret_cast<uint4*>(dst + kb * BKB + col * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
                 }
             }
             cp_async_wait_all();
@@ -706,7 +720,9 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             const Slot& S = slot[b];
             const int ntiles = S.ntiles;
             if (ntiles < 0) break;
-            const int nqv = S.nqv, nrows = S.nrows;
+            // Occupied columns of this warp's half: [0, nact) of its CW.
+            const int nact = (S.nqv + 1 - half) >> 1;
+            const int nrows = S.nrows;
             const long long row0 = S.row0;
             bool ok = true;
             float* R = sR + e * CW;  // this warp's CW columns
@@ -732,13 +748,29 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const float xnv = rvalid ? S.xn[rs_row] : 0.0f;
                 // Rows past the slice end compare as NaN: never candidates.
                 const float ax = rvalid ? (l2 ? xnv - err_row_const(xnv, l2, p.cN) : 0.0f) : __int_as_float(0x7fffffff);
-                // This warp's CW columns in one TMEM load.
+                // This warp's occupied columns in one TMEM load (the first
+                // chunk alone when the rest are empty).
                 uint32_t u[CW];
-                tc::tmem_ld_cols<CW>(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * CW), u);
+                const uint32_t taddr =
+                    tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * CW);
+                if constexpr (CW > CC) {
+                    if (nact <= CC) {
+                        uint32_t u0[CC];
+                        tc::tmem_ld_cols<CC>(taddr, u0);
+#pragma unroll
+                        for (int j = 0; j < CC; ++j) u[j] = u0[j];
+#pragma unroll
+                        for (int j = CC; j < CW; ++j) u[j] = 0u;
+                    } else {
+                        tc::tmem_ld_cols<CW>(taddr, u);
+                    }
+                } else {
+                    tc::tmem_ld_cols<CW>(taddr, u);
+                }
 #pragma unroll
                 for (int c = 0; c < CW / CC; ++c) {
                     const int col0 = half * CW + c * CC;
-                    if (col0 >= nqv) continue;
+                    if (c * CC >= nact) continue;
                     // The chunk's test bounds (and, for e4m3, the
                     // accumulator scales) in registers.
                     float r[CC], m[CC];
