@@ -689,28 +689,29 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         const int half = e >> 2;           // columns [CW*half, CW*half+CW)
         int* wq = s_cq + e * CB;
         uint64_t* wk = s_ck + e * CB;
-        // Staged candidates of this warp: wc entries (warp-uniform, kept in
-        // a register; only this warp writes its staging rows).
-        int wc = 0;
-        auto flush = [&]() {
-            __syncwarp();
-            const int n = min(wc, CB);
-            // All of this lane's counter atomics first (independent, so their
-            // latencies overlap), then the stores that depend on them.
-            int pos[CB / 32], qid[CB / 32];
+        // Candidate staging: a ring of CB entries in NSEG segments; wc counts
+        // every candidate this warp staged (warp-uniform, in a register).
+        // When the fill crosses into a new segment, the segment just filled
+        // reserves its buffer slots (one counter atomic per entry, results
+        // kept in registers) and the oldest reserved segment, which the fill
+        // is about to overwrite, stores its entries: the atomics' latency
+        // overlaps the emission of the next segments.
+        constexpr int NSEG = 4, SEG = CB / NSEG, SJ = SEG / 32;
+        int wc = 0, npend = 0;
+        int pos0[SJ], pos1[SJ], pos2[SJ];  // reserved slots, oldest .. newest
+        auto reserve = [&](int seg, int n, int (&pos)[SJ]) {
 #pragma unroll
-            for (int j = 0; j < CB / 32; ++j) {
+            for (int j = 0; j < SJ; ++j) {
                 const int i = lane + 32 * j;
-                qid[j] = i < n ? wq[i] : 0;
-                pos[j] = i < n ? atomicAdd(&p.cand_cnt[qid[j]], 1) : p.capq;
+                pos[j] = i < n ? atomicAdd(&p.cand_cnt[wq[seg * SEG + i]], 1) : p.capq;
             }
+        };
+        auto store = [&](int seg, const int (&pos)[SJ]) {
 #pragma unroll
-            for (int j = 0; j < CB / 32; ++j) {
-                const int i = lane + 32 * j;
-                if (pos[j] < p.capq) p.cand[static_cast<int64_t>(qid[j]) * p.capq + pos[j]] = wk[i];
+            for (int j = 0; j < SJ; ++j) {
+                const int i = seg * SEG + lane + 32 * j;
+                if (pos[j] < p.capq) p.cand[static_cast<int64_t>(wq[i]) * p.capq + pos[j]] = wk[i];
             }
-            __syncwarp();
-            wc = 0;
         };
         const float cf = l2 ? -2.0f : -1.0f;
         uint32_t tile_it = 0;
@@ -817,14 +818,31 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                             const bool mine = (mask >> j) & 1u;
                             const unsigned bal = __ballot_sync(FULL, mine);
                             const int cnt = __popc(bal);
-                            if (wc + cnt > CB) flush();  // warp-uniform
+                            const bool cross = (wc + cnt) / SEG != wc / SEG;  // warp-uniform
+                            if (cross && npend == NSEG - 1) {
+                                // The segment about to be refilled: its slots
+                                // were reserved three crossings ago.
+                                store((wc / SEG + 1) % NSEG, pos0);
+                                --npend;
+                                __syncwarp();
+                            }
                             if (mine) {
                                 const int q = col0 + j;
                                 const float ip = F8 ? sip[j] * S.sc[q] : sip[j];
                                 const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
-                                const int at = wc + __popc(bal & ((1u << lane) - 1u));
+                                const int at = (wc + __popc(bal & ((1u << lane) - 1u))) & (CB - 1);
                                 wq[at] = S.qid[q];
                                 wk[at] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                            }
+                            if (cross) {
+                                __syncwarp();
+#pragma unroll
+                                for (int j = 0; j < SJ; ++j) {
+                                    pos0[j] = pos1[j];
+                                    pos1[j] = pos2[j];
+                                }
+                                reserve((wc / SEG) % NSEG, SEG, pos2);
+                                ++npend;
                             }
                             wc += cnt;
                         }
@@ -833,12 +851,19 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 tc::fence_before_sync();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cta(&acce[buf]);
-                if (wc > CB - 64) flush();
             }
-            flush();
             if (lane == 0) mbar_arrive_cta(&sfree[b]);
             if (!ok) break;
         }
+        // Drain: the reserved segments, then the partly filled one.
+        const int last = (wc / SEG + NSEG - 1) % NSEG;  // newest reserved segment
+        if (npend >= 3) store((last + NSEG - 2) % NSEG, pos0);
+        if (npend >= 2) store((last + NSEG - 1) % NSEG, pos1);
+        if (npend >= 1) store(last, pos2);
+        __syncwarp();
+        int posr[SJ];
+        reserve((wc / SEG) % NSEG, wc % SEG, posr);
+        store((wc / SEG) % NSEG, posr);
     }
     tc::fence_before_sync();
     __syncthreads();
