@@ -24,6 +24,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstddef>
 
@@ -375,6 +376,7 @@ struct BatchedParams {
     const int32_t* pair_cnt;        // [nlist]
     const float* xn;                // [arena rows] squared norms (f32)
     const float2* tile_aux;         // [arena tiles] {max |x~|, max |x - x~|} over the tile's rows
+    const float2* xaux;             // [arena rows] {|x~|, |x - x~|} (dense items' error bounds)
     const unsigned char* qb;        // [nq][nkb*128 bytes] queries in the operand type
     const float4* qaux;             // [nq] {|q|^2, |q|, |q~|, |q - q~|}
     const float* lscale;            // e4m3 form: [nlist] list scales (x~ = lscale * code), else null
@@ -385,6 +387,7 @@ struct BatchedParams {
     unsigned int* work;             // work-queue counter
     int* err;
     int nlist, nkb, rs, capq, metric;
+    int dense_max;                  // lists of at most this many rows: dense items (0 = none)
     float cK, cN;                   // error-bound constants (see err_coef)
 };
 
@@ -406,6 +409,8 @@ struct ItemSlot {
     int ntiles;  // -1 = no more items
     int nqv;
     int nrows;
+    int lrow0;   // first row of the slice within its list
+    int dense;   // 1: every row's score at its offset in the list, no threshold test
     long long row0;
     alignas(16) float xn[RS_MAX];  // |x|^2 of the slice's rows (cp.async target: 16-byte aligned)
     float2 taux[RS_MAX / TM];    // per tile {max |x~|, max |x - x~|}
@@ -414,6 +419,7 @@ struct ItemSlot {
     float V[QG];     // threshold + bound constant - |q|^2 (score units)
     float aq[QG];    // bound coefficient of |x~|
     float bq[QG];    // bound coefficient of |x - x~|
+    float cq[QG];    // bound constant
     alignas(16) float sc[QG];    // accumulator -> inner product scale (1, or list scale x query scale)
 };
 
@@ -551,9 +557,15 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             if (gt == 0) {
                 S.nqv = nqv;
                 S.nrows = nrows;
+                S.lrow0 = rsl * p.rs;
+                S.dense = sz <= p.dense_max;
                 S.row0 = row0;
                 S.ntiles = (nrows + TM - 1) / TM;
             }
+            // A dense item: the list's first slice records each query's
+            // entry count (the list size).
+            if (sz <= p.dense_max && rsl == 0)
+                for (int i = gt; i < nqv; i += 32 * N_GATHER) p.cand_cnt[grp[i]] = sz;
             // Row norms and tile bounds of the slice: asynchronous 16-byte
             // copies (the arena is padded to whole tiles, so the rounded-up
             // ranges stay inside it).
@@ -574,12 +586,14 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     S.V[col] = p.thr[qid] + ec.cq - (l2 ? qa.x : 0.0f);
                     S.aq[col] = ec.aq;
                     S.bq[col] = ec.bq;
+                    S.cq[col] = ec.cq;
                     S.sc[col] = F8 ? ls * p.qscale[qid] : 1.0f;
                 } else {
                     S.qn[col] = 0.0f;
                     S.V[col] = -INFINITY;
                     S.aq[col] = 0.0f;
                     S.bq[col] = 0.0f;
+                    S.cq[col] = 0.0f;
                     S.sc[col] = 0.0f;
                 }
             }
@@ -750,7 +764,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 // Rows past the slice end compare as NaN: never candidates.
                 const float ax = rvalid ? (l2 ? xnv - err_row_const(xnv, l2, p.cN) : 0.0f) : __int_as_float(0x7fffffff);
                 // This warp's occupied columns in one TMEM load (the first
-                // chunk alone when the rest are empty).
+                // chunk alone when the rest are empty); the accumulator is
+                // released to the MMA warp right after it.
                 uint32_t u[CW];
                 const uint32_t taddr =
                     tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(buf * QG + half * CW);
@@ -767,6 +782,32 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     }
                 } else {
                     tc::tmem_ld_cols<CW>(taddr, u);
+                }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cta(&acce[buf]);
+                if (S.dense) {
+                    // Dense item: every valid row of every occupied column
+                    // writes {score, error bound} at the row's offset in the
+                    // list (the warp's 32 rows are 256 contiguous bytes of
+                    // the query's buffer); the threshold is not consulted.
+                    // The bound is the tightening step's own expression.
+                    const int pos = S.lrow0 + rs_row;
+                    if (rvalid && pos < p.capq) {
+                        const float2 xa = p.xaux[arow];
+                        const float rc = err_row_const(xnv, l2, p.cN);
+                        float2* cf2 = reinterpret_cast<float2*>(p.cand);
+#pragma unroll
+                        for (int j = 0; j < CW; ++j) {
+                            if (j >= nact) break;
+                            const int q = half * CW + j;
+                            const float ip = F8 ? __uint_as_float(u[j]) * S.sc[q] : __uint_as_float(u[j]);
+                            const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
+                            const float eb = fmaf(xa.x, S.aq[q], fmaf(xa.y, S.bq[q], rc + S.cq[q]));
+                            cf2[static_cast<int64_t>(S.qid[q]) * p.capq + pos] = make_float2(score, eb);
+                        }
+                    }
+                    continue;
                 }
 #pragma unroll
                 for (int c = 0; c < CW / CC; ++c) {
@@ -848,9 +889,6 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                         }
                     }
                 }
-                tc::fence_before_sync();
-                __syncwarp();
-                if (lane == 0) mbar_arrive_cta(&acce[buf]);
             }
             if (lane == 0) mbar_arrive_cta(&sfree[b]);
             if (!ok) break;
@@ -890,10 +928,10 @@ __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ 
     __shared__ uint32_t sh[2];
     __shared__ int s_m;
     const bool l2 = metric == 1;
-    // Queries left by the warp kernel (w.big: count, then ids), a CTA each.
-    const int nbig = w.big[0];
+    // Queries left by the warp kernel (w.big2: count, then ids), a CTA each.
+    const int nbig = w.big2[0];
     for (int li = blockIdx.x; li < nbig; li += gridDim.x) {
-    const int qi = w.big[1 + li];
+    const int qi = w.big2[1 + li];
     __syncthreads();  // the previous query's shared state is no longer read
     const int cnt = w.cand_cnt[qi];
     if (cnt < k || cnt > capq) continue;
@@ -935,28 +973,13 @@ __global__ void __launch_bounds__(256) tighten_kernel(const float* __restrict__ 
     }
 }
 
-// Warp tighten: one warp per query with at most 1024 candidates (32 per
-// lane in registers); larger buffers go to the CTA kernel through w.big.
-constexpr int TIGHTEN_WARP_MAX = 1024;
-
-__global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restrict__ xn,
-                                                           const float2* __restrict__ xaux,
-                                                           const float4* __restrict__ qaux, int nq, BatchWork w,
-                                                           int capq, int k, int metric, float cK, float cN,
-                                                           float* __restrict__ thr) {
-    __shared__ int hist[8][256];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int qi = blockIdx.x * 8 + warp;
-    if (qi >= nq) return;  // whole warp
-    const int cnt = w.cand_cnt[qi];
-    if (cnt < k) return;
-    if (cnt > capq) return;  // overflowed: left for the re-rank to report
-    if (cnt > TIGHTEN_WARP_MAX) {
-        if (lane == 0) w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
-        return;
-    }
-    constexpr int PER = TIGHTEN_WARP_MAX / 32;
-    const bool l2 = metric == 1;
+// Warp tighten of one query with k <= cnt <= 32 * PER candidates (PER per
+// lane in registers).
+template <int PER>
+__device__ inline void tighten_warp_query(int qi, int cnt, const float* __restrict__ xn,
+                                          const float2* __restrict__ xaux, const float4* __restrict__ qaux,
+                                          const BatchWork& w, int capq, int k, bool l2, float cK, float cN,
+                                          float* __restrict__ thr, int* hist, int lane) {
     const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     uint32_t hi[PER];
@@ -976,7 +999,7 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
             lo[r] = sc - eb;
         }
     }
-    const float U = o2f(warp_radix_select<PER>(hi, cnt, k, hist[warp], lane));
+    const float U = o2f(warp_select_bound<PER>(hi, cnt, k, hist, lane));
     // In-place compaction of the candidates that can still enter the top-k:
     // every element of a round is read before any of that round's writes.
     int m = 0;
@@ -993,6 +1016,174 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
     if (lane == 0) {
         w.cand_cnt[qi] = m;
         if (U < thr[qi]) thr[qi] = U;
+    }
+}
+
+// Warp tighten of a query whose first-pass list was scanned densely: its
+// buffer holds cnt {score, error bound} pairs, entry i for row i of the list
+// (arena rows from row0).  U = an upper bound on the k-th smallest
+// score + bound with at least k entries at or below it (two 8-bit radix
+// passes below the bits all entries share; U is the upper edge of the final
+// bin that holds the k-th value); the entries with score - bound <= U are rewritten in place as keys
+// (score, arena row) at the front of the buffer.  Fewer than k entries: every
+// entry is kept and the threshold is left alone.
+__device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const BatchWork& w, int capq, int k,
+                                           float* __restrict__ thr, int* hist, int lane) {
+    uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
+    const float2* ce = reinterpret_cast<const float2*>(cq);
+    float U = INFINITY;
+    if (cnt >= k) {
+        uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll 4
+        for (int e = lane; e < cnt; e += 32) {
+            const float2 v = ce[e];
+            const uint32_t h = f2o(v.x + v.y);
+            mn = min(mn, h);
+            mx = max(mx, h);
+        }
+        mn = __reduce_min_sync(FULL, mn);
+        mx = __reduce_max_sync(FULL, mx);
+        uint32_t ub = mn;
+        if (mn != mx) {
+            // Two 8-bit radix passes below the bits every value shares.
+            int top = 31 - __clz(mn ^ mx);
+            uint32_t mask = ~((2u << top) - 1u);
+            uint32_t prefix = mn & mask;
+            int rem = k;
+#pragma unroll 1
+            for (int pass = 0; pass < 2 && top >= 0; ++pass) {
+                const int shift = top > 7 ? top - 7 : 0;
+                const uint32_t wmask = ((2u << top) - 1u) & ~((1u << shift) - 1u);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
+                __syncwarp();
+#pragma unroll 4
+                for (int e = lane; e < cnt; e += 32) {
+                    const float2 v = ce[e];
+                    const uint32_t h = f2o(v.x + v.y);
+                    if ((h & mask) == prefix) atomicAdd(&hist[(h & wmask) >> shift], 1);
+                }
+                __syncwarp();
+                int loc[8], sum = 0;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    loc[i] = hist[lane * 8 + i];
+                    sum += loc[i];
+                }
+                int incl = sum;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int excl = incl - sum;
+                const bool mine = excl < rem && incl >= rem;
+                int digit = lane * 8 + 7, before = excl;
+                if (mine) {
+                    int cum = excl;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        if (cum + loc[i] >= rem) {
+                            digit = lane * 8 + i;
+                            before = cum;
+                            break;
+                        }
+                        cum += loc[i];
+                    }
+                }
+                const int src = __ffs(__ballot_sync(FULL, mine)) - 1;
+                digit = __shfl_sync(FULL, digit, src);
+                before = __shfl_sync(FULL, before, src);
+                prefix |= static_cast<uint32_t>(digit) << shift;
+                mask |= wmask;
+                rem -= before;
+                top = shift - 1;
+                __syncwarp();
+            }
+            ub = top >= 0 ? (prefix | ((2u << top) - 1u)) : prefix;
+        }
+        U = o2f(ub);
+    }
+    // In-place rewrite: every element of a round is read before any of that
+    // round's writes, and writes never pass the round's reads.
+    int m = 0;
+    for (int base = 0; base < cnt; base += 32) {
+        const int e = base + lane;
+        const float2 v = e < cnt ? ce[e] : make_float2(0.0f, 0.0f);
+        const bool keep = e < cnt && v.x - v.y <= U;
+        const unsigned b = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep)
+            cq[m + __popc(b & ((1u << lane) - 1u))] =
+                (static_cast<uint64_t>(f2o(v.x)) << 32) | static_cast<uint32_t>(row0 + e);
+        m += __popc(b);
+    }
+    if (lane == 0) {
+        w.cand_cnt[qi] = m;
+        if (U < thr[qi]) thr[qi] = U;
+    }
+}
+
+// Warp tighten: one warp per query with at most 1024 candidates (or a dense
+// first-pass list of any size); buffers of up to 2048 go to
+// tighten_warp2_kernel through w.big, larger ones to the CTA kernel through
+// w.big2.
+constexpr int TIGHTEN_WARP_MAX = 1024;
+
+__global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restrict__ xn,
+                                                           const float2* __restrict__ xaux,
+                                                           const float4* __restrict__ qaux, int nq, BatchWork w,
+                                                           int capq, int k, int metric, float cK, float cN,
+                                                           float* __restrict__ thr, DenseFirst df) {
+    __shared__ int hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    const int cnt = w.cand_cnt[qi];
+    if (df.dense_max > 0) {
+        const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
+        if (l0 >= 0 && df.list_size[l0] <= df.dense_max) return;  // tighten_dense_kernel's
+    }
+    if (cnt < k) return;
+    if (cnt > capq) return;  // overflowed: left for the re-rank to report
+    if (cnt > TIGHTEN_WARP_MAX) {
+        if (lane == 0) {
+            if (cnt > 2 * TIGHTEN_WARP_MAX)
+                w.big2[1 + atomicAdd(&w.big2[0], 1)] = qi;
+            else
+                w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
+        }
+        return;
+    }
+    tighten_warp_query<TIGHTEN_WARP_MAX / 32>(qi, cnt, xn, xaux, qaux, w, capq, k, metric == 1, cK, cN, thr,
+                                              hist[warp], lane);
+}
+
+// Queries whose first-pass list was scanned densely, one warp each.
+__global__ void __launch_bounds__(256) tighten_dense_kernel(int nq, BatchWork w, int capq, int k,
+                                                            float* __restrict__ thr, DenseFirst df) {
+    __shared__ int hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
+    if (l0 < 0 || df.list_size[l0] > df.dense_max) return;
+    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], w, capq, k, thr, hist[warp], lane);
+}
+
+// Queries with 1025..2048 candidates (w.big), one warp each.
+__global__ void __launch_bounds__(256) tighten_warp2_kernel(const float* __restrict__ xn,
+                                                            const float2* __restrict__ xaux,
+                                                            const float4* __restrict__ qaux, BatchWork w, int capq,
+                                                            int k, int metric, float cK, float cN,
+                                                            float* __restrict__ thr) {
+    __shared__ int hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nbig = w.big[0];
+    for (int li = blockIdx.x * 8 + warp; li < nbig; li += gridDim.x * 8) {
+        const int qi = w.big[1 + li];
+        tighten_warp_query<2 * TIGHTEN_WARP_MAX / 32>(qi, w.cand_cnt[qi], xn, xaux, qaux, w, capq, k, metric == 1,
+                                                      cK, cN, thr, hist[warp], lane);
     }
 }
 
@@ -1304,12 +1495,21 @@ static void err_consts(int d, bool f8, float* cK, float* cN) {
 }
 
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s) {
+                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s,
+                           DenseFirst df) {
+    df.dense_max = std::min(df.dense_max, capq);
     float cK, cN;
     err_consts(d, f8, &cK, &cN);
     cudaError_t e = cudaMemsetAsync(w.big, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
-    tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr);
+    if ((e = cudaMemsetAsync(w.big2, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
+    if (df.dense_max > 0) {
+        tighten_dense_kernel<<<(nq + 7) / 8, 256, 0, s>>>(nq, w, capq, k, thr, df);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    tighten_warp2_kernel<<<2 * nsm, 256, 0, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t smem = static_cast<size_t>(capq) * 8;
     if ((e = cudaFuncSetAttribute(tighten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1432,6 +1632,8 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.rs = b.rs;
     p.capq = b.capq;
     p.metric = b.metric;
+    p.dense_max = std::min(b.dense_max, b.capq);
+    p.xaux = b.xaux;
     err_consts(b.d, b.f8, &p.cK, &p.cN);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s)) != cudaSuccess) return e;

@@ -56,15 +56,32 @@ struct BatchWork {
     int32_t* cand_cnt;   // [nq]
     int32_t* overflow;   // [1 + nq]: count, then query ids
     int32_t* big;        // [1 + nq]: queries re-ranked by the CTA kernel (count, then ids)
+    int32_t* big2;       // [1 + nq]: queries tightened by the CTA kernel (count, then ids)
 };
 
 // Inverts probe columns [j0, j1) of every query into per-list query groups
 // and builds the work items.
 cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
                                  const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s);
-// thr := min(thr, k-th smallest upper bound over each query's candidates).
+// The first pass's dense lists: a query whose probes[q * nprobe] list has at
+// most dense_max rows (capped at capq) holds {score, error bound} pairs, one
+// per row of that list.  dense_max 0: no dense lists.
+struct DenseFirst {
+    const int64_t* probes = nullptr;
+    int nprobe = 0;
+    const int32_t* list_size = nullptr;
+    const int64_t* list_off = nullptr;
+    int dense_max = 0;
+};
+// thr := min(thr, k-th smallest upper bound over each query's candidates),
+// and the candidates that can still reach the top-k are compacted as keys.
 cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qaux, int nq, const BatchWork& w,
-                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s);
+                           int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s,
+                           DenseFirst df);
+
+// Largest list the batched search's first pass scans densely (the candidate
+// buffer's size caps it further).
+constexpr size_t DENSE_MAX = 16384;
 
 struct BatchedLaunch {
     const void* abf;
@@ -72,6 +89,7 @@ struct BatchedLaunch {
     const int32_t* list_size;
     const float* xn;
     const float2* tile_aux;
+    const float2* xaux;  // per-row {|x~|, |x - x~|} of the operand type's image
     const void* qb;
     const float4* qaux;
     const float* thr;
@@ -80,6 +98,13 @@ struct BatchedLaunch {
     int nlist, d, rs, capq, metric, nsm;
     int qg = 128;     // queries per group (batched_group_size)
     bool f8 = false;  // e4m3 operands
+    // Lists of at most dense_max rows (capped at capq) are scanned densely:
+    // every row's {score, error bound} lands at the row's offset in the list
+    // within the query's candidate buffer, with no threshold test, and the
+    // query's count is set to the list size (each query must have one such
+    // list in the launch; launch_tighten turns them into keys).  0 = every
+    // list through the threshold test.
+    int dense_max = 0;
 };
 
 cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int* err, cudaStream_t s);

@@ -633,7 +633,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
-    HY_RET(h->b_big.ensure((qc + 1) * sizeof(int32_t)));
+    HY_RET(h->b_big.ensure(2 * (qc + 1) * sizeof(int32_t)));
     // Exact fallback on the device: up to FB_CAP overflowed queries per chunk
     // are searched again by the plain scan over the same probe lists.
     const size_t fbcap = std::min<size_t>(qc, FB_CAP);
@@ -645,7 +645,11 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_fbtot.ensure(2 * sizeof(unsigned long long)));
     HY_CUDA(cudaMemsetAsync(h->b_fbtot.p, 0, 2 * sizeof(unsigned long long), s));
     // Warm-up for the bf16 form: its threshold only bounds the first pass
-    // (each query's nearest list), so three lists suffice by default.
+    // (each query's nearest list), so three lists suffice by default.  A
+    // query whose nearest list has between k and dense_max rows needs none:
+    // the first pass scans that list densely and the tightening step takes
+    // the k-th smallest bound over all of its rows.
+    const int dense_max = (int)std::min<size_t>(capq, hy::DENSE_MAX);
     const size_t wl = h->warmup_list ? std::min<size_t>(h->warmup_list, 3) : 3;
     const size_t wls = h->warmup_list_size ? h->warmup_list_size : k;
     HY_CHECK(std::min(wl, nprobe) * wls <= 32768, HY_ERR_ARG, "presearch: warmup_list * warmup_list_size above 32768");
@@ -670,6 +674,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     w.cand = h->b_cand.as<uint64_t>();
     w.cand_cnt = h->b_ccnt.as<int32_t>();
     w.big = h->b_big.as<int32_t>();
+    w.big2 = w.big + (qc + 1);
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
@@ -688,10 +693,12 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         if (h->metric == HY_METRIC_L2) {
             HY_CUDA(hy::launch_warmup(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(), h->list_size.as<int32_t>(),
                                       qq, (int)m, h->w_probes.as<int64_t>(), (int)nprobe, (int)k, (int)wl, (int)wls, 1,
-                                      h->w_thr.as<uint32_t>(), h->b_thr.as<float>(), h->w_err.as<int>(), s));
+                                      h->w_thr.as<uint32_t>(), h->b_thr.as<float>(), h->w_err.as<int>(), s, (int)k,
+                                      dense_max));
         } else {
-            // Inner products have no warm-up threshold in the reference; the
-            // candidate buffers then hold every probed row.
+            // Inner products have no warm-up threshold in the reference: the
+            // first pass's dense lists bound the pass after it; the other
+            // lists' candidate buffers hold every probed row.
             HY_CUDA(hy::launch_fill_f32(h->b_thr.as<float>(), (int64_t)m, INFINITY, s));
         }
         HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(),
@@ -705,6 +712,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         b.list_size = h->list_size.as<int32_t>();
         b.xn = h->norms.as<float>();
         b.tile_aux = f8 ? h->t8aux.as<float2>() : h->taux.as<float2>();
+        b.xaux = f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>();
         b.lscale = f8 ? h->lscale.as<float>() : nullptr;
         b.qscale = f8 ? h->b_qs.as<float>() : nullptr;
         b.f8 = f8;
@@ -718,20 +726,29 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         b.capq = (int)capq;
         b.metric = h->metric;
         b.nsm = h->nsm;
-        // Pass 1: each query's nearest list under the warm-up threshold; the
+        // Pass 1: each query's nearest list, densely (every row) when it has
+        // at most dense_max rows, else under the warm-up threshold; the
         // threshold is then tightened to the k-th smallest candidate upper
         // bound; pass 2: the remaining probed lists under the tight threshold.
         const bool last = timed && q0 + qc >= n;
         HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
                                          h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
         if (last) HY_CUDA(ev_record(h->ev[6], s));
+        b.dense_max = dense_max;
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        b.dense_max = 0;
         if (last) HY_CUDA(ev_record(h->ev[7], s));
         if (last) h->kev = 1;
+        hy::DenseFirst df;
+        df.probes = h->w_probes.as<int64_t>();
+        df.nprobe = (int)nprobe;
+        df.list_size = h->list_size.as<int32_t>();
+        df.list_off = h->list_off.as<int64_t>();
+        df.dense_max = dense_max;
+        HY_CUDA(hy::launch_tighten(h->norms.as<float>(), f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(),
+                                   h->b_qn.as<float4>(), (int)m, w, (int)capq, (int)k, h->metric, (int)h->d, f8,
+                                   h->nsm, h->b_thr.as<float>(), s, df));
         if (nprobe > 1) {
-            HY_CUDA(hy::launch_tighten(h->norms.as<float>(), f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(),
-                                       h->b_qn.as<float4>(), (int)m, w, (int)capq, (int)k, h->metric, (int)h->d, f8,
-                                       h->nsm, h->b_thr.as<float>(), s));
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
                                              (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
             if (last) HY_CUDA(ev_record(h->ev[8], s));
@@ -754,7 +771,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
                                       dI + q0 * k, h->b_fbtot.as<unsigned long long>(),
                                       h->b_fbtot.as<unsigned long long>() + 1, s));
         h->launches += 5;
-        h->launches += nprobe > 1 ? 22 : 14;
+        h->launches += nprobe > 1 ? 24 : 18;
     }
     return HY_OK;
 }

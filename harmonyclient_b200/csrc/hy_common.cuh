@@ -204,6 +204,82 @@ __device__ inline uint32_t warp_radix_select(const uint32_t (&v)[PER], int n, in
     return prefix;
 }
 
+// An upper bound U on the k-th smallest of the warp's values (k <= n; lane l
+// holds elements r*32 + l, valid below n) with at least k values <= U: two
+// 8-bit radix passes over the bits below the prefix that every value shares
+// (found from the warp's minimum and maximum), so the passes split the values'
+// actual range; U is the upper edge of the bin that holds the k-th value,
+// within 2^(top - 15) of it in the ordered-bits order (top = the highest bit
+// in which the values differ).
+template <int PER>
+__device__ inline uint32_t warp_select_bound(const uint32_t (&v)[PER], int n, int k, int* hist, int lane) {
+    uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+    for (int r = 0; r < PER; ++r)
+        if (r * 32 + lane < n) {
+            mn = min(mn, v[r]);
+            mx = max(mx, v[r]);
+        }
+    mn = __reduce_min_sync(FULL, mn);
+    mx = __reduce_max_sync(FULL, mx);
+    if (mn == mx) return mn;
+    int top = 31 - __clz(mn ^ mx);  // highest differing bit
+    uint32_t mask = ~((2u << top) - 1u);
+    uint32_t prefix = mn & mask;
+    int rem = k;
+#pragma unroll 1
+    for (int pass = 0; pass < 2 && top >= 0; ++pass) {
+        const int shift = top > 7 ? top - 7 : 0;
+        const uint32_t wmask = ((2u << top) - 1u) & ~((1u << shift) - 1u);  // bits [shift, top]
+#pragma unroll
+        for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < PER; ++r)
+            if (r * 32 + lane < n && (v[r] & mask) == prefix) atomicAdd(&hist[(v[r] & wmask) >> shift], 1);
+        __syncwarp();
+        int loc[8], sum = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            loc[i] = hist[lane * 8 + i];
+            sum += loc[i];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - sum;
+        const bool mine = excl < rem && incl >= rem;
+        int digit = 0, before = 0;
+        if (mine) {
+            int cum = excl;
+            digit = lane * 8 + 7;
+            before = excl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (cum + loc[i] >= rem) {
+                    digit = lane * 8 + i;
+                    before = cum;
+                    break;
+                }
+                cum += loc[i];
+            }
+        }
+        const unsigned who = __ballot_sync(FULL, mine);
+        const int src = __ffs(who) - 1;
+        digit = __shfl_sync(FULL, digit, src);
+        before = __shfl_sync(FULL, before, src);
+        prefix |= static_cast<uint32_t>(digit) << shift;
+        mask |= wmask;
+        rem -= before;
+        top = shift - 1;
+        __syncwarp();
+    }
+    return top >= 0 ? (prefix | ((2u << top) - 1u)) : prefix;
+}
+
 __host__ __device__ inline int next_pow2(int x) {
     int p = 1;
     while (p < x) p <<= 1;

@@ -203,12 +203,23 @@ __global__ void argmin_kernel(const float* __restrict__ scores, int nrows, int n
 // probed lists; FLT_MAX when fewer than k rows were seen.  One CTA per query;
 // distances are collected in shared memory and the k-th found by radix
 // selection.
+// True when query qi's nearest list has between skip_lo and skip_hi rows.
+__device__ inline bool warmup_skipped(const int32_t* list_size, const int64_t* probes, int qi, int nprobe, int skip_lo,
+                                      int skip_hi) {
+    if (skip_hi < skip_lo) return false;
+    const int64_t l0 = probes[static_cast<size_t>(qi) * nprobe];
+    if (l0 < 0) return false;
+    const int sz = list_size[l0];
+    return sz >= skip_lo && sz <= skip_hi;
+}
+
 __global__ void __launch_bounds__(256) warmup_kernel(ArenaLayout L, const float* __restrict__ codes,
                                                      const int64_t* __restrict__ list_off,
                                                      const int32_t* __restrict__ list_size,
                                                      const float* __restrict__ q, const int64_t* __restrict__ probes,
                                                      int nprobe, int k, int wl, int wls, int blockwise,
-                                                     uint32_t* __restrict__ out_thr, float* __restrict__ out_f) {
+                                                     uint32_t* __restrict__ out_thr, float* __restrict__ out_f,
+                                                     int skip_lo, int skip_hi) {
     extern __shared__ __align__(16) unsigned char sm[];
     float* qs = reinterpret_cast<float*>(sm);
     int* rbase = reinterpret_cast<int*>(qs + L.row_pitch);  // [wl+1] prefix of rows
@@ -218,6 +229,13 @@ __global__ void __launch_bounds__(256) warmup_kernel(ArenaLayout L, const float*
     __shared__ uint32_t sh[2];
     const int qi = blockIdx.x;
     const int wle = min(wl, nprobe);
+    if (warmup_skipped(list_size, probes, qi, nprobe, skip_lo, skip_hi)) {
+        if (threadIdx.x == 0) {
+            out_thr[qi] = f2o(FLT_MAX);
+            if (out_f) out_f[qi] = FLT_MAX;
+        }
+        return;  // whole block
+    }
     stage_query(L, q + static_cast<size_t>(qi) * L.d, qs);
     if (threadIdx.x == 0) {
         int acc = 0;
@@ -260,7 +278,8 @@ __global__ void __launch_bounds__(256) warmup_warp_kernel(const __grid_constant_
                                                           const float* __restrict__ q,
                                                           const int64_t* __restrict__ probes, int nq, int nprobe,
                                                           int k, int wl, int wls, int blockwise,
-                                                          uint32_t* __restrict__ out_thr, float* __restrict__ out_f) {
+                                                          uint32_t* __restrict__ out_thr, float* __restrict__ out_f,
+                                                          int skip_lo, int skip_hi) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ int hist[8][256];
     __shared__ int s_base[8][33];
@@ -268,6 +287,13 @@ __global__ void __launch_bounds__(256) warmup_warp_kernel(const __grid_constant_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
+    if (warmup_skipped(list_size, probes, qi, nprobe, skip_lo, skip_hi)) {
+        if (lane == 0) {
+            out_thr[qi] = f2o(FLT_MAX);
+            if (out_f) out_f[qi] = FLT_MAX;
+        }
+        return;  // whole warp
+    }
     float* qs = reinterpret_cast<float*>(sm) + static_cast<size_t>(warp) * L.row_pitch;
     const float* src = q + static_cast<size_t>(qi) * L.d;
     for (int i = lane; i < L.row_pitch; i += 32) {
@@ -926,7 +952,8 @@ cudaError_t launch_argmin(const float* scores, int nrows, int n, int64_t* out_id
 
 cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_t* list_off,
                           const int32_t* list_size, const float* q, int nq, const int64_t* probes, int nprobe, int k,
-                          int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s) {
+                          int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s,
+                          int skip_lo, int skip_hi) {
     (void)err;
     const int wle = wl < nprobe ? wl : nprobe;
     cudaError_t e;
@@ -936,7 +963,7 @@ cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_
                                       static_cast<int>(wsmem))) != cudaSuccess)
             return e;
         warmup_warp_kernel<<<(nq + 7) / 8, 256, wsmem, s>>>(L, codes, list_off, list_size, q, probes, nq, nprobe, k,
-                                                            wl, wls, blockwise, out_thr, out_f);
+                                                            wl, wls, blockwise, out_thr, out_f, skip_lo, skip_hi);
         return cudaGetLastError();
     }
     const size_t smem = static_cast<size_t>(L.row_pitch) * 4 + static_cast<size_t>((wl + 2) & ~1) * 4 +
@@ -945,7 +972,7 @@ cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_
         cudaSuccess)
         return e;
     warmup_kernel<<<nq, 256, smem, s>>>(L, codes, list_off, list_size, q, probes, nprobe, k, wl, wls, blockwise,
-                                        out_thr, out_f);
+                                        out_thr, out_f, skip_lo, skip_hi);
     return cudaGetLastError();
 }
 

@@ -58,9 +58,13 @@ cudaError_t launch_select(const float* scores, int nq, int n, int m, int64_t* ou
                           cudaStream_t s);
 cudaError_t launch_argmin(const float* scores, int nrows, int n, int64_t* out_idx, float* out_score,
                           cudaStream_t s);
+// skip_lo <= skip_hi: a query whose nearest list has between skip_lo and
+// skip_hi rows gets no warm-up (threshold FLT_MAX); the batched search's dense
+// first pass bounds it instead.
 cudaError_t launch_warmup(const ArenaLayout& L, const float* codes, const int64_t* list_off,
                           const int32_t* list_size, const float* q, int nq, const int64_t* probes, int nprobe, int k,
-                          int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s);
+                          int wl, int wls, int blockwise, uint32_t* out_thr, float* out_f, int* err, cudaStream_t s,
+                          int skip_lo = 0, int skip_hi = -1);
 cudaError_t launch_scan_plain(const ScanParams& p, int* smem_bytes_out, cudaStream_t s);
 // rows (optional): the arena row of every result (-1 when unfilled).
 // nq_dev (optional): device count; queries at or past it are skipped.
