@@ -13,6 +13,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "hy.h")
 
 HY_OK, HY_ERR_ARG, HY_ERR_OOM, HY_ERR_CUDA, HY_ERR_TIMEOUT, HY_ERR_STATE, HY_ERR_IO, HY_ERR_UNSUPPORTED = range(8)
 HY_FORM_PLAIN, HY_FORM_BF16, HY_FORM_FP8 = 0, 1, 2
+HY_COARSE_EXACT, HY_COARSE_TENSOR = 0, 1
 HY_MAX_K = 256
 
 
@@ -75,6 +76,7 @@ def load():
     L.hy_index_presearch.argtypes = [H, sz, sz]
     L.hy_index_set_form.argtypes = [H, i]
     L.hy_index_set_batch_params.argtypes = [H, sz, sz, sz]
+    L.hy_index_set_coarse.argtypes = [H, i]
     L.hy_index_search.argtypes = [H, sz, vp, sz, vp, vp]
     L.hy_index_search_device.argtypes = [H, sz, vp, sz, vp, vp, vp]
     L.hy_index_search_preassigned.argtypes = [H, sz, vp, sz, sz, vp, vp, vp]

@@ -35,6 +35,7 @@
 namespace hy {
 namespace {
 
+constexpr int METRIC_IP = 0, METRIC_L2 = 1;  // include/hy.h's HY_METRIC_*
 constexpr int TM = 128;      // rows per tile (MMA M)
 constexpr int NS = 4;        // A stages (one 16 KiB k-block each)
 constexpr int KB_BYTES = 16384;
@@ -1019,91 +1020,96 @@ __device__ inline void tighten_warp_query(int qi, int cnt, const float* __restri
     }
 }
 
+// An upper bound U on the k-th smallest score + bound of cnt >= k dense
+// {score, bound} entries, with at least k entries at or below it: two 8-bit
+// radix passes below the bits all the entries' ordered values share; U is
+// the upper edge of the final bin that holds the k-th value.  One warp.
+__device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, int k, int* hist, int lane) {
+    uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll 4
+    for (int e = lane; e < cnt; e += 32) {
+        const float2 v = ce[e];
+        const uint32_t h = f2o(v.x + v.y);
+        mn = min(mn, h);
+        mx = max(mx, h);
+    }
+    mn = __reduce_min_sync(FULL, mn);
+    mx = __reduce_max_sync(FULL, mx);
+    uint32_t ub = mn;
+    if (mn != mx) {
+        // Two 8-bit radix passes below the bits every value shares.
+        int top = 31 - __clz(mn ^ mx);
+        uint32_t mask = ~((2u << top) - 1u);
+        uint32_t prefix = mn & mask;
+        int rem = k;
+#pragma unroll 1
+        for (int pass = 0; pass < 2 && top >= 0; ++pass) {
+            const int shift = top > 7 ? top - 7 : 0;
+            const uint32_t wmask = ((2u << top) - 1u) & ~((1u << shift) - 1u);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
+            __syncwarp();
+#pragma unroll 4
+            for (int e = lane; e < cnt; e += 32) {
+                const float2 v = ce[e];
+                const uint32_t h = f2o(v.x + v.y);
+                if ((h & mask) == prefix) atomicAdd(&hist[(h & wmask) >> shift], 1);
+            }
+            __syncwarp();
+            int loc[8], sum = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                loc[i] = hist[lane * 8 + i];
+                sum += loc[i];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - sum;
+            const bool mine = excl < rem && incl >= rem;
+            int digit = lane * 8 + 7, before = excl;
+            if (mine) {
+                int cum = excl;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (cum + loc[i] >= rem) {
+                        digit = lane * 8 + i;
+                        before = cum;
+                        break;
+                    }
+                    cum += loc[i];
+                }
+            }
+            const int src = __ffs(__ballot_sync(FULL, mine)) - 1;
+            digit = __shfl_sync(FULL, digit, src);
+            before = __shfl_sync(FULL, before, src);
+            prefix |= static_cast<uint32_t>(digit) << shift;
+            mask |= wmask;
+            rem -= before;
+            top = shift - 1;
+            __syncwarp();
+        }
+        ub = top >= 0 ? (prefix | ((2u << top) - 1u)) : prefix;
+    }
+    return o2f(ub);
+}
+
 // Warp tighten of a query whose first-pass list was scanned densely: its
 // buffer holds cnt {score, error bound} pairs, entry i for row i of the list
 // (arena rows from row0).  U = an upper bound on the k-th smallest
 // score + bound with at least k entries at or below it (two 8-bit radix
 // passes below the bits all entries share; U is the upper edge of the final
-// bin that holds the k-th value); the entries with score - bound <= U are rewritten in place as keys
-// (score, arena row) at the front of the buffer.  Fewer than k entries: every
-// entry is kept and the threshold is left alone.
+// bin that holds the k-th value); the entries with score - bound <= U are
+// rewritten in place as keys (score, arena row) at the front of the buffer.
+// Fewer than k entries: every entry is kept and the threshold is left alone.
 __device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const BatchWork& w, int capq, int k,
                                            float* __restrict__ thr, int* hist, int lane) {
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     const float2* ce = reinterpret_cast<const float2*>(cq);
-    float U = INFINITY;
-    if (cnt >= k) {
-        uint32_t mn = 0xffffffffu, mx = 0u;
-#pragma unroll 4
-        for (int e = lane; e < cnt; e += 32) {
-            const float2 v = ce[e];
-            const uint32_t h = f2o(v.x + v.y);
-            mn = min(mn, h);
-            mx = max(mx, h);
-        }
-        mn = __reduce_min_sync(FULL, mn);
-        mx = __reduce_max_sync(FULL, mx);
-        uint32_t ub = mn;
-        if (mn != mx) {
-            // Two 8-bit radix passes below the bits every value shares.
-            int top = 31 - __clz(mn ^ mx);
-            uint32_t mask = ~((2u << top) - 1u);
-            uint32_t prefix = mn & mask;
-            int rem = k;
-#pragma unroll 1
-            for (int pass = 0; pass < 2 && top >= 0; ++pass) {
-                const int shift = top > 7 ? top - 7 : 0;
-                const uint32_t wmask = ((2u << top) - 1u) & ~((1u << shift) - 1u);
-#pragma unroll
-                for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
-                __syncwarp();
-#pragma unroll 4
-                for (int e = lane; e < cnt; e += 32) {
-                    const float2 v = ce[e];
-                    const uint32_t h = f2o(v.x + v.y);
-                    if ((h & mask) == prefix) atomicAdd(&hist[(h & wmask) >> shift], 1);
-                }
-                __syncwarp();
-                int loc[8], sum = 0;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    loc[i] = hist[lane * 8 + i];
-                    sum += loc[i];
-                }
-                int incl = sum;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(FULL, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                const int excl = incl - sum;
-                const bool mine = excl < rem && incl >= rem;
-                int digit = lane * 8 + 7, before = excl;
-                if (mine) {
-                    int cum = excl;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        if (cum + loc[i] >= rem) {
-                            digit = lane * 8 + i;
-                            before = cum;
-                            break;
-                        }
-                        cum += loc[i];
-                    }
-                }
-                const int src = __ffs(__ballot_sync(FULL, mine)) - 1;
-                digit = __shfl_sync(FULL, digit, src);
-                before = __shfl_sync(FULL, before, src);
-                prefix |= static_cast<uint32_t>(digit) << shift;
-                mask |= wmask;
-                rem -= before;
-                top = shift - 1;
-                __syncwarp();
-            }
-            ub = top >= 0 ? (prefix | ((2u << top) - 1u)) : prefix;
-        }
-        U = o2f(ub);
-    }
+    const float U = cnt >= k ? dense_kth_bound(ce, cnt, k, hist, lane) : INFINITY;
     // In-place rewrite: every element of a round is read before any of that
     // round's writes, and writes never pass the round's reads.
     int m = 0;
@@ -1184,6 +1190,240 @@ __global__ void __launch_bounds__(256) tighten_warp2_kernel(const float* __restr
         const int qi = w.big[1 + li];
         tighten_warp_query<2 * TIGHTEN_WARP_MAX / 32>(qi, w.cand_cnt[qi], xn, xaux, qaux, w, capq, k, metric == 1,
                                                       cK, cN, thr, hist[warp], lane);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The coarse quantiser on the tensor cores.  The centroids form a one-list
+// index of their own (rows padded to whole 128-row tiles with zeros): its
+// bf16 image, per-row {|c~|, |c - c~|}, squared norms (the sequential f32
+// sum the arena's rows get) and per-tile maxima.
+__global__ void rowmajor_image_kernel(const float* __restrict__ x, int64_t n, int d, int nkb, int64_t rows,
+                                      unsigned char* __restrict__ out) {
+    const int w = nkb * 64;
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= rows * w) return;
+    const int64_t r = i / w;
+    const int j = static_cast<int>(i % w);
+    const float v = (r < n && j < d) ? x[r * d + j] : 0.0f;
+    unsigned char* dst =
+        out + ((r >> 7) * nkb + (j >> 6)) * KB_BYTES + tc::kblock_offset(static_cast<uint32_t>(r & 127), j & 63);
+    *reinterpret_cast<__nv_bfloat16*>(dst) = __float2bfloat16_rn(v);
+}
+
+__global__ void rowmajor_aux_kernel(const float* __restrict__ x, int64_t n, int d, int64_t rows,
+                                    float2* __restrict__ aux, float* __restrict__ xn) {
+    const int lane = threadIdx.x & 31;
+    const int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (r >= rows) return;
+    float nn = 0.0f, ee = 0.0f;
+    if (r < n)
+        for (int j = lane; j < d; j += 32) {
+            const float v = x[r * d + j];
+            const float vb = __bfloat162float(__float2bfloat16_rn(v));
+            nn = fmaf(vb, vb, nn);
+            ee = fmaf(v - vb, v - vb, ee);
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nn += __shfl_xor_sync(FULL, nn, o);
+        ee += __shfl_xor_sync(FULL, ee, o);
+    }
+    if (lane == 0) {
+        float sq = 0.0f;
+        if (r < n)
+            for (int j = 0; j < d; ++j) sq = __fadd_rn(sq, __fmul_rn(x[r * d + j], x[r * d + j]));
+        aux[r] = make_float2(sqrtf(nn), sqrtf(ee));
+        xn[r] = sq;
+    }
+}
+
+// Work of one coarse launch: every query in the centroid list's groups, each
+// group split into nslices row slices.
+__global__ void coarse_items_kernel(int nq, int nlist, int64_t rows, int ngroups, int nslices,
+                                    int64_t* __restrict__ list_off, int32_t* __restrict__ list_size, BatchWork w) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t nitems = static_cast<int64_t>(ngroups) * nslices;
+    if (i < nq) w.pairs[i] = static_cast<int32_t>(i);
+    if (i < nitems) w.items[i] = make_int4(0, static_cast<int>(i / nslices), static_cast<int>(i % nslices), 0);
+    if (i == 0) {
+        list_off[0] = 0;
+        list_off[1] = rows;
+        list_size[0] = nlist;
+        w.pair_cnt[0] = nq;
+        w.pair_off[0] = 0;
+        w.pair_off[1] = nq;
+        w.item_off[0] = 0;
+        w.item_off[1] = nitems;
+    }
+}
+
+// Staging row pitch of coarse_refine_kernel (floats): d + 4 when d is a
+// multiple of 4 (16-byte rows), else d + 1 (conflict-free column reads).
+__host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4 : d + 1; }
+
+// Exact coarse selection from the tensor-core scores.  Per query (one warp):
+// cand holds nlist {score, error bound} pairs (held in registers, PER per
+// lane); U = an upper bound on the m-th smallest score + bound
+// (warp_select_bound); every centroid whose score - bound <= U (a set that
+// holds the exact m best, ties included) gets its exact FP32 coarse score
+// with the same sequential arithmetic as coarse_scores_kernel (dimension
+// order, separately rounded operations), and the m best (score, centroid)
+// keys, ascending with ties to the lower centroid, are written as
+// select_warp_kernel writes them.  The candidate keys overwrite the query's
+// pairs in cand.  Shared memory per warp: 256 histogram bins, the query and
+// a 32-row staging block of centroids.
+template <int METRIC, int PER>
+__global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
+                                                            const float* __restrict__ q,
+                                                            const float* __restrict__ cent, int d, int m,
+                                                            int64_t* __restrict__ out_idx,
+                                                            float* __restrict__ out_score) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pitch = refine_pitch(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
+    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
+    int* hist = reinterpret_cast<int*>(base);
+    float* qs = reinterpret_cast<float*>(hist + 256);
+    float* stage = qs + pitch;
+    const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (qi >= nq) return;  // whole warp
+    const float* qrow = q + static_cast<size_t>(qi) * d;
+    for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
+    // Every centroid's upper bound (ordered bits) and lower bound in
+    // registers: entry r * 32 + lane.  The query's pairs are then free and
+    // their space holds its candidate keys.
+    float2* ce = cand + static_cast<int64_t>(qi) * nlist;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(ce);
+    uint32_t hi[PER];
+    float lo[PER];
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        hi[r] = 0xffffffffu;
+        lo[r] = INFINITY;
+        if (e < nlist) {
+            const float2 v = ce[e];
+            hi[r] = f2o(v.x + v.y);
+            lo[r] = v.x - v.y;
+        }
+    }
+    const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
+    __syncwarp();  // every pair has been read before the first key is written
+    // Centroids that can be among the m best.
+    int c = 0;
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        const bool keep = e < nlist && lo[r] <= U;
+        const unsigned bal = __ballot_sync(FULL, keep);
+        if (keep) keys[c + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint64_t>(e);
+        c += __popc(bal);
+    }
+    __syncwarp();
+    // Their exact scores, 32 at a time: the rows are staged in shared memory
+    // by asynchronous copies (all in flight at once), then lane i sums row i
+    // in dimension order.  With d a multiple of 4 the copies and the reads
+    // are 16 bytes wide (row pitch d + 4: a 512-byte read by the warp takes
+    // the minimum four shared-memory wavefronts).
+    const bool v4 = (d & 3) == 0;
+    for (int c0 = 0; c0 < c; c0 += 32) {
+        const int nr = min(32, c - c0);
+        const int cidr = lane < nr ? static_cast<int>(keys[c0 + lane]) : 0;
+        for (int r = 0; r < nr; ++r) {
+            const float* src = cent + static_cast<size_t>(__shfl_sync(FULL, cidr, r)) * d;
+            float* dst = stage + r * pitch;
+            if (v4)
+                for (int j = 4 * lane; j < d; j += 128) cp_async16(dst + j, src + j);
+            else
+                for (int j = lane; j < d; j += 32) cp_async4(dst + j, src + j);
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        if (lane < nr) {
+            const float* row = stage + lane * pitch;
+            float acc = 0.0f;
+            if (v4) {
+#pragma unroll 4
+                for (int jj = 0; jj < d; jj += 4) {
+                    const float4 a = *reinterpret_cast<const float4*>(qs + jj);
+                    const float4 b = *reinterpret_cast<const float4*>(row + jj);
+                    if (METRIC == METRIC_L2) {
+                        acc = sq_add(acc, a.x, b.x);
+                        acc = sq_add(acc, a.y, b.y);
+                        acc = sq_add(acc, a.z, b.z);
+                        acc = sq_add(acc, a.w, b.w);
+                    } else {
+                        acc = ip_add(acc, a.x, b.x);
+                        acc = ip_add(acc, a.y, b.y);
+                        acc = ip_add(acc, a.z, b.z);
+                        acc = ip_add(acc, a.w, b.w);
+                    }
+                }
+            } else {
+                for (int jj = 0; jj < d; ++jj)
+                    acc = METRIC == METRIC_L2 ? sq_add(acc, qs[jj], row[jj]) : ip_add(acc, qs[jj], row[jj]);
+            }
+            const float score = METRIC == METRIC_L2 ? acc : -acc;
+            const uint64_t cid = keys[c0 + lane];
+            keys[c0 + lane] = (static_cast<uint64_t>(f2o(score)) << 32) | cid;
+        }
+        __syncwarp();
+    }
+    // The m smallest keys, ascending.  Up to 128 candidates: each key's rank
+    // is the number of smaller keys (keys are distinct: the centroid is in
+    // the low bits), and it goes to that position.
+    if (c <= 128) {
+        uint64_t kk[4];
+        int rank[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int e = r * 32 + lane;
+            kk[r] = e < c ? keys[e] : KEY_MAX;
+            rank[r] = 0;
+        }
+#pragma unroll 4
+        for (int j = 0; j < c; ++j) {
+            const uint64_t kj = keys[j];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) rank[r] += kj < kk[r] ? 1 : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (r * 32 + lane < c && rank[r] < m) {
+                out_idx[static_cast<int64_t>(qi) * m + rank[r]] = static_cast<int64_t>(kk[r] & 0xffffffffu);
+                if (out_score)
+                    out_score[static_cast<int64_t>(qi) * m + rank[r]] = o2f(static_cast<uint32_t>(kk[r] >> 32));
+            }
+        }
+        return;
+    }
+    // More: sorted blocks of 256 merged into the running best 256.
+    uint64_t t[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = r * 32 + lane;
+        t[r] = e < c ? keys[e] : KEY_MAX;
+    }
+    warp_sort<8>(t, lane);
+    for (int c0 = 256; c0 < c; c0 += 256) {
+        uint64_t u[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int e = c0 + r * 32 + lane;
+            u[r] = e < c ? keys[e] : KEY_MAX;
+        }
+        warp_sort<8>(u, lane);
+        warp_merge<8>(t, u, lane);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int e = r * 32 + lane;
+        if (e < m) {
+            out_idx[static_cast<int64_t>(qi) * m + e] = static_cast<int64_t>(t[r] & 0xffffffffu);
+            if (out_score) out_score[static_cast<int64_t>(qi) * m + e] = o2f(static_cast<uint32_t>(t[r] >> 32));
+        }
     }
 }
 
@@ -1529,6 +1769,52 @@ cudaError_t launch_fb_scatter(const int32_t* ovf, const float* fD, const int64_t
                               int64_t* I, unsigned long long* total, unsigned long long* unresolved, cudaStream_t s) {
     fb_scatter_kernel<<<64, 128, 0, s>>>(ovf, fD, fI, k, cap, D, I, total, unresolved);
     return cudaGetLastError();
+}
+
+cudaError_t launch_centroid_image(const float* cent, int nlist, int d, void* img, float2* aux, float2* tile_aux,
+                                  float* xn, cudaStream_t s) {
+    const int64_t rows = (static_cast<int64_t>(nlist) + TM - 1) / TM * TM;
+    const int nkb = (d + 63) / 64;
+    rowmajor_image_kernel<<<grid_for(rows * nkb * 64, 256), 256, 0, s>>>(cent, nlist, d, nkb, rows,
+                                                                         static_cast<unsigned char*>(img));
+    rowmajor_aux_kernel<<<grid_for(rows * 32, 256), 256, 0, s>>>(cent, nlist, d, rows, aux, xn);
+    tile_aux_kernel<<<grid_for(rows / TM * 32, 256), 256, 0, s>>>(aux, rows / TM, tile_aux);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int64_t* list_off, int32_t* list_size,
+                                const BatchWork& w, cudaStream_t s) {
+    const int64_t rows = (static_cast<int64_t>(nlist) + TM - 1) / TM * TM;
+    const int64_t n = std::max<int64_t>(nq, static_cast<int64_t>(ngroups) * nslices);
+    coarse_items_kernel<<<grid_for(std::max<int64_t>(n, 1), 256), 256, 0, s>>>(nq, nlist, rows, ngroups, nslices,
+                                                                              list_off, list_size, w);
+    return cudaGetLastError();
+}
+
+size_t coarse_refine_smem(int nlist, int d, int warps) {
+    const int pitch = refine_pitch(d);
+    (void)nlist;
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
+    return static_cast<size_t>(warps) * ((per_warp + 15) & ~size_t(15));
+}
+
+cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent, int d,
+                                 int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s) {
+    int warps = 4;
+    while (warps > 1 && coarse_refine_smem(nlist, d, warps) > 200 * 1024) warps >>= 1;
+    const size_t smem = coarse_refine_smem(nlist, d, warps);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    const dim3 grid((nq + warps - 1) / warps);
+    auto run = [&](auto kern) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        kern<<<grid, 32 * warps, smem, s>>>(cand, nq, nlist, q, cent, d, m, out_idx, out_score);
+        return cudaGetLastError();
+    };
+    if (nlist > 2048) return cudaErrorInvalidValue;
+    if (metric == METRIC_L2)
+        return nlist <= 1024 ? run(coarse_refine_kernel<METRIC_L2, 32>) : run(coarse_refine_kernel<METRIC_L2, 64>);
+    return nlist <= 1024 ? run(coarse_refine_kernel<METRIC_IP, 32>) : run(coarse_refine_kernel<METRIC_IP, 64>);
 }
 
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s) {

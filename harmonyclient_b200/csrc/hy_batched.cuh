@@ -79,6 +79,25 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
                            int capq, int k, int metric, int d, bool f8, int nsm, float* thr, cudaStream_t s,
                            DenseFirst df);
 
+// The coarse quantiser on the tensor cores (bf16 form).  The centroids
+// (row-major, nlist x d) as a one-list index: bf16 image, per-row
+// {|c~|, |c - c~|}, per-tile maxima and squared norms, rows padded to whole
+// 128-row tiles (img: bf16_image_bytes(rows), aux/xn: rows, tile_aux: rows/128).
+cudaError_t launch_centroid_image(const float* cent, int nlist, int d, void* img, float2* aux, float2* tile_aux,
+                                  float* xn, cudaStream_t s);
+// Work of one coarse launch over nq queries: list_off[2], list_size[1] of the
+// centroid index; w.pairs [nq], w.items [ngroups*nslices], w.pair_cnt [1],
+// w.pair_off [2], w.item_off [2].
+cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int64_t* list_off, int32_t* list_size,
+                                const BatchWork& w, cudaStream_t s);
+// From the dense {score, bound} pairs of the coarse launch (cand, nq x nlist):
+// the exact m best centroids per query and their exact coarse scores, as
+// launch_select gives them from coarse_scores (cand is overwritten).  Needs m <= 256 and
+// coarse_refine_smem(nlist, d, 1) <= 200 KiB.
+size_t coarse_refine_smem(int nlist, int d, int warps);
+cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent, int d,
+                                 int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
+
 // Largest list the batched search's first pass scans densely (the candidate
 // buffer's size caps it further).
 constexpr size_t DENSE_MAX = 16384;

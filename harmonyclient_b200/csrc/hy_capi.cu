@@ -189,6 +189,13 @@ struct hy_index {
     DevBuf b_big;             // queries re-ranked by the CTA kernel
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
     DevBuf b_fq, b_fpr, b_fD, b_fI, b_fcnt, b_fbtot;  // device-side exact fallback
+    // coarse quantiser on the tensor cores (bf16 form): the centroids as a
+    // one-list index (image, row aux, tile aux, norms, list offsets/sizes)
+    // and the work of one launch
+    int coarse_mode = HY_COARSE_TENSOR;
+    bool cimg_valid = false;
+    DevBuf c_img, c_aux, c_taux, c_norm, c_off, c_size;
+    DevBuf c_pcnt, c_poff, c_pairs, c_ioff, c_items, c_work, c_cand, c_ccnt;
 
     // learned probe predictor
     bool model_ready = false;
@@ -275,6 +282,7 @@ int kmeans_device(hy_index* h, const float* xs, size_t ns, const std::vector<int
     HY_CUDA(cudaMemcpyAsync(h->h_cent.data(), h->cent.p, nlist * d * sizeof(float), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
     h->trained = true;
+    h->cimg_valid = false;
     return HY_OK;
 }
 
@@ -596,6 +604,89 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
     return HY_OK;
 }
 
+// Whether the bf16 form's coarse step runs on the tensor cores (the
+// conditions launch_coarse_refine's shared memory and select width need).
+bool coarse_on_tensor(const hy_index* h, size_t nprobe) {
+    return h->coarse_mode == HY_COARSE_TENSOR && h->form == HY_FORM_BF16 && h->nlist <= 2048 && nprobe <= 256 &&
+           h->d <= 256 && hy::batched_group_size((int)h->d, false) > 0;
+}
+
+int ensure_centroid_image(hy_index* h, cudaStream_t s) {
+    if (h->cimg_valid) return HY_OK;
+    const size_t rows = (h->nlist + hy::BATCH_ROW_ALIGN - 1) / hy::BATCH_ROW_ALIGN * hy::BATCH_ROW_ALIGN;
+    HY_RET(h->c_img.ensure(hy::bf16_image_bytes((int64_t)rows, (int)h->d)));
+    HY_RET(h->c_aux.ensure(rows * sizeof(float2)));
+    HY_RET(h->c_taux.ensure(rows / hy::BATCH_ROW_ALIGN * sizeof(float2)));
+    HY_RET(h->c_norm.ensure(rows * sizeof(float)));
+    HY_RET(h->c_off.ensure(2 * sizeof(int64_t)));
+    HY_RET(h->c_size.ensure(sizeof(int32_t)));
+    HY_CUDA(hy::launch_centroid_image(h->cent.as<float>(), (int)h->nlist, (int)h->d, h->c_img.p, h->c_aux.as<float2>(),
+                                      h->c_taux.as<float2>(), h->c_norm.as<float>(), s));
+    h->cimg_valid = true;
+    return HY_OK;
+}
+
+// Coarse step on the tensor cores for m queries whose bf16 image and
+// {|q|^2, |q|, |q~|, |q - q~|} are in b_qb / b_qn: one dense batched launch
+// over the centroid index, then the exact m best per query.
+int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t* probes, float* pscore,
+                  cudaStream_t s) {
+    HY_RET(ensure_centroid_image(h, s));
+    const int nlist = (int)h->nlist;
+    const int qg = hy::batched_group_size((int)h->d, false);
+    const int ngroups = (int)((m + qg - 1) / qg);
+    // Enough row slices to give every SM an item, each at most 2048 rows.
+    const int tiles = (nlist + 127) / 128;
+    int nslices = std::min(tiles, std::max(1, (h->nsm + ngroups - 1) / ngroups));
+    nslices = std::max(nslices, (tiles + 15) / 16);
+    const int rs = (tiles + nslices - 1) / nslices * 128;
+    nslices = (nlist + rs - 1) / rs;
+    HY_RET(h->c_pcnt.ensure(sizeof(int32_t)));
+    HY_RET(h->c_poff.ensure(2 * sizeof(int64_t)));
+    HY_RET(h->c_pairs.ensure(m * sizeof(int32_t)));
+    HY_RET(h->c_ioff.ensure(2 * sizeof(int64_t)));
+    HY_RET(h->c_items.ensure((size_t)ngroups * nslices * sizeof(int4)));
+    HY_RET(h->c_work.ensure(sizeof(unsigned int)));
+    HY_RET(h->c_cand.ensure(m * nlist * sizeof(float2)));
+    HY_RET(h->c_ccnt.ensure(m * sizeof(int32_t)));
+    hy::BatchWork w{};
+    w.items = h->c_items.as<int4>();
+    w.item_cap = (int64_t)ngroups * nslices;
+    w.pair_cnt = h->c_pcnt.as<int32_t>();
+    w.pair_off = h->c_poff.as<int64_t>();
+    w.pairs = h->c_pairs.as<int32_t>();
+    w.item_off = h->c_ioff.as<int64_t>();
+    w.work = h->c_work.as<unsigned int>();
+    w.cand = h->c_cand.as<uint64_t>();
+    w.cand_cnt = h->c_ccnt.as<int32_t>();
+    HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, nslices, h->c_off.as<int64_t>(), h->c_size.as<int32_t>(), w,
+                                    s));
+    hy::BatchedLaunch b;
+    b.abf = h->c_img.p;
+    b.list_off = h->c_off.as<int64_t>();
+    b.list_size = h->c_size.as<int32_t>();
+    b.xn = h->c_norm.as<float>();
+    b.tile_aux = h->c_taux.as<float2>();
+    b.xaux = h->c_aux.as<float2>();
+    b.qb = h->b_qb.p;
+    b.qaux = h->b_qn.as<float4>();
+    b.thr = h->b_thr.as<float>();  // not read by a dense launch's test
+    b.nlist = 1;
+    b.d = (int)h->d;
+    b.rs = rs;
+    b.capq = nlist;
+    b.metric = h->metric;
+    b.nsm = h->nsm;
+    b.qg = qg;
+    b.f8 = false;
+    b.dense_max = nlist;
+    HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+    HY_CUDA(hy::launch_coarse_refine(reinterpret_cast<float2*>(h->c_cand.p), (int)m, nlist, qq,
+                                     h->cent.as<float>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+    h->launches += 3;
+    return HY_OK;
+}
+
 // Batched bf16 search of n device queries: coarse quantisation, warm-up
 // thresholds, probe inversion, the persistent tensor-core scan and the exact
 // re-rank, in query chunks sized so the candidate buffers stay within 2 GiB.
@@ -681,10 +772,18 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then chunk-local query ids
         HY_CUDA(cudaMemsetAsync(w.overflow, 0, sizeof(int32_t), s));
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
-        HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
-                                         h->w_scores.as<float>(), s));
-        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe, h->w_probes.as<int64_t>(),
-                                  learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(),
+                                        f8 ? h->b_qs.as<float>() : nullptr, s));
+        if (coarse_on_tensor(h, nprobe)) {
+            HY_RET(coarse_tensor(h, m, qq, nprobe, h->w_probes.as<int64_t>(),
+                                 learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        } else {
+            HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)nlist, (int)h->d, h->metric,
+                                             h->w_scores.as<float>(), s));
+            HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)nlist, (int)nprobe,
+                                      h->w_probes.as<int64_t>(), learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+            h->launches += 2;
+        }
         if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s, nullptr, q0));
         if (h->q_nprobe) {
             HY_CUDA(hy::launch_cut_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, h->q_nprobe + q0, s));
@@ -701,8 +800,6 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
             // lists' candidate buffers hold every probed row.
             HY_CUDA(hy::launch_fill_f32(h->b_thr.as<float>(), (int64_t)m, INFINITY, s));
         }
-        HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(),
-                                        f8 ? h->b_qs.as<float>() : nullptr, s));
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[1], s));
         HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[2], s));
@@ -770,7 +867,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         HY_CUDA(hy::launch_fb_scatter(w.overflow, h->b_fD.as<float>(), h->b_fI.as<int64_t>(), (int)k, fb, dD + q0 * k,
                                       dI + q0 * k, h->b_fbtot.as<unsigned long long>(),
                                       h->b_fbtot.as<unsigned long long>() + 1, s));
-        h->launches += 5;
+        h->launches += 3;
         h->launches += nprobe > 1 ? 24 : 18;
     }
     return HY_OK;
@@ -1040,6 +1137,7 @@ int hy_index_set_centroids(hy_index* h, const float* c) {
     h->h_cent.assign(c, c + h->nlist * h->d);
     HY_CUDA(cudaMemcpy(h->cent.p, c, bytes, cudaMemcpyHostToDevice));
     h->trained = true;
+    h->cimg_valid = false;
     return HY_OK;
 }
 
@@ -1098,6 +1196,14 @@ int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_
                  "set_batch_params: row_slice must be a multiple of 128, at most 2048");
         h->row_slice = row_slice;
     }
+    return HY_OK;
+}
+
+int hy_index_set_coarse(hy_index* h, int mode) {
+    HY_CHECK(h, HY_ERR_ARG, "set_coarse: NULL handle");
+    HY_CHECK(mode == HY_COARSE_EXACT || mode == HY_COARSE_TENSOR, HY_ERR_ARG, "set_coarse: unknown mode");
+    h->epoch++;  // a captured search graph no longer matches
+    h->coarse_mode = mode;
     return HY_OK;
 }
 
@@ -1671,13 +1777,28 @@ int hy_index_probes(hy_index* h, size_t n, const float* q, int64_t* probes) {
         HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
     }
     HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    const bool tensor = coarse_on_tensor(h, nprobe);
+    if (tensor) {
+        HY_RET(ensure_common(h));
+        if (h->nsm == 0) HY_CUDA(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+        HY_RET(h->b_qb.ensure(qc * ((h->d + 63) / 64) * 128));
+        HY_RET(h->b_qn.ensure(qc * sizeof(float4)));
+        HY_RET(h->b_thr.ensure(qc * sizeof(float)));
+    }
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
-        HY_CUDA(hy::launch_coarse_scores(h->w_q.as<float>() + q0 * h->d, (int)m, h->cent.as<float>(), (int)h->nlist,
-                                         (int)h->d, h->metric, h->w_scores.as<float>(), s));
-        HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
-                                  h->w_probes.as<int64_t>() + q0 * nprobe,
-                                  learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        const float* qq = h->w_q.as<float>() + q0 * h->d;
+        if (tensor) {
+            HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(), nullptr, s));
+            HY_RET(coarse_tensor(h, m, qq, nprobe, h->w_probes.as<int64_t>() + q0 * nprobe,
+                                 learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        } else {
+            HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d, h->metric,
+                                             h->w_scores.as<float>(), s));
+            HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,
+                                      h->w_probes.as<int64_t>() + q0 * nprobe,
+                                      learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
+        }
         if (learned_on(h)) HY_RET(apply_learned_probes(h, m, nprobe, s, h->w_probes.as<int64_t>() + q0 * nprobe));
     }
     HY_CUDA(cudaMemcpyAsync(probes, h->w_probes.p, n * nprobe * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -1959,6 +2080,7 @@ int hy_index_load(hy_index* h, const char* path) {
     h->h_cent = f.cent;
     HY_CUDA(cudaMemcpyAsync(h->cent.p, h->h_cent.data(), h->nlist * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
     h->trained = true;
+    h->cimg_valid = false;
     // Rows list by list in file order; a later record of the same list
     // replaces an earlier one, as load_IVF does.
     std::vector<const FileList*> byid(h->nlist, nullptr);

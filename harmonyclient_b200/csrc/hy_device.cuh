@@ -66,6 +66,11 @@ __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ inline void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+// 4-byte asynchronous copy global -> shared (through L1), both addresses
+// 4-byte aligned; cp_async_wait_all covers it too.
+__device__ inline void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Plain arrival (count 1) on a CTA-local mbarrier.

@@ -126,6 +126,14 @@ class Index:
         f = {"plain": _lib.HY_FORM_PLAIN, "bf16": _lib.HY_FORM_BF16, "fp8": _lib.HY_FORM_FP8}.get(form, form)
         check(self._L.hy_index_set_form(self._h, int(f)))
 
+    def set_coarse(self, mode):
+        """The bf16 form's coarse step: 'tensor' (default; bf16 tensor-core
+        scores with error bounds, exact FP32 scores only for the centroids
+        that can reach the nprobe best) or 'exact' (exact FP32 scores of every
+        centroid).  Both give the same probe lists."""
+        m = {"exact": _lib.HY_COARSE_EXACT, "tensor": _lib.HY_COARSE_TENSOR}.get(mode, mode)
+        check(self._L.hy_index_set_coarse(self._h, int(m)))
+
     def set_batch_params(self, capq=0, oversample=0, row_slice=0):
         check(self._L.hy_index_set_batch_params(self._h, int(capq), int(oversample), int(row_slice)))
 

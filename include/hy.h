@@ -153,6 +153,18 @@ HY_API int hy_index_set_form(hy_index* h, int form);
  * most 3 warm-up lists (its warm-up threshold only bounds the first pass). */
 HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice);
 
+/* Coarse quantiser of the bf16 form (no counterpart in the reference, which
+ * scores every centroid exactly, src/Index.cpp:985-990).  HY_COARSE_EXACT:
+ * exact FP32 scores of every centroid, then the nprobe best.
+ * HY_COARSE_TENSOR (default): bf16 tensor-core scores of every centroid with
+ * rigorous error bounds, then exact FP32 scores only for the centroids whose
+ * bound can reach the nprobe-th best; the probe lists (and the learned
+ * predictor's coarse scores) are identical to HY_COARSE_EXACT's.  Used when
+ * nlist <= 2048, nprobe <= 256 and d <= 256; otherwise the exact path runs.
+ * The plain and e4m3 forms always use the exact path. */
+enum { HY_COARSE_EXACT = 0, HY_COARSE_TENSOR = 1 };
+HY_API int hy_index_set_coarse(hy_index* h, int mode);
+
 /* Warm-up threshold parameters.  Mirrors Index::preSearch's warmUpSearchList /
  * warmUpSearchListSize (src/Index.h:90, src/Index.cpp:45-55): when
  * warmup_list > 0, each query's pruning threshold starts at the k-th best
