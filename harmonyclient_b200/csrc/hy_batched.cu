@@ -225,13 +225,16 @@ __global__ void prep_queries_f8_kernel(const float* __restrict__ q, int nq, int 
 // Queries: bf16 rows padded to nkb*64, and per query {|q|^2 (sequential f32,
 // the exact arithmetic's value), |q|, |q~|, |q - q~|}.
 __global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, int nkb,
-                                    __nv_bfloat16* __restrict__ qb, float4* __restrict__ qaux) {
+                                    __nv_bfloat16* __restrict__ qb, float4* __restrict__ qaux, float amax,
+                                    int32_t* __restrict__ qexact) {
     const int i = blockIdx.x;
     if (i >= nq) return;
     const float* src = q + static_cast<size_t>(i) * d;
     float nn = 0.0f, ee = 0.0f;
+    bool integral = true;
     for (int j = threadIdx.x; j < nkb * 64; j += blockDim.x) {
         const float v = j < d ? src[j] : 0.0f;
+        integral = integral && v == rintf(v) && fabsf(v) <= 256.0f;
         const __nv_bfloat16 b = __float2bfloat16_rn(v);
         qb[static_cast<size_t>(i) * nkb * 64 + j] = b;
         const float vb = __bfloat162float(b);
@@ -248,7 +251,7 @@ __global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, 
         red[0][threadIdx.x >> 5] = nn;
         red[1][threadIdx.x >> 5] = ee;
     }
-    __syncthreads();
+    const int all_integral = __syncthreads_and(integral ? 1 : 0);
     if (threadIdx.x == 0) {
         float s = 0.0f;
         for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(src[j], src[j]));
@@ -258,7 +261,29 @@ __global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, 
             te += red[1][w];
         }
         qaux[i] = make_float4(s, sqrtf(s), sqrtf(tn), sqrtf(te));
+        if (qexact) qexact[i] = (amax >= 0.0f && all_integral && s + amax < 8388608.0f) ? 1 : 0;
     }
+}
+
+// Exactness certificate of the bf16 image: flag = every arena value is an
+// integer of magnitude at most 256 (exact in bf16); maxxn = the largest row
+// squared norm (bit pattern of a non-negative float).
+__global__ void arena_integral_kernel(const float* __restrict__ codes, int64_t n, const float* __restrict__ xn,
+                                      int64_t rows, int* __restrict__ flag, unsigned int* __restrict__ maxxn) {
+    bool ok = true;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float v = codes[i];
+        ok = ok && v == rintf(v) && fabsf(v) <= 256.0f;
+    }
+    unsigned int mx = 0u;
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < rows;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        mx = max(mx, __float_as_uint(xn[r]));
+    if (!__syncthreads_and(ok ? 1 : 0) && threadIdx.x == 0) atomicAnd(flag, 0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(FULL, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxxn, mx);
 }
 
 // Bound on |bf16 distance - exact FP32 distance| for one (query, row) pair,
@@ -1448,8 +1473,8 @@ template <int KR>
 __device__ void rerank_warp_query(const ArenaLayout& L, const float* __restrict__ codes,
                                   const int64_t* __restrict__ ids, const float* __restrict__ xn,
                                   const float2* __restrict__ xaux, const ErrCoef& ec, const uint64_t* cq, int n, int k,
-                                  int rmax, bool l2, float cN, const float* qs, uint64_t* sl, float* __restrict__ Dq,
-                                  int64_t* __restrict__ Iq, int lane) {
+                                  int rmax, bool l2, float cN, bool exact, const float* qs, uint64_t* sl,
+                                  float* __restrict__ Dq, int64_t* __restrict__ Iq, int lane) {
     uint64_t key[KR], srt[KR];
     float lo[KR];
 #pragma unroll
@@ -1491,24 +1516,30 @@ __device__ void rerank_warp_query(const ArenaLayout& L, const float* __restrict_
 #pragma unroll
         for (int r = 0; r < KR; ++r) sel[r] = sel[r] && static_cast<uint32_t>(key[r] >> 32) <= Sr;
     }
-    int m = 0;
+    if (exact) {
+        // Certified exact tensor-core distances: the selected keys are final.
 #pragma unroll
-    for (int r = 0; r < KR; ++r) {
-        const unsigned b = __ballot_sync(FULL, sel[r]);
-        if (sel[r]) sl[m + __popc(b & ((1u << lane) - 1u))] = key[r] & 0xffffffffu;
-        m += __popc(b);
-    }
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) {
-        const int64_t row = static_cast<int64_t>(sl[i]);
-        const float sc = l2 ? row_l2_global(L, codes, row, qs, true) : -row_ip_global(L, codes, row, qs);
-        sl[i] = (static_cast<uint64_t>(f2o(sc)) << 32) | static_cast<uint32_t>(row);
-    }
-    __syncwarp();
+        for (int r = 0; r < KR; ++r) srt[r] = sel[r] ? key[r] : KEY_MAX;
+    } else {
+        int m = 0;
 #pragma unroll
-    for (int r = 0; r < KR; ++r) {
-        const int e = r * 32 + lane;
-        srt[r] = e < m ? sl[e] : KEY_MAX;
+        for (int r = 0; r < KR; ++r) {
+            const unsigned b = __ballot_sync(FULL, sel[r]);
+            if (sel[r]) sl[m + __popc(b & ((1u << lane) - 1u))] = key[r] & 0xffffffffu;
+            m += __popc(b);
+        }
+        __syncwarp();
+        for (int i = lane; i < m; i += 32) {
+            const int64_t row = static_cast<int64_t>(sl[i]);
+            const float sc = l2 ? row_l2_global(L, codes, row, qs, true) : -row_ip_global(L, codes, row, qs);
+            sl[i] = (static_cast<uint64_t>(f2o(sc)) << 32) | static_cast<uint32_t>(row);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < KR; ++r) {
+            const int e = r * 32 + lane;
+            srt[r] = e < m ? sl[e] : KEY_MAX;
+        }
     }
     warp_sort<KR>(srt, lane);
 #pragma unroll
@@ -1538,8 +1569,8 @@ __global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant_
                                                           const float2* __restrict__ xaux,
                                                           const float4* __restrict__ qaux, const float* __restrict__ q,
                                                           int nq, BatchWork w, int capq, int k, int rmax, int metric,
-                                                          float cK, float cN, float* __restrict__ D,
-                                                          int64_t* __restrict__ I) {
+                                                          float cK, float cN, const int32_t* __restrict__ qexact,
+                                                          float* __restrict__ D, int64_t* __restrict__ I) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint64_t* sl = reinterpret_cast<uint64_t*>(sm) + static_cast<size_t>(warp) * 256;  // [8][256] selected keys
@@ -1567,10 +1598,11 @@ __global__ void __launch_bounds__(256) rerank_warp_kernel(const __grid_constant_
     float* Dq = D + static_cast<size_t>(qi) * k;
     int64_t* Iq = I + static_cast<size_t>(qi) * k;
     const int need = max(n, k);
+    const bool exact = qexact != nullptr && qexact[qi] != 0;
     if (need <= 128)
-        rerank_warp_query<4>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+        rerank_warp_query<4>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, exact, qs, sl, Dq, Iq, lane);
     else
-        rerank_warp_query<8>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, qs, sl, Dq, Iq, lane);
+        rerank_warp_query<8>(L, codes, ids, xn, xaux, ec, cq, n, k, rmax, l2, cN, exact, qs, sl, Dq, Iq, lane);
 }
 
 __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float* __restrict__ codes,
@@ -1578,7 +1610,8 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
                                                      const float2* __restrict__ xaux, const float4* __restrict__ qaux,
                                                      const float* __restrict__ q, BatchWork w, int qbase, int capq,
                                                      int k, int rmax, int metric, float cK, float cN,
-                                                     float* __restrict__ D, int64_t* __restrict__ I) {
+                                                     const int32_t* __restrict__ qexact, float* __restrict__ D,
+                                                     int64_t* __restrict__ I) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t* sel = reinterpret_cast<uint64_t*>(sm);                  // [RERANK_MAX]
     float* qs = reinterpret_cast<float*>(sel + RERANK_MAX);           // [row_pitch]
@@ -1644,7 +1677,8 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
         const int pos = atomicAdd(&w.overflow[0], 1);
         w.overflow[1 + pos] = qbase + qi;
     }
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const bool exact = qexact != nullptr && qexact[qi] != 0;  // certified exact keys need no recompute
+    for (int i = threadIdx.x; i < m && !exact; i += blockDim.x) {
         const int64_t row = static_cast<int64_t>(sel[i] & 0xffffffffu);
         const float sc = l2 ? row_l2_global(L, codes, row, qs, true) : -row_ip_global(L, codes, row, qs);
         sel[i] = (static_cast<uint64_t>(f2o(sc)) << 32) | static_cast<uint32_t>(row);
@@ -1822,13 +1856,21 @@ cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s) {
+cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s,
+                                float amax, int32_t* qexact) {
     if (qscale) {
         prep_queries_f8_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 127) / 128, static_cast<unsigned char*>(qb), qaux,
                                                   qscale);
     } else {
-        prep_queries_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 63) / 64, static_cast<__nv_bfloat16*>(qb), qaux);
+        prep_queries_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 63) / 64, static_cast<__nv_bfloat16*>(qb), qaux, amax,
+                                               qexact);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_arena_integral(const float* codes, int64_t n, const float* xn, int64_t rows, int* flag,
+                                  unsigned int* maxxn, cudaStream_t s) {
+    arena_integral_kernel<<<1184, 256, 0, s>>>(codes, n, xn, rows, flag, maxxn);
     return cudaGetLastError();
 }
 
@@ -1937,7 +1979,7 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
                           int capq, int k, int rmax, int metric, bool f8, int nsm, float* D, int64_t* I,
-                          cudaStream_t s) {
+                          cudaStream_t s, const int32_t* qexact) {
     float cK, cN;
     err_consts(L.d, f8, &cK, &cN);
     cudaError_t e = cudaMemsetAsync(w.big, 0, sizeof(int32_t), s);
@@ -1947,7 +1989,7 @@ cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_
                                   static_cast<int>(wsmem))) != cudaSuccess)
         return e;
     rerank_warp_kernel<<<(nq + 7) / 8, 256, wsmem, s>>>(L, codes, ids, xn, xaux, qaux, q, nq, w, capq, k, rmax, metric,
-                                                        cK, cN, D, I);
+                                                        cK, cN, qexact, D, I);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t smem = static_cast<size_t>(RERANK_MAX) * 8 + static_cast<size_t>(L.row_pitch) * 4 +
                         static_cast<size_t>(capq) * 8;
@@ -1956,7 +1998,7 @@ cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_
                                   static_cast<int>(smem))) != cudaSuccess)
         return e;
     rerank_kernel<<<2 * nsm, 256, smem, s>>>(L, codes, ids, xn, xaux, qaux, q, w, qbase, capq, k, rmax, metric, cK, cN,
-                                             D, I);
+                                             qexact, D, I);
     return cudaGetLastError();
 }
 

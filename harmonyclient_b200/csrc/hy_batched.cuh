@@ -34,7 +34,20 @@ cudaError_t launch_to_f8_arena(const ArenaLayout& L, const float* codes, int64_t
                                const int32_t* list_size, int nlist, float* tile_max, float* lscale, float* tscale,
                                void* out, cudaStream_t s);
 // qscale == nullptr: bf16 queries; else e4m3 queries with per-query scales.
-cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s);
+// bf16 queries with qexact: qexact[i] = 1 when query i and the arena admit
+// exact tensor-core distances: amax >= 0 (the arena's certificate, see
+// launch_arena_integral: every value an integer of magnitude <= 256 and the
+// largest row squared norm amax), the query's values integers of magnitude
+// <= 256 and |q|^2 + amax < 2^23.  Then every product and partial sum of the
+// bf16 distance is an integer below 2^24, exact in f32, and the distance
+// equals the plain scan's bit for bit.
+cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4* qaux, float* qscale, cudaStream_t s,
+                                float amax = -1.0f, int32_t* qexact = nullptr);
+// flag (int, preset to 1) := 0 unless every one of the n values of codes is
+// an integer of magnitude <= 256; maxxn (preset to 0) := bit pattern of the
+// largest of xn[0..rows).
+cudaError_t launch_arena_integral(const float* codes, int64_t n, const float* xn, int64_t rows, int* flag,
+                                  unsigned int* maxxn, cudaStream_t s);
 // Per arena row {|x~|, |x - x~|} for the error bound (tscale == nullptr: the
 // bf16 image, else the e4m3 image with those tile scales), and per 128-row
 // tile the maxima of both.
@@ -131,11 +144,12 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
 // qbase: added to the query ids listed in w.overflow.  rmax > 0: at most the
 // rmax candidates with the smallest tensor-core distance are re-ranked (the
 // e4m3 form's oversampled re-rank); 0 re-ranks every candidate whose bound
-// can reach the top-k.
+// can reach the top-k.  qexact (optional, see launch_prep_queries): queries
+// whose tensor-core distances are exact keep them instead of recomputing.
 cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_t* ids, const float* xn,
                           const float2* xaux, const float4* qaux, const float* q, int nq, const BatchWork& w, int qbase,
                           int capq, int k, int rmax, int metric, bool f8, int nsm, float* D, int64_t* I,
-                          cudaStream_t s);
+                          cudaStream_t s, const int32_t* qexact = nullptr);
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s);
 
 // Device-side exact fallback for queries whose candidates overflowed

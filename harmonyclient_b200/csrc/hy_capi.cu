@@ -182,6 +182,9 @@ struct hy_index {
     DevBuf xaux;              // per arena row {|x~|, |x - x~|}
     DevBuf taux;              // per 128-row tile, maxima of xaux
     bool abf_valid = false;
+    DevBuf b_cert;            // the bf16 image's exactness certificate {integral, max row norm}
+    float arena_maxxn = -1.0f;  // its largest row squared norm when integral (<= 256), else -1
+    DevBuf b_qx;              // per-query exact-distance flags
     DevBuf a8, x8aux, t8aux;  // the same for the e4m3 image
     DevBuf lscale, tscale, tmax;  // e4m3 per-list and per-tile scales, tile maxima
     bool a8_valid = false;
@@ -600,6 +603,19 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
     HY_CUDA(hy::launch_to_bf16_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->abf.p, s));
     HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, nullptr, h->xaux.as<float2>(), h->taux.as<float2>(),
                                s));
+    // Exactness certificate of the image (see launch_prep_queries).
+    HY_RET(h->b_cert.ensure(2 * sizeof(int32_t)));
+    const int32_t init[2] = {1, 0};
+    HY_CUDA(cudaMemcpyAsync(h->b_cert.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    HY_CUDA(hy::launch_arena_integral(h->codes.as<float>(), (int64_t)(rows * h->L.row_pitch), h->norms.as<float>(),
+                                      (int64_t)rows, h->b_cert.as<int>(), reinterpret_cast<unsigned int*>(h->b_cert.as<int>() + 1),
+                                      s));
+    int32_t cert[2] = {0, 0};
+    HY_CUDA(cudaMemcpyAsync(cert, h->b_cert.p, sizeof(cert), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaStreamSynchronize(s));
+    float mx;
+    std::memcpy(&mx, &cert[1], sizeof(float));
+    h->arena_maxxn = cert[0] ? mx : -1.0f;
     h->abf_valid = true;
     return HY_OK;
 }
@@ -714,6 +730,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_qb.ensure(qc * nkb * 128));
     if (f8) HY_RET(h->b_qs.ensure(qc * sizeof(float)));
     HY_RET(h->b_qn.ensure(qc * sizeof(float4)));
+    HY_RET(h->b_qx.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_pcnt.ensure(nlist * sizeof(int32_t)));
     HY_RET(h->b_pfill.ensure(nlist * sizeof(int32_t)));
     HY_RET(h->b_poff.ensure((nlist + 1) * sizeof(int64_t)));
@@ -773,7 +790,8 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         HY_CUDA(cudaMemsetAsync(w.overflow, 0, sizeof(int32_t), s));
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
         HY_CUDA(hy::launch_prep_queries(qq, (int)m, (int)h->d, h->b_qb.p, h->b_qn.as<float4>(),
-                                        f8 ? h->b_qs.as<float>() : nullptr, s));
+                                        f8 ? h->b_qs.as<float>() : nullptr, s, f8 ? -1.0f : h->arena_maxxn,
+                                        f8 ? nullptr : h->b_qx.as<int32_t>()));
         if (coarse_on_tensor(h, nprobe)) {
             HY_RET(coarse_tensor(h, m, qq, nprobe, h->w_probes.as<int64_t>(),
                                  learned_on(h) ? h->m_pscore.as<float>() : nullptr, s));
@@ -857,7 +875,8 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         const int rmax = f8 ? (int)std::min<size_t>(h->oversample * k, 4096) : 0;
         HY_CUDA(hy::launch_rerank(h->L, h->codes.as<float>(), h->ids.as<int64_t>(), h->norms.as<float>(),
                                   f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(), h->b_qn.as<float4>(), qq, (int)m,
-                                  w, 0, (int)capq, (int)k, rmax, h->metric, f8, h->nsm, dD + q0 * k, dI + q0 * k, s));
+                                  w, 0, (int)capq, (int)k, rmax, h->metric, f8, h->nsm, dD + q0 * k, dI + q0 * k, s,
+                                  f8 ? nullptr : h->b_qx.as<int32_t>()));
         if (timed && q0 + qc >= n) HY_CUDA(ev_record(h->ev[4], s));
         const int fb = (int)std::min<size_t>(m, fbcap);
         HY_CUDA(hy::launch_fb_gather(w.overflow, qq, h->w_probes.as<int64_t>(), (int)nprobe, (int)h->d, fb,
