@@ -1269,7 +1269,7 @@ int hy_index_autotune(hy_index* h, size_t n, const float* q, size_t k, int reps,
     // of an item) x candidate slots per query.  Every shape returns the same
     // exact answer; the fastest is kept.
     const size_t slices[3] = {512, 1024, 2048};
-    const size_t capqs[2] = {4096, 8192};
+    const size_t capqs[2] = {8192, 12288};  // the first pass scans lists of up to capq rows densely
     const size_t keep_rs = h->row_slice, keep_capq = h->capq;
     std::vector<int64_t> ref_I;
     std::vector<int64_t> got_I(n * k);
@@ -1373,17 +1373,23 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     HY_RET(h->w_D.ensure(nt * k * sizeof(float)));
     HY_RET(h->w_I.ensure(nt * k * sizeof(int64_t)));
     HY_RET(reset_counters(h, s));
-    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * h->d * sizeof(float), cudaMemcpyHostToDevice, s));
+    const size_t d = h->d;
+    HY_CUDA(cudaMemcpyAsync(h->w_q.p, q, n * d * sizeof(float), cudaMemcpyHostToDevice, s));
     if (m) {
         HY_RET(h->w_jrows.ensure(m * sizeof(int64_t)));
         HY_CUDA(cudaMemcpyAsync(h->w_jrows.p, judge_rows->data(), m * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-        HY_CUDA(hy::launch_gather_rows(h->w_q.as<float>(), h->w_jrows.as<int64_t>(), (int64_t)m, (int)h->d,
-                                       h->w_q.as<float>() + n * h->d, s));
+        HY_CUDA(hy::launch_gather_rows(h->w_q.as<float>(), h->w_jrows.as<int64_t>(), (int64_t)m, (int)d,
+                                       h->w_q.as<float>() + n * d, s));
     }
     h->learned_rows = n;
     const int rc = search_device_impl(h, nt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true);
     h->learned_rows = SIZE_MAX;
     HY_RET(rc);
+    // The results go back before the status checks (one synchronisation for
+    // both); a batch searched again below is copied again.
+    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (m) HY_CUDA(cudaMemcpyAsync(jI, h->w_I.as<int64_t>() + n * k, m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     HY_RET(finish_host_call(h, s, true, nt, std::min(h->nprobe, h->nlist)));
     h->stats.nq = n;
     h->stats.fallback_queries = 0;
@@ -1399,11 +1405,16 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
         const uint64_t fb = h->stats.fallback_queries;
         h->stats = keep;
         h->stats.fallback_queries = fb;
+        if (fb == nt) {
+            // The whole batch was searched again in the plain form.
+            HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
+            HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            if (m)
+                HY_CUDA(cudaMemcpyAsync(jI, h->w_I.as<int64_t>() + n * k, m * k * sizeof(int64_t),
+                                        cudaMemcpyDeviceToHost, s));
+            HY_CUDA(cudaStreamSynchronize(s));
+        }
     }
-    HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
-    HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    if (m) HY_CUDA(cudaMemcpyAsync(jI, h->w_I.as<int64_t>() + n * k, m * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    HY_CUDA(cudaStreamSynchronize(s));
     return HY_OK;
 }
 

@@ -183,7 +183,7 @@ HY_API int hy_index_search_device(hy_index* h, size_t n, const float* dq, size_t
 /* Autotuner of the bf16 form (no counterpart in the reference): times the
  * search of n sample queries (host pointer) at k for every candidate work
  * shape (rows per work item 512 / 1024 / 2048 x candidate slots per query
- * 4096 / 8192; reps timed searches each, after one untimed) and keeps the
+ * 8192 / 12288; reps timed searches each, after one untimed) and keeps the
  * fastest whose results equal the first shape's.  report (may be NULL)
  * receives 6 x {row_slice, capq, ms} (ms negated for a shape whose results
  * differed). */
