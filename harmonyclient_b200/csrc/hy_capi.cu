@@ -160,9 +160,11 @@ struct hy_index {
         size_t n, k, nprobe;
         const void *dq, *dD, *dI, *np;
         cudaStream_t s;
+        size_t learned_rows;
+        int learned;
         bool operator==(const GraphKey& o) const {
             return epoch == o.epoch && n == o.n && k == o.k && nprobe == o.nprobe && dq == o.dq && dD == o.dD &&
-                   dI == o.dI && np == o.np && s == o.s;
+                   dI == o.dI && np == o.np && s == o.s && learned_rows == o.learned_rows && learned == o.learned;
         }
     } gkey{};
     uint64_t graph_kernels = 0;
@@ -965,7 +967,7 @@ int run_device_search(hy_index* h, size_t n, const float* dq, size_t k, float* d
     h->stats.graph_replayed = 0;
     h->ev = h->ev_direct;
     if (!h->graph_on) return search_device_impl(h, n, dq, k, dD, dI, s, true);
-    const hy_index::GraphKey key{h->epoch, n, k, h->nprobe, dq, dD, dI, h->q_nprobe, s};
+    const hy_index::GraphKey key{h->epoch, n, k, h->nprobe, dq, dD, dI, h->q_nprobe, s, h->learned_rows, h->learned};
     cudaStream_t run = s ? s : h->stream;
     if (h->gexec && key == h->gkey) {
         if (!s) {
@@ -1382,7 +1384,12 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
                                        h->w_q.as<float>() + n * d, s));
     }
     h->learned_rows = n;
-    const int rc = search_device_impl(h, nt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, true);
+    // Graph mode replays the captured search (the workspace pointers and
+    // the stream are the handle's own, so repeated calls of one shape match).
+    const int rc = h->graph_on
+                       ? run_device_search(h, nt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s)
+                       : search_device_impl(h, nt, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s,
+                                            true);
     h->learned_rows = SIZE_MAX;
     HY_RET(rc);
     // The results go back before the status checks (one synchronisation for

@@ -105,3 +105,34 @@ def test_autotune_needs_bf16_form(index):
     idx, x, q = index
     with pytest.raises(hb.HyError):
         idx.autotune(q[:10], 10)
+
+
+def test_host_search_replays_the_graph(index):
+    """The host-pointer search in graph mode: upload, replayed search,
+    download; every answer equals the plain search's."""
+    idx, x, q = index
+    D0, I0 = idx.search(q, 30)
+    idx.set_form("bf16")
+    idx.set_graph(True)
+    try:
+        replayed = []
+        for _ in range(3):
+            D, I = idx.search(q, 30)
+            replayed.append(idx.last_stats()["graph_replayed"])
+            np.testing.assert_array_equal(I, I0)
+            np.testing.assert_array_equal(D, D0)
+        assert replayed == [0, 1, 1]
+        idx.nprobe = 8
+        D8, I8 = idx.search(q, 30)
+        assert idx.last_stats()["graph_replayed"] == 0
+    finally:
+        idx.nprobe = 16
+        idx.set_graph(False)
+        idx.set_form("plain")
+    idx.nprobe = 8
+    try:
+        Dp8, Ip8 = idx.search(q, 30)
+    finally:
+        idx.nprobe = 16
+    np.testing.assert_array_equal(I8, Ip8)
+    np.testing.assert_array_equal(D8, Dp8)

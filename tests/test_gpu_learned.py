@@ -203,3 +203,36 @@ def test_model_round_trip_and_errors(trained):
     np.testing.assert_array_equal(Da, Db)
     with pytest.raises(hb.HyError):
         idx.set_learned(True, judge_fraction=2.0)
+
+
+def test_graph_mode_learned_and_judge_fallback(trained):
+    """Graph mode with the learned form: replays keep the learned answer, and
+    the judge's fallback search (learned off, same batch shape) is not served
+    by the learned graph."""
+    idx, x, q, _ = trained
+    qt = q[10_000:10_500]
+    D0, I0 = idx.search(qt, 10)
+    idx.set_learned(True, judge_fraction=0.0)
+    Dl, Il = idx.search(qt, 10)
+    keep = idx.get_probe_model()
+    weak = keep.copy()
+    weak[:mlp.NPARAM] = 0.0
+    weak[mlp.B3] = -10.0
+    weak[-2] = 0.0
+    idx.set_graph(True)
+    try:
+        for _ in range(2):
+            D, I = idx.search(qt, 10)
+            np.testing.assert_array_equal(I, Il)
+            np.testing.assert_array_equal(D, Dl)
+        idx.set_probe_model(weak)
+        idx.set_learned(True, judge_fraction=1.0, judge_recall=1.0)
+        for _ in range(2):
+            D, I = idx.search(qt, 10)
+            assert idx.last_stats()["learned_fallback"] == 1
+            np.testing.assert_array_equal(I, I0)
+            np.testing.assert_array_equal(D, D0)
+    finally:
+        idx.set_graph(False)
+        idx.set_learned(False)
+        idx.set_probe_model(keep)
