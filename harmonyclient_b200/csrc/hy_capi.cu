@@ -113,6 +113,14 @@ ArenaLayout make_layout(int d, int nb) {
 
 }  // namespace
 
+// Device status of a host-pointer call, read back in one pinned block.
+struct HostStatus {
+    int err = 0;
+    unsigned long long counters[2] = {0, 0};  // scan tile-block counters
+    unsigned long long learned_total = 0;     // sum of the learned nprobes
+    unsigned long long fallback[2] = {0, 0};  // device fallback: answered, unresolved
+};
+
 struct hy_index {
     std::mutex mu;
     int device = 0;
@@ -171,6 +179,9 @@ struct hy_index {
     int graph_kev = 0;
     cudaEvent_t gev[2] = {};
     bool times_pending = false;  // a device-API search recorded events not yet read
+    HostStatus* hstat = nullptr;  // pinned status block of host-pointer calls (finish_host_call)
+    int64_t* hjudge = nullptr;    // pinned results of the learned judge's rows
+    size_t hjudge_cap = 0;
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
 
@@ -920,20 +931,28 @@ void collect_times(hy_index* h) {
     h->times_pending = false;
 }
 
+// End of a host-pointer call: the device status (error flag, scan
+// counters, learned nprobe total, fallback counters) comes back in one
+// pinned block with the stream's single synchronisation.
 int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t nprobe) {
+    if (!h->hstat) HY_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h->hstat), sizeof(HostStatus), cudaHostAllocDefault));
+    HostStatus* st = h->hstat;
+    *st = HostStatus{};
+    HY_CUDA(cudaMemcpyAsync(&st->err, h->w_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HY_CUDA(cudaMemcpyAsync(st->counters, h->w_counters.p, sizeof(st->counters), cudaMemcpyDeviceToHost, s));
+    if (h->m_total.p)
+        HY_CUDA(cudaMemcpyAsync(&st->learned_total, h->m_total.p, sizeof(st->learned_total), cudaMemcpyDeviceToHost, s));
+    if (h->b_fbtot.p) HY_CUDA(cudaMemcpyAsync(st->fallback, h->b_fbtot.p, sizeof(st->fallback), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
-    int err = 0;
-    HY_CUDA(cudaMemcpy(&err, h->w_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err != 0) {
+    if (st->err != 0) {
+        const int err = st->err;
         cudaMemset(h->w_err.p, 0, sizeof(int));
         return fail(err == HY_ERR_TIMEOUT ? HY_ERR_TIMEOUT : HY_ERR_CUDA, "device reported an error in the scan kernel");
     }
-    unsigned long long c[2] = {0, 0};
-    HY_CUDA(cudaMemcpy(c, h->w_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
     h->stats.nq = n;
     h->stats.pairs = n * nprobe;
-    h->stats.tile_blocks = c[0];
-    h->stats.tile_blocks_max = c[1];
+    h->stats.tile_blocks = st->counters[0];
+    h->stats.tile_blocks_max = st->counters[1];
     h->stats.launches = h->launches;
     h->launches = 0;
     if (timed) collect_times(h);
@@ -1022,9 +1041,9 @@ int run_device_search(hy_index* h, size_t n, const float* dq, size_t k, float* d
 // answered again on the device by the plain scan (up to FB_CAP per chunk);
 // if more overflowed in some chunk, the whole batch is searched again here
 // with the plain form (its queries are still in h->w_q).
+// After finish_host_call (its status block holds the fallback counters).
 int bf16_fallback(hy_index* h, size_t n, size_t k, cudaStream_t s) {
-    unsigned long long c[2] = {0, 0};
-    HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
+    const unsigned long long c[2] = {h->hstat->fallback[0], h->hstat->fallback[1]};
     h->stats.fallback_queries = c[0];
     h->stats.unresolved_queries = 0;
     if (c[1] == 0) return HY_OK;
@@ -1108,6 +1127,8 @@ int hy_index_destroy(hy_index* h) {
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : h->gev)
         if (ev) cudaEventDestroy(ev);
+    if (h->hstat) cudaFreeHost(h->hstat);
+    if (h->hjudge) cudaFreeHost(h->hjudge);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HY_OK;
@@ -1401,11 +1422,7 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     h->stats.nq = n;
     h->stats.fallback_queries = 0;
     h->stats.mean_nprobe = (double)std::min(h->nprobe, h->nlist);
-    if (learned_on(h)) {
-        unsigned long long tot = 0;
-        HY_CUDA(cudaMemcpy(&tot, h->m_total.p, sizeof(tot), cudaMemcpyDeviceToHost));
-        h->stats.mean_nprobe = (double)tot / (double)n;
-    }
+    if (learned_on(h)) h->stats.mean_nprobe = (double)h->hstat->learned_total / (double)n;
     if (batched_form(h) && h->arena_rows > 0) {
         const hy_search_stats_t keep = h->stats;
         HY_RET(bf16_fallback(h, nt, k, s));
@@ -1434,8 +1451,17 @@ int search_learned_judged(hy_index* h, size_t n, const float* q, size_t k, float
     std::vector<int64_t> rows;
     for (size_t i = 0; i < n; i += step) rows.push_back((int64_t)i);
     const size_t m = rows.size();
-    std::vector<int64_t> sI(m * k);
-    HY_RET(search_host(h, n, q, k, D, I, &rows, sI.data()));
+    // The judged rows' results land in pinned memory (a pageable target
+    // would make their copy a separate staged transfer).
+    if (h->hjudge_cap < m * k) {
+        if (h->hjudge) cudaFreeHost(h->hjudge);
+        h->hjudge = nullptr;
+        h->hjudge_cap = 0;
+        HY_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h->hjudge), m * k * sizeof(int64_t), cudaHostAllocDefault));
+        h->hjudge_cap = m * k;
+    }
+    const int64_t* sI = h->hjudge;
+    HY_RET(search_host(h, n, q, k, D, I, &rows, h->hjudge));
     const size_t kk = std::min<size_t>(10, k);
     size_t hit = 0, tot = 0;
     for (size_t i = 0; i < m; ++i) {
