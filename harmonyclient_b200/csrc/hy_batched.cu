@@ -365,6 +365,61 @@ __global__ void probe_fill_kernel(const int64_t* __restrict__ probes, int nq, in
     }
 }
 
+// The same two steps with shared-memory counters (nlist <= INVERT_SMEM_LISTS):
+// each CTA takes a contiguous range of `per` pairs, counts them per list in
+// shared memory and adds each list's count to the global one once; the fill
+// reserves each list's share of the CTA with one global add and places the
+// pairs at shared-memory ranks.  Few global atomics per list instead of one
+// per pair.
+constexpr int INVERT_SMEM_LISTS = 6144;  // the fill's 8 bytes per list stay within 48 KiB
+__global__ void __launch_bounds__(512) probe_hist_smem_kernel(const int64_t* __restrict__ probes, int nq, int nprobe,
+                                                              int j0, int j1, int nlist, int64_t per,
+                                                              int32_t* __restrict__ cnt) {
+    extern __shared__ int h[];  // [nlist]
+    const int w = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * w;
+    const int64_t a = blockIdx.x * per, b = min(n, a + per);
+    for (int l = threadIdx.x; l < nlist; l += blockDim.x) h[l] = 0;
+    __syncthreads();
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+        const int64_t l = probes[(i / w) * nprobe + j0 + i % w];
+        if (l >= 0) atomicAdd(&h[l], 1);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < nlist; l += blockDim.x)
+        if (h[l]) atomicAdd(&cnt[l], h[l]);
+}
+
+__global__ void __launch_bounds__(512) probe_fill_smem_kernel(const int64_t* __restrict__ probes, int nq, int nprobe,
+                                                              int j0, int j1, int nlist, int64_t per,
+                                                              const int64_t* __restrict__ off,
+                                                              int32_t* __restrict__ fill,
+                                                              int32_t* __restrict__ pairs) {
+    extern __shared__ int h[];  // [nlist] counts, then ranks; [nlist] bases
+    int* base = h + nlist;
+    const int w = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * w;
+    const int64_t a = blockIdx.x * per, b = min(n, a + per);
+    for (int l = threadIdx.x; l < nlist; l += blockDim.x) h[l] = 0;
+    __syncthreads();
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+        const int64_t l = probes[(i / w) * nprobe + j0 + i % w];
+        if (l >= 0) atomicAdd(&h[l], 1);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < nlist; l += blockDim.x) {
+        base[l] = h[l] ? atomicAdd(&fill[l], h[l]) : 0;
+        h[l] = 0;
+    }
+    __syncthreads();
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+        const int64_t l = probes[(i / w) * nprobe + j0 + i % w];
+        if (l < 0) continue;
+        const int pos = base[l] + atomicAdd(&h[l], 1);
+        pairs[off[l] + pos] = static_cast<int32_t>(i / w);
+    }
+}
+
 // Items of a list = query groups x row slices (none for an empty list).
 __global__ void item_count_kernel(const int32_t* __restrict__ cnt, const int32_t* __restrict__ list_size, int nlist,
                                   int rs, int qg, int32_t* __restrict__ items) {
@@ -772,6 +827,11 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 // Per-tile test bound of this warp's queries:
                 // V + max|x~| aq + max|x - x~| bq over the tile's rows.
                 const float2 ta = S.taux[t];
+                // A dense item's per-row bound terms, fetched before the wait
+                // for the accumulator so the load overlaps the MMA.
+                const int pre_row = t * TM + quad * 32 + lane;
+                const float2 xa_pre =
+                    (S.dense && pre_row < nrows) ? p.xaux[row0 + pre_row] : make_float2(0.0f, 0.0f);
                 __syncwarp();
                 for (int cc = lane; cc < CW; cc += 32) {
                     const int q = half * CW + cc;
@@ -820,7 +880,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     // The bound is the tightening step's own expression.
                     const int pos = S.lrow0 + rs_row;
                     if (rvalid && pos < p.capq) {
-                        const float2 xa = p.xaux[arow];
+                        const float2 xa = xa_pre;
                         const float rc = err_row_const(xnv, l2, p.cN);
                         float2* cf2 = reinterpret_cast<float2*>(p.cand);
 #pragma unroll
@@ -1902,10 +1962,21 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.pair_cnt, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.pair_fill, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
-    probe_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_cnt);
-    scan_kernel<<<1, 1024, 0, s>>>(w.pair_cnt, nlist, w.pair_off);
-    probe_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_off, w.pair_fill,
-                                                       w.pairs);
+    if (nlist <= INVERT_SMEM_LISTS) {
+        // About 160 CTAs of 512 threads (at least 512 pairs each).
+        const int64_t per = std::max<int64_t>(512, (n + 159) / 160);
+        const int nblk = static_cast<int>(std::max<int64_t>(1, (n + per - 1) / per));
+        probe_hist_smem_kernel<<<nblk, 512, static_cast<size_t>(nlist) * 4, s>>>(probes, nq, nprobe, j0, j1, nlist,
+                                                                                 per, w.pair_cnt);
+        scan_kernel<<<1, 1024, 0, s>>>(w.pair_cnt, nlist, w.pair_off);
+        probe_fill_smem_kernel<<<nblk, 512, static_cast<size_t>(nlist) * 8, s>>>(probes, nq, nprobe, j0, j1, nlist,
+                                                                                 per, w.pair_off, w.pair_fill, w.pairs);
+    } else {
+        probe_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_cnt);
+        scan_kernel<<<1, 1024, 0, s>>>(w.pair_cnt, nlist, w.pair_off);
+        probe_fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(probes, nq, nprobe, j0, j1, w.pair_off, w.pair_fill,
+                                                           w.pairs);
+    }
     item_count_kernel<<<grid_for(nlist, 256), 256, 0, s>>>(w.pair_cnt, list_size, nlist, rs, qg, w.item_cnt);
     scan_kernel<<<1, 1024, 0, s>>>(w.item_cnt, nlist, w.item_off);
     item_fill_kernel<<<grid_for(static_cast<int64_t>(nlist) * 32, 256), 256, 0, s>>>(w.item_off, list_size, nlist, rs,
