@@ -919,7 +919,14 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                             m[j] = m[j + 1] = m[j + 2] = m[j + 3] = cf;
                         }
                     }
-                    // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef)
+                    // candidate test: cf*ip + (|x|^2 - cx) <= R_q (see err_coef).
+                    // First only whether any row of the warp has one in the
+                    // chunk (two instructions per element); the per-column
+                    // mask is built for such chunks alone.
+                    bool hit = false;
+#pragma unroll
+                    for (int j = 0; j < CC; ++j) hit |= fmaf(m[j], __uint_as_float(u[c * CC + j]), ax) <= r[j];
+                    if (!__any_sync(FULL, hit)) continue;
                     uint32_t mask = 0;
 #pragma unroll
                     for (int j = 0; j < CC; ++j)
