@@ -1112,15 +1112,17 @@ __device__ inline void tighten_warp_query(int qi, int cnt, const float* __restri
     }
 }
 
-// An upper bound U on the k-th smallest score + bound of cnt >= k dense
-// {score, bound} entries, with at least k entries at or below it: two 8-bit
-// radix passes below the bits all the entries' ordered values share; U is
-// the upper edge of the final bin that holds the k-th value.  One warp.
-__device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, int k, int* hist, int lane) {
+// An upper bound U on the k-th smallest score + bound of cnt >= k
+// {score, bound} entries (get(e) gives entry e), with at least k entries at
+// or below it: two 8-bit radix passes below the bits all the entries'
+// ordered values share; U is the upper edge of the final bin that holds the
+// k-th value.  One warp; the entries are read on every pass.
+template <typename Get>
+__device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int lane) {
     uint32_t mn = 0xffffffffu, mx = 0u;
 #pragma unroll 4
     for (int e = lane; e < cnt; e += 32) {
-        const float2 v = ce[e];
+        const float2 v = get(e);
         const uint32_t h = f2o(v.x + v.y);
         mn = min(mn, h);
         mx = max(mx, h);
@@ -1143,7 +1145,7 @@ __device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, 
             __syncwarp();
 #pragma unroll 4
             for (int e = lane; e < cnt; e += 32) {
-                const float2 v = ce[e];
+                const float2 v = get(e);
                 const uint32_t h = f2o(v.x + v.y);
                 if ((h & mask) == prefix) atomicAdd(&hist[(h & wmask) >> shift], 1);
             }
@@ -1187,6 +1189,10 @@ __device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, 
         ub = top >= 0 ? (prefix | ((2u << top) - 1u)) : prefix;
     }
     return o2f(ub);
+}
+
+__device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, int k, int* hist, int lane) {
+    return kth_bound_stream([ce](int e) { return ce[e]; }, cnt, k, hist, lane);
 }
 
 // Warp tighten of a query whose first-pass list was scanned densely: its
@@ -1365,60 +1371,23 @@ __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4
 // select_warp_kernel writes them.  The candidate keys overwrite the query's
 // pairs in cand.  Shared memory per warp: 256 histogram bins, the query and
 // a 32-row staging block of centroids.
-template <int METRIC, int PER>
-__global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
-                                                            const float* __restrict__ q,
-                                                            const float* __restrict__ cent, int d, int m,
-                                                            int64_t* __restrict__ out_idx,
-                                                            float* __restrict__ out_score) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pitch = refine_pitch(d);
-    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
-    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
-    int* hist = reinterpret_cast<int*>(base);
-    float* qs = reinterpret_cast<float*>(hist + 256);
-    float* stage = qs + pitch;
-    const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (qi >= nq) return;  // whole warp
-    const float* qrow = q + static_cast<size_t>(qi) * d;
-    for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
-    // Every centroid's upper bound (ordered bits) and lower bound in
-    // registers: entry r * 32 + lane.  The query's pairs are then free and
-    // their space holds its candidate keys.
-    float2* ce = cand + static_cast<int64_t>(qi) * nlist;
-    uint64_t* keys = reinterpret_cast<uint64_t*>(ce);
-    uint32_t hi[PER];
-    float lo[PER];
-#pragma unroll
-    for (int r = 0; r < PER; ++r) {
-        const int e = r * 32 + lane;
-        hi[r] = 0xffffffffu;
-        lo[r] = INFINITY;
-        if (e < nlist) {
-            const float2 v = ce[e];
-            hi[r] = f2o(v.x + v.y);
-            lo[r] = v.x - v.y;
-        }
+// The exact m best of a query's c candidate centroids (ids in keys[0, c),
+// overwritten): exact FP32 coarse scores with coarse_scores_kernel's
+// arithmetic, 32 at a time (rows staged in shared memory by asynchronous
+// copies, all in flight at once; lane i sums row i in dimension order; with d
+// a multiple of 4 the copies and reads are 16 bytes wide, row pitch d + 4, so
+// a 512-byte warp read takes the minimum four wavefronts), then ordered by
+// (score, centroid) and written as select_warp_kernel writes them.
+template <int METRIC>
+__device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs, float* stage, int pitch,
+                                         const float* __restrict__ cent, int d, int m, int qi,
+                                         int64_t* __restrict__ out_idx, float* __restrict__ out_score, int lane) {
+    // Fewer candidates than m (not reached when the bound holds m of them):
+    // the missing probes are -1.
+    for (int e = c + lane; e < m; e += 32) {
+        out_idx[static_cast<int64_t>(qi) * m + e] = -1;
+        if (out_score) out_score[static_cast<int64_t>(qi) * m + e] = FLT_MAX;
     }
-    const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
-    __syncwarp();  // every pair has been read before the first key is written
-    // Centroids that can be among the m best.
-    int c = 0;
-#pragma unroll
-    for (int r = 0; r < PER; ++r) {
-        const int e = r * 32 + lane;
-        const bool keep = e < nlist && lo[r] <= U;
-        const unsigned bal = __ballot_sync(FULL, keep);
-        if (keep) keys[c + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint64_t>(e);
-        c += __popc(bal);
-    }
-    __syncwarp();
-    // Their exact scores, 32 at a time: the rows are staged in shared memory
-    // by asynchronous copies (all in flight at once), then lane i sums row i
-    // in dimension order.  With d a multiple of 4 the copies and the reads
-    // are 16 bytes wide (row pitch d + 4: a 512-byte read by the warp takes
-    // the minimum four shared-memory wavefronts).
     const bool v4 = (d & 3) == 0;
     for (int c0 = 0; c0 < c; c0 += 32) {
         const int nr = min(32, c - c0);
@@ -1512,11 +1481,151 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const int e = r * 32 + lane;
-        if (e < m) {
+        if (e < m && e < c) {
             out_idx[static_cast<int64_t>(qi) * m + e] = static_cast<int64_t>(t[r] & 0xffffffffu);
             if (out_score) out_score[static_cast<int64_t>(qi) * m + e] = o2f(static_cast<uint32_t>(t[r] >> 32));
         }
     }
+}
+
+template <int METRIC, int PER>
+__global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
+                                                            const float* __restrict__ q,
+                                                            const float* __restrict__ cent, int d, int m,
+                                                            int64_t* __restrict__ out_idx,
+                                                            float* __restrict__ out_score) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pitch = refine_pitch(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
+    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
+    int* hist = reinterpret_cast<int*>(base);
+    float* qs = reinterpret_cast<float*>(hist + 256);
+    float* stage = qs + pitch;
+    const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (qi >= nq) return;  // whole warp
+    const float* qrow = q + static_cast<size_t>(qi) * d;
+    for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
+    // Every centroid's upper bound (ordered bits) and lower bound in
+    // registers: entry r * 32 + lane.  The query's pairs are then free and
+    // their space holds its candidate keys.
+    float2* ce = cand + static_cast<int64_t>(qi) * nlist;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(ce);
+    uint32_t hi[PER];
+    float lo[PER];
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        hi[r] = 0xffffffffu;
+        lo[r] = INFINITY;
+        if (e < nlist) {
+            const float2 v = ce[e];
+            hi[r] = f2o(v.x + v.y);
+            lo[r] = v.x - v.y;
+        }
+    }
+    const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
+    __syncwarp();  // every pair has been read before the first key is written
+    // Centroids that can be among the m best.
+    int c = 0;
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+        const int e = r * 32 + lane;
+        const bool keep = e < nlist && lo[r] <= U;
+        const unsigned bal = __ballot_sync(FULL, keep);
+        if (keep) keys[c + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint64_t>(e);
+        c += __popc(bal);
+    }
+    __syncwarp();
+    coarse_exact_best<METRIC>(keys, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
+}
+
+// The coarse step for more than 2048 lists, in two tensor-core launches.
+// First a dense launch over the first S centroids; coarse_thr_kernel takes
+// each query's bound on the m-th smallest score + bound among them, which
+// bounds its m-th best exact coarse score over all centroids from above.
+// Then a thresholded launch over all centroids emits the (score, centroid)
+// keys whose lower bound reaches it, and coarse_refine_keys_kernel selects
+// and re-scores them exactly.
+__global__ void __launch_bounds__(256) coarse_thr_kernel(const float2* __restrict__ cand, int nq, int S, int m,
+                                                         float* __restrict__ thr) {
+    __shared__ int hist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;  // whole warp
+    const float2* ce = cand + static_cast<int64_t>(qi) * S;
+    uint32_t hv[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        const int e = r * 32 + lane;
+        hv[r] = 0xffffffffu;
+        if (e < S) {
+            const float2 v = ce[e];
+            hv[r] = f2o(v.x + v.y);
+        }
+    }
+    const float U = o2f(warp_select_bound<32>(hv, S, m, hist[warp], lane));
+    if (lane == 0) thr[qi] = U;
+}
+
+// Per query (one warp): its n keys (score, centroid) at cand + qi * stride;
+// every key's bound from the centroid's {|c~|, |c - c~|} and squared norm and
+// the query's coefficients; U = an upper bound on the m-th smallest
+// score + bound; the centroids with score - bound <= U go to
+// coarse_exact_best.
+template <int METRIC>
+__global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __restrict__ cand,
+                                                                 const int32_t* __restrict__ ccnt, int nq, int stride,
+                                                                 const float* __restrict__ q,
+                                                                 const float* __restrict__ cent,
+                                                                 const float* __restrict__ cxn,
+                                                                 const float2* __restrict__ caux,
+                                                                 const float4* __restrict__ qaux, int d, int m,
+                                                                 float cK, float cN, int64_t* __restrict__ out_idx,
+                                                                 float* __restrict__ out_score) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pitch = refine_pitch(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
+    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
+    int* hist = reinterpret_cast<int*>(base);
+    float* qs = reinterpret_cast<float*>(hist + 256);
+    float* stage = qs + pitch;
+    const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (qi >= nq) return;  // whole warp
+    const float* qrow = q + static_cast<size_t>(qi) * d;
+    for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
+    const bool l2 = METRIC == METRIC_L2;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    uint64_t* keys = cand + static_cast<int64_t>(qi) * stride;
+    const int n = min(ccnt[qi], stride);
+    auto get = [&](int e) {
+        const uint64_t kk = keys[e];
+        const uint32_t row = static_cast<uint32_t>(kk & 0xffffffffu);
+        const float2 xa = caux[row];
+        const float eb = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(cxn[row], l2, cN) + ec.cq));
+        return make_float2(o2f(static_cast<uint32_t>(kk >> 32)), eb);
+    };
+    const float U = n >= m ? kth_bound_stream(get, n, m, hist, lane) : INFINITY;
+    // In place: the kept centroids' ids to the front (every element of a
+    // round is read before any of that round's writes).
+    int c = 0;
+    for (int b0 = 0; b0 < n; b0 += 32) {
+        const int e = b0 + lane;
+        bool keep = false;
+        uint64_t id = 0;
+        if (e < n) {
+            const float2 v = get(e);
+            keep = v.x - v.y <= U;
+            id = keys[e] & 0xffffffffu;
+        }
+        const unsigned bal = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep) keys[c + __popc(bal & ((1u << lane) - 1u))] = id;
+        c += __popc(bal);
+    }
+    __syncwarp();
+    coarse_exact_best<METRIC>(keys, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -1916,6 +2025,32 @@ cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q
     if (metric == METRIC_L2)
         return nlist <= 1024 ? run(coarse_refine_kernel<METRIC_L2, 32>) : run(coarse_refine_kernel<METRIC_L2, 64>);
     return nlist <= 1024 ? run(coarse_refine_kernel<METRIC_IP, 32>) : run(coarse_refine_kernel<METRIC_IP, 64>);
+}
+
+cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, float* thr, cudaStream_t s) {
+    if (S > 1024 || m > S) return cudaErrorInvalidValue;
+    coarse_thr_kernel<<<(nq + 7) / 8, 256, 0, s>>>(cand, nq, S, m, thr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int nq, int stride, const float* q,
+                                      const float* cent, const float* cxn, const float2* caux, const float4* qaux,
+                                      int d, int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s) {
+    int warps = 4;
+    while (warps > 1 && coarse_refine_smem(0, d, warps) > 200 * 1024) warps >>= 1;
+    const size_t smem = coarse_refine_smem(0, d, warps);
+    if (smem > 200 * 1024 || m > 256) return cudaErrorInvalidValue;
+    float cK, cN;
+    err_consts(d, false, &cK, &cN);
+    const dim3 grid((nq + warps - 1) / warps);
+    auto run = [&](auto kern) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        kern<<<grid, 32 * warps, smem, s>>>(cand, ccnt, nq, stride, q, cent, cxn, caux, qaux, d, m, cK, cN, out_idx,
+                                            out_score);
+        return cudaGetLastError();
+    };
+    return metric == METRIC_L2 ? run(coarse_refine_keys_kernel<METRIC_L2>) : run(coarse_refine_keys_kernel<METRIC_IP>);
 }
 
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s) {

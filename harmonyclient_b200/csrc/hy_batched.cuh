@@ -111,6 +111,17 @@ size_t coarse_refine_smem(int nlist, int d, int warps);
 cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent, int d,
                                  int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
 
+// More than 2048 centroids: thr[q] := a bound on the m-th smallest
+// score + bound among the S <= 1024 dense pairs of query q (cand, nq x S),
+// then, from the keys a thresholded launch over all centroids emitted
+// (cand + q * stride, ccnt[q] of them), the exact m best as
+// launch_coarse_refine gives them (cand is overwritten).  cxn / caux: the
+// centroid index's squared norms and {|c~|, |c - c~|}.
+cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, float* thr, cudaStream_t s);
+cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int nq, int stride, const float* q,
+                                      const float* cent, const float* cxn, const float2* caux, const float4* qaux,
+                                      int d, int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
+
 // Largest list the batched search's first pass scans densely (the candidate
 // buffer's size caps it further).
 constexpr size_t DENSE_MAX = 16384;

@@ -636,8 +636,8 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
 // Whether the bf16 form's coarse step runs on the tensor cores (the
 // conditions launch_coarse_refine's shared memory and select width need).
 bool coarse_on_tensor(const hy_index* h, size_t nprobe) {
-    return h->coarse_mode == HY_COARSE_TENSOR && h->form == HY_FORM_BF16 && h->nlist <= 2048 && nprobe <= 256 &&
-           h->d <= 256 && hy::batched_group_size((int)h->d, false) > 0;
+    return h->coarse_mode == HY_COARSE_TENSOR && h->form == HY_FORM_BF16 && nprobe <= 256 && h->d <= 256 &&
+           hy::batched_group_size((int)h->d, false) > 0;
 }
 
 int ensure_centroid_image(hy_index* h, cudaStream_t s) {
@@ -664,23 +664,28 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     const int nlist = (int)h->nlist;
     const int qg = hy::batched_group_size((int)h->d, false);
     const int ngroups = (int)((m + qg - 1) / qg);
-    // Enough row slices to give every SM an item, each at most 2048 rows.
-    const int tiles = (nlist + 127) / 128;
-    int nslices = std::min(tiles, std::max(1, (h->nsm + ngroups - 1) / ngroups));
-    nslices = std::max(nslices, (tiles + 15) / 16);
-    const int rs = (tiles + nslices - 1) / nslices * 128;
-    nslices = (nlist + rs - 1) / rs;
+    // Row slices of a launch over the first `rows` centroids: enough to give
+    // every SM an item, each at most 2048 rows.
+    auto slicing = [&](int rows, int* rs_out) {
+        const int tiles = (rows + 127) / 128;
+        int ns = std::min(tiles, std::max(1, (h->nsm + ngroups - 1) / ngroups));
+        ns = std::max(ns, (tiles + 15) / 16);
+        const int rs = (tiles + ns - 1) / ns * 128;
+        *rs_out = rs;
+        return (rows + rs - 1) / rs;
+    };
+    int rs_full;
+    const int ns_full = slicing(nlist, &rs_full);
     HY_RET(h->c_pcnt.ensure(sizeof(int32_t)));
     HY_RET(h->c_poff.ensure(2 * sizeof(int64_t)));
     HY_RET(h->c_pairs.ensure(m * sizeof(int32_t)));
     HY_RET(h->c_ioff.ensure(2 * sizeof(int64_t)));
-    HY_RET(h->c_items.ensure((size_t)ngroups * nslices * sizeof(int4)));
+    HY_RET(h->c_items.ensure((size_t)ngroups * ns_full * sizeof(int4)));
     HY_RET(h->c_work.ensure(sizeof(unsigned int)));
     HY_RET(h->c_cand.ensure(m * nlist * sizeof(float2)));
     HY_RET(h->c_ccnt.ensure(m * sizeof(int32_t)));
     hy::BatchWork w{};
     w.items = h->c_items.as<int4>();
-    w.item_cap = (int64_t)ngroups * nslices;
     w.pair_cnt = h->c_pcnt.as<int32_t>();
     w.pair_off = h->c_poff.as<int64_t>();
     w.pairs = h->c_pairs.as<int32_t>();
@@ -688,8 +693,6 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     w.work = h->c_work.as<unsigned int>();
     w.cand = h->c_cand.as<uint64_t>();
     w.cand_cnt = h->c_ccnt.as<int32_t>();
-    HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, nslices, h->c_off.as<int64_t>(), h->c_size.as<int32_t>(), w,
-                                    s));
     hy::BatchedLaunch b;
     b.abf = h->c_img.p;
     b.list_off = h->c_off.as<int64_t>();
@@ -699,20 +702,54 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     b.xaux = h->c_aux.as<float2>();
     b.qb = h->b_qb.p;
     b.qaux = h->b_qn.as<float4>();
-    b.thr = h->b_thr.as<float>();  // not read by a dense launch's test
+    b.thr = h->b_thr.as<float>();
     b.nlist = 1;
     b.d = (int)h->d;
-    b.rs = rs;
-    b.capq = nlist;
     b.metric = h->metric;
     b.nsm = h->nsm;
     b.qg = qg;
     b.f8 = false;
-    b.dense_max = nlist;
+    if (nlist <= 2048) {
+        // Every (query, centroid) {score, bound} pair, then the exact best.
+        w.item_cap = (int64_t)ngroups * ns_full;
+        HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, ns_full, h->c_off.as<int64_t>(),
+                                        h->c_size.as<int32_t>(), w, s));
+        b.rs = rs_full;
+        b.capq = nlist;
+        b.dense_max = nlist;
+        HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+        HY_CUDA(hy::launch_coarse_refine(reinterpret_cast<float2*>(h->c_cand.p), (int)m, nlist, qq,
+                                         h->cent.as<float>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+        h->launches += 3;
+        return HY_OK;
+    }
+    // More lists: a dense launch over the first S centroids bounds each
+    // query's nprobe-th best score (b_thr); a thresholded launch over all
+    // centroids emits the keys that can reach it (stride nlist, no
+    // overflow); the keys are selected and re-scored exactly.
+    const int S = 1024;
+    int rs_a;
+    const int ns_a = slicing(S, &rs_a);
+    w.item_cap = (int64_t)ngroups * ns_a;
+    HY_CUDA(hy::launch_coarse_items((int)m, S, ngroups, ns_a, h->c_off.as<int64_t>(), h->c_size.as<int32_t>(), w, s));
+    b.rs = rs_a;
+    b.capq = S;
+    b.dense_max = S;
     HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
-    HY_CUDA(hy::launch_coarse_refine(reinterpret_cast<float2*>(h->c_cand.p), (int)m, nlist, qq,
-                                     h->cent.as<float>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
-    h->launches += 3;
+    HY_CUDA(hy::launch_coarse_thr(reinterpret_cast<const float2*>(h->c_cand.p), (int)m, S, (int)nprobe,
+                                  h->b_thr.as<float>(), s));
+    w.item_cap = (int64_t)ngroups * ns_full;
+    HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, ns_full, h->c_off.as<int64_t>(), h->c_size.as<int32_t>(),
+                                    w, s));
+    HY_CUDA(cudaMemsetAsync(w.cand_cnt, 0, m * sizeof(int32_t), s));
+    b.rs = rs_full;
+    b.capq = nlist;
+    b.dense_max = 0;
+    HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
+    HY_CUDA(hy::launch_coarse_refine_keys(h->c_cand.as<uint64_t>(), w.cand_cnt, (int)m, nlist, qq, h->cent.as<float>(),
+                                          h->c_norm.as<float>(), h->c_aux.as<float2>(), h->b_qn.as<float4>(),
+                                          (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+    h->launches += 6;
     return HY_OK;
 }
 

@@ -160,7 +160,9 @@ HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample
  * rigorous error bounds, then exact FP32 scores only for the centroids whose
  * bound can reach the nprobe-th best; the probe lists (and the learned
  * predictor's coarse scores) are identical to HY_COARSE_EXACT's.  Used when
- * nlist <= 2048, nprobe <= 256 and d <= 256; otherwise the exact path runs.
+ * nprobe <= 256 and d <= 256 (above 2048 lists in two tensor-core launches:
+ * a bound from the first 1024 centroids, then a thresholded pass over all);
+ * otherwise the exact path runs.
  * The plain and e4m3 forms always use the exact path. */
 enum { HY_COARSE_EXACT = 0, HY_COARSE_TENSOR = 1 };
 HY_API int hy_index_set_coarse(hy_index* h, int mode);

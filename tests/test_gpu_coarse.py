@@ -95,3 +95,49 @@ def test_set_coarse_rejects_unknown_mode(wide):
     idx, x, q = wide
     with pytest.raises(hb.HyError):
         idx.set_coarse(7)
+
+
+@pytest.fixture(scope="module")
+def many_lists():
+    # 4,096 lists (above 2,048: the two-launch tensor-core coarse step).
+    x, q = datasets.gmm_uint8(200_000, 2_000, d=64, ncomp=4_096, sigma=15.0, seed=43)
+    idx = hb.Index(64, 4096, 64)
+    idx.train(x)
+    idx.add(x)
+    return idx, x, q
+
+
+@pytest.mark.parametrize("nprobe", [1, 32, 128, 256])
+def test_tensor_probes_equal_exact_above_2048_lists(many_lists, nprobe):
+    idx, x, q = many_lists
+    idx.nprobe = nprobe
+    try:
+        plain = idx.probes(q)
+        got = _probes(idx, q, "tensor")
+    finally:
+        idx.nprobe = 64
+    np.testing.assert_array_equal(got, plain)
+
+
+def test_search_above_2048_lists_equals_plain(many_lists):
+    idx, x, q = many_lists
+    Dp, Ip = idx.search(q, 20)
+    idx.set_form("bf16")
+    try:
+        Dt, It = idx.search(q, 20)
+    finally:
+        idx.set_form("plain")
+    np.testing.assert_array_equal(It, Ip)
+    np.testing.assert_array_equal(Dt, Dp)
+
+
+def test_inner_product_above_2048_lists():
+    rng = np.random.default_rng(44)
+    x = rng.standard_normal((60_000, 32)).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    q = x[rng.integers(0, 60_000, 500)] + 0.05 * rng.standard_normal((500, 32)).astype(np.float32)
+    idx = hb.Index(32, 3000, 40, 0)
+    idx.train(x)
+    idx.add(x)
+    plain = idx.probes(q)
+    np.testing.assert_array_equal(_probes(idx, q, "tensor"), plain)
