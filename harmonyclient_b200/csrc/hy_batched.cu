@@ -1120,7 +1120,7 @@ __device__ inline void tighten_warp_query(int qi, int cnt, const float* __restri
 template <typename Get>
 __device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int lane) {
     uint32_t mn = 0xffffffffu, mx = 0u;
-#pragma unroll 4
+#pragma unroll 8
     for (int e = lane; e < cnt; e += 32) {
         const float2 v = get(e);
         const uint32_t h = f2o(v.x + v.y);
@@ -1143,7 +1143,7 @@ __device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int
 #pragma unroll
             for (int i = 0; i < 8; ++i) hist[lane * 8 + i] = 0;
             __syncwarp();
-#pragma unroll 4
+#pragma unroll 8
             for (int e = lane; e < cnt; e += 32) {
                 const float2 v = get(e);
                 const uint32_t h = f2o(v.x + v.y);
@@ -1208,19 +1208,28 @@ __device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const 
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     const float2* ce = reinterpret_cast<const float2*>(cq);
     const float U = cnt >= k ? dense_kth_bound(ce, cnt, k, hist, lane) : INFINITY;
-    // In-place rewrite: every element of a round is read before any of that
-    // round's writes, and writes never pass the round's reads.
+    // In-place rewrite, four rounds of 32 at a time: all four rounds are
+    // read (loads in flight together) before any of their writes, and writes
+    // never pass the reads.
     int m = 0;
-    for (int base = 0; base < cnt; base += 32) {
-        const int e = base + lane;
-        const float2 v = e < cnt ? ce[e] : make_float2(0.0f, 0.0f);
-        const bool keep = e < cnt && v.x - v.y <= U;
-        const unsigned b = __ballot_sync(FULL, keep);
+    for (int base = 0; base < cnt; base += 128) {
+        float2 v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = base + 32 * i + lane;
+            v[i] = e < cnt ? ce[e] : make_float2(0.0f, 0.0f);
+        }
         __syncwarp();
-        if (keep)
-            cq[m + __popc(b & ((1u << lane) - 1u))] =
-                (static_cast<uint64_t>(f2o(v.x)) << 32) | static_cast<uint32_t>(row0 + e);
-        m += __popc(b);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = base + 32 * i + lane;
+            const bool keep = e < cnt && v[i].x - v[i].y <= U;
+            const unsigned b = __ballot_sync(FULL, keep);
+            if (keep)
+                cq[m + __popc(b & ((1u << lane) - 1u))] =
+                    (static_cast<uint64_t>(f2o(v[i].x)) << 32) | static_cast<uint32_t>(row0 + e);
+            m += __popc(b);
+        }
     }
     if (lane == 0) {
         w.cand_cnt[qi] = m;
