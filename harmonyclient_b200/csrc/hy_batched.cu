@@ -1436,8 +1436,7 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
                     acc = METRIC == METRIC_L2 ? sq_add(acc, qs[jj], row[jj]) : ip_add(acc, qs[jj], row[jj]);
             }
             const float score = METRIC == METRIC_L2 ? acc : -acc;
-            const uint64_t cid = keys[c0 + lane];
-            keys[c0 + lane] = (static_cast<uint64_t>(f2o(score)) << 32) | cid;
+            keys[c0 + lane] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cidr);
         }
         __syncwarp();
     }
@@ -1453,11 +1452,16 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
             kk[r] = e < c ? keys[e] : KEY_MAX;
             rank[r] = 0;
         }
-#pragma unroll 4
-        for (int j = 0; j < c; ++j) {
-            const uint64_t kj = keys[j];
+        // Every key, broadcast from the lane that holds it.
 #pragma unroll
-            for (int r = 0; r < 4; ++r) rank[r] += kj < kk[r] ? 1 : 0;
+        for (int r = 0; r < 4; ++r) {
+            if (r * 32 >= c) break;  // warp-uniform
+            const int lim = min(32, c - r * 32);
+            for (int src = 0; src < lim; ++src) {
+                const uint64_t kj = __shfl_sync(FULL, kk[r], src);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) rank[i] += kj < kk[i] ? 1 : 0;
+            }
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
