@@ -147,10 +147,12 @@ HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
 HY_API int hy_index_set_form(hy_index* h, int form);
 
 /* bf16 form parameters (0 keeps the current value): candidate slots per
- * query (default 8192, at most 12288), re-rank oversampling factor (kept for
- * compatibility: the re-rank set is chosen by error bounds) and rows per work
- * item (default 2048, a multiple of 128, at most 2048).  The bf16 form uses at
- * most 3 warm-up lists (its warm-up threshold only bounds the first pass). */
+ * query (default 8192, at most 12288; the first pass scans each query's
+ * nearest list densely when it has at most this many rows), re-rank
+ * oversampling factor (e4m3 form: at most oversample x k candidates are
+ * re-ranked) and rows per work item (default 2048, a multiple of 128, at most
+ * 2048).  The bf16 form runs the warm-up (at most 3 lists) only for queries
+ * whose nearest list is not scanned densely or has fewer than k rows. */
 HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice);
 
 /* Coarse quantiser of the bf16 form (no counterpart in the reference, which
