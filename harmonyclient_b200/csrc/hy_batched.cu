@@ -1,26 +1,29 @@
-// Batched list-major scan on the tcgen05 tensor cores (the "bf16" form).
+// Batched list-major scan on the tcgen05 tensor cores (the "bf16" and
+// "e4m3" forms) and the steps around it.
 //
 // Queries that probe the same list share one pass over it.  After coarse
 // quantisation, the (query, probed list) pairs are inverted into per-list
 // query groups; a persistent kernel (one CTA per SM) drains a work queue of
-// (list, group of <=128 queries, slice of <=RS rows) items.  Per item the CTA
-// gathers the group's bf16 query vectors into shared memory (the MMA's B
-// operand), then streams the slice's 128-row tiles of the bf16 list arena
-// (already stored in the tensor core's swizzled shared-memory image, so each
-// 64-dimension k-block of a tile is one 16 KiB bulk copy) through a ring of
-// stages.  One thread issues tcgen05.mma (M = 128 rows, N = 128 queries,
-// K = 16) into one of two TMEM accumulators; four epilogue warps read the
-// accumulator (thread = row), form dist = |x|^2 + |q|^2 - 2 q.x (or -q.x for
-// inner product) and emit every (query, row) whose distance passes the
-// query's threshold into that query's candidate buffer.  A final kernel
-// re-ranks each query's best candidates with the exact FP32 distance (the
-// plain scan's arithmetic) and writes the top-k.
+// (list, group of <=128 queries, slice of <=2048 rows) items.  Per item the
+// CTA gathers the group's query vectors into shared memory (the MMA's B
+// operand), then streams the slice's 128-row tiles of the list image (already
+// in the tensor core's swizzled shared-memory layout, so each k-block of a
+// tile is one 16 KiB bulk copy) through a ring of stages.  One thread issues
+// tcgen05.mma (M = 128 rows, N = up to 128 queries) into one of two TMEM
+// accumulators; eight epilogue warps read the accumulator (thread = row) and
+// form dist = |x|^2 + |q|^2 - 2 q.x (or -q.x for inner product) with a
+// rigorous bound on its distance from the plain scan's exact FP32 value.
 //
-// The threshold is an upper bound on the query's final k-th distance (the
-// warm-up threshold), so no row of the exact top-k is rejected as long as its
-// bf16 distance is not above it; on integer-valued data below 2^8 the bf16
-// distances are exact.  A query whose candidates overflow its buffer is
-// reported so the caller can answer it with the plain scan.
+// First pass (each query's nearest list): dense items write {dist, bound}
+// for every row; the tightening step takes each query's k-th smallest
+// dist + bound as its threshold and keeps the rows whose dist - bound reach
+// it.  Second pass (the other probed lists): rows whose dist - bound passes
+// the threshold are emitted as candidates.  The re-rank keeps the candidates
+// whose bound can reach the top-k and gives them the exact FP32 distance (or
+// keeps the tensor-core distance when the exactness certificate shows it is
+// exact), so the answer is the plain scan's.  A query whose candidates
+// overflow its buffer is answered again by the plain scan.  The same kernel,
+// over the centroids as a one-list index, is the coarse step of the bf16 form.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
