@@ -157,6 +157,12 @@ class Index {
     // Scan form: HY_FORM_PLAIN (exact FP32 scan) or HY_FORM_BF16 (batched
     // tensor-core scan with exact FP32 re-rank).  Not in the reference.
     void set_form(int form) { hy_throw_if(hy_index_set_form(h_, form)); }
+    // Coarse step of the bf16 form: HY_COARSE_TENSOR (default) or
+    // HY_COARSE_EXACT; the probe lists are the same.  Not in the reference.
+    void set_coarse(int mode) { hy_throw_if(hy_index_set_coarse(h_, mode)); }
+    // Replay repeated searches of one shape as a captured CUDA graph.  Not in
+    // the reference.
+    void set_graph(bool on) { hy_throw_if(hy_index_set_graph(h_, on ? 1 : 0)); }
 
     void save_index(std::string path) const {
         const_cast<Index*>(this)->push_centroids();
