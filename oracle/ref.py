@@ -60,6 +60,11 @@ def load():
     L.ref_save.argtypes = [vp, C.c_char_p]
     L.ref_load.argtypes = [vp, C.c_char_p]
     L.ref_info.argtypes = [vp] + [C.POINTER(C.c_size_t)] * 3 + [C.POINTER(C.c_int)]
+    L.ref_xvecs_info.argtypes = [C.c_char_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+    L.ref_load_xvecs.argtypes = [C.c_char_p, C.c_int, C.c_int, fp, sz, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+    L.ref_write_results.argtypes = [ip64, fp, sz, sz, C.c_char_p]
+    L.ref_load_results.argtypes = [C.c_char_p, ip64, fp, sz, sz]
+    L.ref_recall.argtypes = [C.c_int, ip64, fp, ip64, fp, sz, sz, C.c_int, sz, C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -177,3 +182,40 @@ class RefIndex:
         d, nl, npb, m = C.c_size_t(), C.c_size_t(), C.c_size_t(), C.c_int()
         _check(self.L.ref_info(self.h, C.byref(d), C.byref(nl), C.byref(npb), C.byref(m)))
         self.d, self.nlist, self.metric = d.value, nl.value, m.value
+
+
+# The reference's dataset / result-file readers and recall metrics
+# (src/utils.h), for the golden fixtures of harmonyclient_b200/io.py.
+def xvecs_info(path):
+    n, d = C.c_size_t(), C.c_int()
+    _check(load().ref_xvecs_info(str(path).encode(), C.byref(n), C.byref(d)))
+    return n.value, d.value
+
+
+def load_xvecs(path, a=1, b=0, cap=1 << 20):
+    out = np.zeros(cap, np.float32)
+    n, d = C.c_size_t(), C.c_int()
+    _check(load().ref_load_xvecs(str(path).encode(), a, b, _p(out), cap, C.byref(n), C.byref(d)))
+    return out[:n.value * d.value].reshape(n.value, d.value).copy()
+
+
+def write_results(labels, distances, path):
+    labels = np.ascontiguousarray(labels, np.int64)
+    distances = np.ascontiguousarray(distances, np.float32)
+    nq, k = labels.shape
+    _check(load().ref_write_results(_p(labels), _p(distances), nq, k, str(path).encode()))
+
+
+def load_results(path, nq, k):
+    labels = np.zeros((nq, k), np.int64)
+    dist = np.zeros((nq, k), np.float32)
+    _check(load().ref_load_results(str(path).encode(), _p(labels), _p(dist), nq, k))
+    return labels, dist
+
+
+def recall(which, I, D, GT, GD, nq, k, metric, gt_k=0):
+    I, GT = np.ascontiguousarray(I, np.int64), np.ascontiguousarray(GT, np.int64)
+    D, GD = np.ascontiguousarray(D, np.float32), np.ascontiguousarray(GD, np.float32)
+    out = C.c_float()
+    _check(load().ref_recall(which, _p(I), _p(D), _p(GT), _p(GD), nq, k, metric, gt_k, C.byref(out)))
+    return out.value

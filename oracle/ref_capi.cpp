@@ -245,3 +245,57 @@ extern "C" int ref_info(void* h, size_t* d, size_t* nlist, size_t* nprobe, int* 
         *metric = static_cast<int>(I.metric);
     });
 }
+
+// ---------------------------------------------------------------------------
+// The reference's dataset / result-file readers and recall metrics
+// (src/utils.h:187-407, 565-756), for the golden fixtures of
+// harmonyclient_b200/io.py.
+static void xvecs_info(const char* path, size_t* n, int* d) {
+    const std::pair<size_t, int> r = harmony::loadXvecsInfo(path);
+    *n = r.first;
+    *d = r.second;
+}
+
+extern "C" int ref_xvecs_info(const char* path, size_t* n, int* d) { REF_TRY({ xvecs_info(path, n, d); }); }
+
+static void load_xvecs(const char* path, int a, int b, float* out, size_t cap, size_t* n, int* d) {
+    auto t = harmony::loadXvecs(path, std::make_pair(a, b));
+    const size_t nn = std::get<1>(t);
+    const int dd = std::get<2>(t);
+    if (nn * static_cast<size_t>(dd) > cap) throw std::runtime_error("ref_load_xvecs: output too small");
+    std::memcpy(out, std::get<0>(t).get(), nn * static_cast<size_t>(dd) * sizeof(float));
+    *n = nn;
+    *d = dd;
+}
+
+// Rows a..b (1-based, b = 0: to the end) of a .fvecs / .bvecs / .txt file as
+// float32 (the reference's loadXvecs); out must hold cap floats.
+extern "C" int ref_load_xvecs(const char* path, int a, int b, float* out, size_t cap, size_t* n, int* d) {
+    REF_TRY({ load_xvecs(path, a, b, out, cap, n, d); });
+}
+
+extern "C" int ref_write_results(const int64_t* labels, const float* distances, size_t nq, size_t k,
+                                 const char* path) {
+    REF_TRY({ harmony::writeResultsToFile(reinterpret_cast<const idx_t*>(labels), distances, nq, k, path); });
+}
+
+extern "C" int ref_load_results(const char* path, int64_t* labels, float* distances, size_t nq, size_t k) {
+    REF_TRY({ harmony::loadResults(path, reinterpret_cast<idx_t*>(labels), distances, nq, k); });
+}
+
+// which: 0 calculate_recall, 1 calculate_recall_loose, 2 calculate_r2.
+static float recall_of(int which, const int64_t* I, const float* D, const int64_t* GT, const float* GD, size_t nq,
+                       size_t k, int metric, size_t gt_k) {
+    const auto m = static_cast<harmony::MetricType>(metric);
+    const auto* i = reinterpret_cast<const idx_t*>(I);
+    const auto* g = reinterpret_cast<const idx_t*>(GT);
+    Quiet q;
+    if (which == 0) return harmony::calculate_recall(i, D, g, GD, nq, k, m, gt_k);
+    if (which == 1) return harmony::calculate_recall_loose(i, D, g, GD, nq, k, m, gt_k);
+    return harmony::calculate_r2(i, D, g, GD, nq, k, m, gt_k);
+}
+
+extern "C" int ref_recall(int which, const int64_t* I, const float* D, const int64_t* GT, const float* GD, size_t nq,
+                          size_t k, int metric, size_t gt_k, float* out) {
+    REF_TRY({ *out = recall_of(which, I, D, GT, GD, nq, k, metric, gt_k); });
+}
