@@ -185,7 +185,7 @@ class RefIndex:
 
 
 # The reference's dataset / result-file readers and recall metrics
-# (src/utils.h), for the golden fixtures of harmonyclient_b200/io.py.
+# (src/utils.h), for the golden fixtures of harmonyclient_b200/datafiles.py.
 def xvecs_info(path):
     n, d = C.c_size_t(), C.c_int()
     _check(load().ref_xvecs_info(str(path).encode(), C.byref(n), C.byref(d)))

@@ -249,7 +249,7 @@ extern "C" int ref_info(void* h, size_t* d, size_t* nlist, size_t* nprobe, int* 
 // ---------------------------------------------------------------------------
 // The reference's dataset / result-file readers and recall metrics
 // (src/utils.h:187-407, 565-756), for the golden fixtures of
-// harmonyclient_b200/io.py.
+// harmonyclient_b200/datafiles.py.
 static void xvecs_info(const char* path, size_t* n, int* d) {
     const std::pair<size_t, int> r = harmony::loadXvecsInfo(path);
     *n = r.first;

@@ -17,7 +17,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from harmonyclient_b200 import io  # noqa: E402
+from harmonyclient_b200 import datafiles as io  # noqa: E402
 from oracle import ref  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "io")

@@ -1,4 +1,4 @@
-"""Dataset, result-file and recall utilities (harmonyclient_b200/io.py)
+"""Dataset, result-file and recall utilities (harmonyclient_b200/datafiles.py)
 against the reference's own readers and metrics: the fixtures in
 tests/golden/io/ were produced by the reference's src/utils.h code
 (tests/golden/make_io_golden.py)."""
@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from harmonyclient_b200 import io
+from harmonyclient_b200 import datafiles as io
 
 G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "io")
 
