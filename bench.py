@@ -131,9 +131,15 @@ WORKLOADS = {
 
 
 def queries(args, n, query_seed):
-    """Another query set from the workload's mixture."""
+    """Another query set from the workload's mixture (file workloads: n rows
+    of the base file, seeded)."""
     from harmonyclient_b200 import datasets
     W = WORKLOADS[args.workload]
+    if W.get("files"):
+        from harmonyclient_b200 import datafiles
+        x = datafiles.load_xvecs(W["files"][0], (1, args.nb))
+        pick = np.random.default_rng(query_seed).choice(x.shape[0], size=min(n, x.shape[0]), replace=False)
+        return np.ascontiguousarray(x[np.sort(pick)], np.float32)
     return getattr(datasets, W["gen"])(0, n, seed=0, query_seed=query_seed, **W["kw"])[1]
 
 
@@ -145,9 +151,23 @@ def per_query_nprobe(args, nq):
     return np.random.default_rng(1).integers(lo_hi[0], lo_hi[1] + 1, size=nq).astype(np.int32)
 
 
+def file_workload(base_file, query_file, nb, nq):
+    """Base and query rows from .fvecs / .bvecs / .txt files (the reference's
+    readers, harmonyclient_b200.datafiles): the first nb / nq rows (0: all)."""
+    from harmonyclient_b200 import datafiles
+    x = datafiles.load_xvecs(base_file, (1, nb or 0))
+    q = datafiles.load_xvecs(query_file, (1, nq or 0))
+    if x.shape[1] != q.shape[1]:
+        raise SystemExit(f"base d {x.shape[1]} != query d {q.shape[1]}")
+    return np.ascontiguousarray(x, np.float32), np.ascontiguousarray(q, np.float32)
+
+
 def workload(args, rank):
     from harmonyclient_b200 import datasets
     W = WORKLOADS[args.workload]
+    if W.get("files"):
+        # Every rank searches the file's queries.
+        return file_workload(W["files"][0], W["files"][1], args.nb, args.nq)
     x, q = getattr(datasets, W["gen"])(args.nb, args.nq, seed=0, **W["kw"])
     if rank:
         # Other ranks search their own queries from the same mixture.
@@ -569,7 +589,7 @@ def run_reference(args, rank):
     return {
         "metric": METRIC, "value": round(v, 2), "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": W["data"],
         "impl": "reference",
         "config": {"workload": W["desc"].format(nb=args.nb) + f", nlist {nlist}, nprobe {args.nprobe}, k {k}",
                    "name": args.workload, "queries_per_step": per_step},
@@ -606,7 +626,23 @@ def main():
     ap.add_argument("--recall-sample", type=int, default=0, help="queries scored for recall (0: all)")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=5.0)
+    ap.add_argument("--base-file", default=None,
+                    help="base vectors (.fvecs / .bvecs / .txt) instead of the workload's synthetic data; the "
+                         "workload keeps its nlist, nprobe and k")
+    ap.add_argument("--query-file", default=None, help="query vectors for --base-file")
     args = ap.parse_args()
+    if args.base_file:
+        if not args.query_file:
+            raise SystemExit("--base-file needs --query-file")
+        from harmonyclient_b200 import datafiles
+        nb_f, d_f = datafiles.load_xvecs_info(args.base_file)
+        nq_f, _ = datafiles.load_xvecs_info(args.query_file)
+        args.nb = min(args.nb or nb_f, nb_f)
+        args.nq = min(args.nq or nq_f, nq_f)
+        name = f"{os.path.basename(args.base_file)} / {os.path.basename(args.query_file)}"
+        WORKLOADS[args.workload] = {**WORKLOADS[args.workload], "files": (args.base_file, args.query_file),
+                                    "d": d_f, "desc": "{nb} x " + f"{d_f} vectors of {name}",
+                                    "data": f"file: {name}", "per_query": None}
     W = WORKLOADS[args.workload]
     args.nb = W["nb"] if args.nb is None else args.nb
     args.nq = W["nq"] if args.nq is None else args.nq

@@ -82,3 +82,16 @@ def test_csv_rows(tmp_path):
     f = lines[1].split(",")
     assert f[8:11] == ["1", "0", "1"]
     assert f[16] == "1.5000000000000000" and f[19] == "0.9500000"
+
+
+def test_bench_reads_vector_files(tmp_path):
+    """bench.py --base-file / --query-file: the first nb / nq rows."""
+    import bench
+
+    x = np.arange(60, dtype=np.float32).reshape(10, 6)
+    q = np.arange(18, dtype=np.float32).reshape(3, 6)
+    io.write_fvecs(str(tmp_path / "b.fvecs"), x)
+    io.write_bvecs(str(tmp_path / "q.bvecs"), q.astype(np.uint8))
+    xb, qb = bench.file_workload(str(tmp_path / "b.fvecs"), str(tmp_path / "q.bvecs"), 7, 0)
+    np.testing.assert_array_equal(xb, x[:7])
+    np.testing.assert_array_equal(qb, q)
