@@ -151,12 +151,28 @@ def per_query_nprobe(args, nq):
     return np.random.default_rng(1).integers(lo_hi[0], lo_hi[1] + 1, size=nq).astype(np.int32)
 
 
+def _bvecs_records(path):
+    """The layout of a .bvecs file, told from its size: plain records (the
+    public BIGANN files) or the reference loader's extra 4-byte header."""
+    from harmonyclient_b200 import datafiles
+    return str(path).endswith(".bvecs") and datafiles.bvecs_is_records(path)
+
+
+def _file_info(path):
+    """(rows, d) of a vector file, .bvecs counted in its own layout."""
+    from harmonyclient_b200 import datafiles
+    n, d = datafiles.load_xvecs_info(path)
+    if str(path).endswith(".bvecs"):
+        n = datafiles.bvecs_rows(path, _bvecs_records(path))
+    return n, d
+
+
 def file_workload(base_file, query_file, nb, nq):
     """Base and query rows from .fvecs / .bvecs / .txt files (the reference's
     readers, harmonyclient_b200.datafiles): the first nb / nq rows (0: all)."""
     from harmonyclient_b200 import datafiles
-    x = datafiles.load_xvecs(base_file, (1, nb or 0))
-    q = datafiles.load_xvecs(query_file, (1, nq or 0))
+    x = datafiles.load_xvecs(base_file, (1, nb or 0), _bvecs_records(base_file))
+    q = datafiles.load_xvecs(query_file, (1, nq or 0), _bvecs_records(query_file))
     if x.shape[1] != q.shape[1]:
         raise SystemExit(f"base d {x.shape[1]} != query d {q.shape[1]}")
     return np.ascontiguousarray(x, np.float32), np.ascontiguousarray(q, np.float32)
@@ -192,10 +208,29 @@ def cpu_baseline_ref(x, q, cent, nprobe, k, budget_s):
     dt = time.perf_counter() - t0
     m2 = int(min(q.shape[0], max(m, m * budget_s / max(dt, 1e-6))))
     t0 = time.perf_counter()
-    R.search(q[:m2], k)
+    Dr, Ir = R.search(q[:m2], k)
     dt = time.perf_counter() - t0
-    return {"value": m2 / dt, "unit": "queries/s", "cores": nt, "kind": "reference",
+    info = {"value": m2 / dt, "unit": "queries/s", "cores": nt, "kind": "reference",
             "sample": f"{m2} of {q.shape[0]} queries, reference Index::search ORIGINAL mode, OpenMP x{nt}"}
+    return info, Dr, Ir
+
+
+def parity_block(Dr, Ir, answers, q, cent, nprobe, k, integral):
+    """Row-by-row comparison of the GPU forms' answers with the reference's
+    Index::search on the same centroids (tests/topk_check.py rules): on
+    integer-valued data distances bit-equal (rtol 0), else within 1e-5
+    relative; ids equal below the k-th distance; queries whose nprobe-th and
+    (nprobe+1)-th centroid distances tie within 1e-5 in FP64 are skipped."""
+    from tests.topk_check import probe_tied_rows, row_agree
+    m = Dr.shape[0]
+    tied = probe_tied_rows(q[:m], cent, np.zeros((1, nprobe)), 1)
+    rtol = 0.0 if integral else 1e-5
+    out = {"vs": "reference Index::search, ORIGINAL mode (oracle/_ref), same centroids and lists",
+           "queries": m, "nprobe": nprobe, "k": k, "rtol": rtol, "probe_tied_skipped": len(tied)}
+    for name, (D, I) in answers.items():
+        eq = sum(1 for r in range(m) if r not in tied and row_agree(Dr[r], Ir[r], D[r], I[r], rtol)[0])
+        out[name] = {"rows_compared": m - len(tied), "rows_equal": eq}
+    return out
 
 
 def _search(idx, dq, dD, dI, k, ts, npq=None):
@@ -444,8 +479,28 @@ def run_ours(args, rank, world, dist):
                                    "algorithmic_bytes": palg},
                       "clocks": plain["clocks"]}
 
-    if W.get("cpu_ref", True):
-        cpu = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
+    parity = None
+    if W.get("cpu_ref", True) and npq_host is None:
+        got = cpu_baseline_ref(x, q, idx.centroid_codes, args.nprobe, k, args.cpu_budget)
+        cpu = got[0] if got else None
+        if got:
+            # The GPU forms at the reference's fixed nprobe, on the same queries.
+            answers = {}
+            if plain is not None:
+                answers["plain_fp32"] = (plain["D"], plain["I"])
+            if learned:
+                idx.set_learned(False)
+            if base != "plain":
+                Db, Ib = idx.search(q[:got[1].shape[0]], k)
+                answers[f"{base}_fixed_nprobe"] = (Db, Ib)
+            else:
+                answers["plain_fp32"] = (D_main, I_main)
+            if learned:
+                idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
+            integral = bool(np.all(x == np.rint(x)) and np.all(q == np.rint(q)) and np.abs(x).max() <= 255)
+            parity = parity_block(got[1], got[2], answers, q, idx.centroid_codes, args.nprobe, k, integral)
+    elif W.get("cpu_ref", True):
+        cpu = None
     else:
         cpu = {"value": None, "unit": "queries/s", "cores": os.cpu_count(), "kind": "reference",
                "unavailable": "the reference's host add() of this base (nearest of nlist centroids for every row) "
@@ -488,6 +543,7 @@ def run_ours(args, rank, world, dist):
         "plain_fp32": plain_line,
         "warmup_list": args.warmup_list,
         "fallback_queries": fallback,
+        "parity": parity,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "build_s": round(build_s, 2),
@@ -634,9 +690,8 @@ def main():
     if args.base_file:
         if not args.query_file:
             raise SystemExit("--base-file needs --query-file")
-        from harmonyclient_b200 import datafiles
-        nb_f, d_f = datafiles.load_xvecs_info(args.base_file)
-        nq_f, _ = datafiles.load_xvecs_info(args.query_file)
+        nb_f, d_f = _file_info(args.base_file)
+        nq_f, _ = _file_info(args.query_file)
         args.nb = min(args.nb or nb_f, nb_f)
         args.nq = min(args.nq or nq_f, nq_f)
         name = f"{os.path.basename(args.base_file)} / {os.path.basename(args.query_file)}"

@@ -1913,13 +1913,9 @@ __global__ void fb_gather_kernel(const int32_t* __restrict__ ovf, const float* _
 
 __global__ void fb_scatter_kernel(const int32_t* __restrict__ ovf, const float* __restrict__ fD,
                                   const int64_t* __restrict__ fI, int k, int cap, float* __restrict__ D,
-                                  int64_t* __restrict__ I, unsigned long long* total, unsigned long long* unresolved) {
-    const int all = ovf[0];
-    const int cnt = min(all, cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        atomicAdd(total, static_cast<unsigned long long>(cnt));
-        if (all > cnt) atomicAdd(unresolved, static_cast<unsigned long long>(all - cnt));
-    }
+                                  int64_t* __restrict__ I, unsigned long long* total) {
+    const int cnt = min(ovf[0], cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(total, static_cast<unsigned long long>(cnt));
     for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
         const int qi = ovf[1 + i];
         for (int j = threadIdx.x; j < k; j += blockDim.x) {
@@ -1992,8 +1988,8 @@ cudaError_t launch_fb_gather(const int32_t* ovf, const float* q, const int64_t* 
 }
 
 cudaError_t launch_fb_scatter(const int32_t* ovf, const float* fD, const int64_t* fI, int k, int cap, float* D,
-                              int64_t* I, unsigned long long* total, unsigned long long* unresolved, cudaStream_t s) {
-    fb_scatter_kernel<<<64, 128, 0, s>>>(ovf, fD, fI, k, cap, D, I, total, unresolved);
+                              int64_t* I, unsigned long long* total, cudaStream_t s) {
+    fb_scatter_kernel<<<64, 128, 0, s>>>(ovf, fD, fI, k, cap, D, I, total);
     return cudaGetLastError();
 }
 

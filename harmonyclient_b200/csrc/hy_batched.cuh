@@ -164,13 +164,13 @@ cudaError_t launch_rerank(const ArenaLayout& L, const float* codes, const int64_
 cudaError_t launch_fill_f32(float* p, int64_t n, float v, cudaStream_t s);
 
 // Device-side exact fallback for queries whose candidates overflowed
-// (w.overflow: count, then chunk-local query ids).  Gather packs the first
-// `cap` of them (vectors and probe rows) to the front of fq / fprobes;
-// scatter writes their plain-scan results back into D / I and adds the count
-// to *total (and the ones beyond `cap` to *unresolved).
+// (w.overflow: count, then chunk-local query ids).  Gather packs them
+// (vectors and probe rows) to the front of fq / fprobes; scatter writes their
+// plain-scan results back into D / I and adds the count to *total.  `cap` is
+// the chunk's query count, so every overflowed query of the chunk fits.
 cudaError_t launch_fb_gather(const int32_t* ovf, const float* q, const int64_t* probes, int nprobe, int d, int cap,
                              float* fq, int64_t* fprobes, int32_t* fcount, cudaStream_t s);
 cudaError_t launch_fb_scatter(const int32_t* ovf, const float* fD, const int64_t* fI, int k, int cap, float* D,
-                              int64_t* I, unsigned long long* total, unsigned long long* unresolved, cudaStream_t s);
+                              int64_t* I, unsigned long long* total, cudaStream_t s);
 
 }  // namespace hy

@@ -118,7 +118,7 @@ struct HostStatus {
     int err = 0;
     unsigned long long counters[2] = {0, 0};  // scan tile-block counters
     unsigned long long learned_total = 0;     // sum of the learned nprobes
-    unsigned long long fallback[2] = {0, 0};  // device fallback: answered, unresolved
+    unsigned long long fallback = 0;  // queries answered by the device fallback
 };
 
 struct hy_index {
@@ -455,13 +455,11 @@ int check_search_args(hy_index* h, size_t n, size_t k) {
     return HY_OK;
 }
 
-// Overflowed queries per chunk that the bf16 form answers again on the
-// device with the plain scan (more fall back to a plain search of the batch
-// in the host-pointer API).
-constexpr size_t FB_CAP = 296;
-
 // Search n device queries with device probe lists (nprobe per query) into
 // device D/I.  Runs on stream s; does not synchronise.
+// nq_dev (optional): a device count of the queries to search (the first
+// *nq_dev of the n); the scan's CTAs then loop over them, one wave of
+// query slots per SM.
 int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe, const int64_t* dprobes,
                    const uint32_t* init_thr, float* dD, int64_t* dI, cudaStream_t s, bool timed,
                    int64_t* drows = nullptr, const int32_t* nq_dev = nullptr) {
@@ -499,6 +497,10 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
     p.metric = h->metric;
     p.prune = 1;
     p.nq_dev = nq_dev;
+    if (nq_dev) {
+        if (h->nsm == 0) HY_CUDA(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+        p.qgrid = h->nsm;
+    }
     if (timed) HY_CUDA(ev_record(h->ev[2], s));
     h->launches += 2 + (nsplit > 1 ? 1 : 0);
     int smem = 0;
@@ -792,16 +794,16 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
     HY_RET(h->b_big.ensure(2 * (qc + 1) * sizeof(int32_t)));
-    // Exact fallback on the device: up to FB_CAP overflowed queries per chunk
-    // are searched again by the plain scan over the same probe lists.
-    const size_t fbcap = std::min<size_t>(qc, FB_CAP);
+    // Exact fallback on the device: every overflowed query of a chunk is
+    // searched again by the plain scan over the same probe lists.
+    const size_t fbcap = qc;
     HY_RET(h->b_fq.ensure(fbcap * h->d * sizeof(float)));
     HY_RET(h->b_fpr.ensure(fbcap * nprobe * sizeof(int64_t)));
     HY_RET(h->b_fD.ensure(fbcap * k * sizeof(float)));
     HY_RET(h->b_fI.ensure(fbcap * k * sizeof(int64_t)));
     HY_RET(h->b_fcnt.ensure(sizeof(int32_t)));
-    HY_RET(h->b_fbtot.ensure(2 * sizeof(unsigned long long)));
-    HY_CUDA(cudaMemsetAsync(h->b_fbtot.p, 0, 2 * sizeof(unsigned long long), s));
+    HY_RET(h->b_fbtot.ensure(sizeof(unsigned long long)));
+    HY_CUDA(cudaMemsetAsync(h->b_fbtot.p, 0, sizeof(unsigned long long), s));
     // Warm-up for the bf16 form: its threshold only bounds the first pass
     // (each query's nearest list), so three lists suffice by default.  A
     // query whose nearest list has between k and dense_max rows needs none:
@@ -934,8 +936,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         HY_RET(scan_and_merge(h, (size_t)fb, h->b_fq.as<float>(), k, nprobe, h->b_fpr.as<int64_t>(), nullptr,
                               h->b_fD.as<float>(), h->b_fI.as<int64_t>(), s, false, nullptr, h->b_fcnt.as<int32_t>()));
         HY_CUDA(hy::launch_fb_scatter(w.overflow, h->b_fD.as<float>(), h->b_fI.as<int64_t>(), (int)k, fb, dD + q0 * k,
-                                      dI + q0 * k, h->b_fbtot.as<unsigned long long>(),
-                                      h->b_fbtot.as<unsigned long long>() + 1, s));
+                                      dI + q0 * k, h->b_fbtot.as<unsigned long long>(), s));
         h->launches += 3;
         h->launches += nprobe > 1 ? 24 : 18;
     }
@@ -979,7 +980,7 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
     HY_CUDA(cudaMemcpyAsync(st->counters, h->w_counters.p, sizeof(st->counters), cudaMemcpyDeviceToHost, s));
     if (h->m_total.p)
         HY_CUDA(cudaMemcpyAsync(&st->learned_total, h->m_total.p, sizeof(st->learned_total), cudaMemcpyDeviceToHost, s));
-    if (h->b_fbtot.p) HY_CUDA(cudaMemcpyAsync(st->fallback, h->b_fbtot.p, sizeof(st->fallback), cudaMemcpyDeviceToHost, s));
+    if (h->b_fbtot.p) HY_CUDA(cudaMemcpyAsync(&st->fallback, h->b_fbtot.p, sizeof(st->fallback), cudaMemcpyDeviceToHost, s));
     HY_CUDA(cudaStreamSynchronize(s));
     if (st->err != 0) {
         const int err = st->err;
@@ -1074,23 +1075,11 @@ int run_device_search(hy_index* h, size_t n, const float* dq, size_t k, float* d
     return HY_OK;
 }
 
-// Fallback accounting of a bf16 host-pointer search.  Overflowed queries were
-// answered again on the device by the plain scan (up to FB_CAP per chunk);
-// if more overflowed in some chunk, the whole batch is searched again here
-// with the plain form (its queries are still in h->w_q).
-// After finish_host_call (its status block holds the fallback counters).
-int bf16_fallback(hy_index* h, size_t n, size_t k, cudaStream_t s) {
-    const unsigned long long c[2] = {h->hstat->fallback[0], h->hstat->fallback[1]};
-    h->stats.fallback_queries = c[0];
-    h->stats.unresolved_queries = 0;
-    if (c[1] == 0) return HY_OK;
-    const int form = h->form;
-    h->form = HY_FORM_PLAIN;
-    const int rc = search_device_impl(h, n, h->w_q.as<float>(), k, h->w_D.as<float>(), h->w_I.as<int64_t>(), s, false);
-    h->form = form;
-    HY_RET(rc);
-    HY_CUDA(cudaStreamSynchronize(s));
-    h->stats.fallback_queries = n;
+// Fallback accounting of a bf16 host-pointer search: every overflowed query
+// was answered again on the device by the plain scan.  After
+// finish_host_call (its status block holds the fallback counter).
+int bf16_fallback(hy_index* h) {
+    h->stats.fallback_queries = h->hstat->fallback;
     return HY_OK;
 }
 
@@ -1460,22 +1449,7 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     h->stats.fallback_queries = 0;
     h->stats.mean_nprobe = (double)std::min(h->nprobe, h->nlist);
     if (learned_on(h)) h->stats.mean_nprobe = (double)h->hstat->learned_total / (double)n;
-    if (batched_form(h) && h->arena_rows > 0) {
-        const hy_search_stats_t keep = h->stats;
-        HY_RET(bf16_fallback(h, nt, k, s));
-        const uint64_t fb = h->stats.fallback_queries;
-        h->stats = keep;
-        h->stats.fallback_queries = fb;
-        if (fb == nt) {
-            // The whole batch was searched again in the plain form.
-            HY_CUDA(cudaMemcpyAsync(D, h->w_D.p, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
-            HY_CUDA(cudaMemcpyAsync(I, h->w_I.p, n * k * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-            if (m)
-                HY_CUDA(cudaMemcpyAsync(jI, h->w_I.as<int64_t>() + n * k, m * k * sizeof(int64_t),
-                                        cudaMemcpyDeviceToHost, s));
-            HY_CUDA(cudaStreamSynchronize(s));
-        }
-    }
+    if (batched_form(h) && h->arena_rows > 0) HY_RET(bf16_fallback(h));
     return HY_OK;
 }
 
@@ -1953,10 +1927,9 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
         HY_CUDA(cudaEventSynchronize(h->ev[4]));
         collect_times(h);
         if (batched_form(h) && h->b_fbtot.p) {
-            unsigned long long c[2] = {0, 0};
-            HY_CUDA(cudaMemcpy(c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
-            h->stats.fallback_queries = c[0];
-            h->stats.unresolved_queries = c[1];
+            unsigned long long c = 0;
+            HY_CUDA(cudaMemcpy(&c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
+            h->stats.fallback_queries = c;
         }
     }
     *out = h->stats;
@@ -2024,6 +1997,10 @@ int index_view(const hy_index* h, IndexView* v) {
     return HY_OK;
 }
 int set_error(int code, const char* msg) { return fail(code, msg); }
+// The index's call lock: an entry point that reads the index's device data
+// across several launches holds it until its last launch has completed, so
+// a concurrent add / load / reset cannot free that data under it.
+std::mutex& index_mutex(hy_index* h) { return h->mu; }
 }  // namespace hy
 
 // ---------------------------------------------------------------------------

@@ -9,6 +9,7 @@
 // plain scan accumulates each dimension block from zero and adds the block
 // sums in order, which is the order of the reference's 4-chunk pruning loop
 // (src/node.cpp:640-656).
+#include <algorithm>
 #include <cfloat>
 #include <cub/device/device_radix_sort.cuh>
 
@@ -375,8 +376,13 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     const ArenaLayout& L = p.L;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int qi = blockIdx.x / p.nsplit, split = blockIdx.x % p.nsplit;
-    if (p.nq_dev && qi >= *p.nq_dev) return;  // whole CTA, before any barrier
+    const int split = blockIdx.x % p.nsplit;
+    // Queries of this CTA: blockIdx.x / nsplit, then every (grid / nsplit)-th
+    // after it, below the device count when one is given (a grid of nq *
+    // nsplit CTAs takes one query each).
+    const int nq_eff = p.nq_dev ? min(*p.nq_dev, p.nq) : p.nq;
+    const int qstride = gridDim.x / p.nsplit;
+    if (static_cast<int>(blockIdx.x / p.nsplit) >= nq_eff) return;  // whole CTA, before any barrier
     const int npc = (p.nprobe - split + p.nsplit - 1) / p.nsplit;  // probes of this CTA
     const int npa = ((p.nprobe + p.nsplit - 1) / p.nsplit + 3) & ~3;  // table entries, padded for alignment
     const size_t slot_floats = static_cast<size_t>(32) * L.max_pitch;
@@ -392,7 +398,21 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     __shared__ unsigned int s_thr;
     __shared__ int s_next, s_ntiles, s_lock;
 
-    // --- CTA setup: query, probe table (tile prefix), threshold, barriers.
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < W * S; ++i) mbar_init(&bars[i], 1);
+        fence_mbar_init();
+    }
+    // Barrier phases carry over from one query to the next: every copy a
+    // query issues is waited for before its scan ends.
+    uint32_t sphase[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) sphase[s] = 0;
+
+    for (int qi = blockIdx.x / p.nsplit; qi < nq_eff; qi += qstride) {
+    // The previous query's result has been copied out (and, first time, the
+    // barriers are initialised) before the shared state is set up again.
+    __syncthreads();
+    // --- CTA setup: query, probe table (tile prefix), threshold.
     stage_query(L, p.q + static_cast<size_t>(qi) * L.d, qs);
     if (warp == 0) {
         int carry = 0;
@@ -428,10 +448,6 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
         }
     }
     for (int i = threadIdx.x; i < KP; i += blockDim.x) ctop[i] = KEY_MAX;
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < W * S; ++i) mbar_init(&bars[i], 1);
-        fence_mbar_init();
-    }
     __syncthreads();
 
     const int ntiles = s_ntiles;
@@ -449,7 +465,6 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     int sblk[S];
     float spart[S];
     bool salive[S];
-    uint32_t sphase[S];
     bool sact[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -457,7 +472,6 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
         sblk[s] = 0;
         spart[s] = 0.0f;
         salive[s] = false;
-        sphase[s] = 0;
         sact[s] = false;
     }
 
@@ -554,10 +568,7 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     };
 
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-        sphase[s] = 0;
-        sact[s] = grab(s);
-    }
+    for (int s = 0; s < S; ++s) sact[s] = grab(s);
 
     // Accumulate the staged block of slot s into one partial sum per lane
     // (lane = row), dimension by dimension.
@@ -706,24 +717,28 @@ __global__ void __launch_bounds__(512, 1) scan_plain_kernel(const __grid_constan
     __syncthreads();
     uint64_t* dst = p.out + (static_cast<size_t>(qi) * p.nsplit + split) * KP;
     for (int i = threadIdx.x; i < KP; i += blockDim.x) dst[i] = ctop[i];
+    }  // queries of this CTA
 }
 
 // Final merge: per query, the k best of nparts sorted lists of kp keys, then
 // keys -> (distance, id).  Unfilled entries get the reference's heap_init
 // values (FLT_MAX / -FLT_MAX, id -1; src/heap.hpp:13-25).
-__global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__ parts, int nparts, int kp, int k,
+__global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__ parts, int nq, int nparts, int kp, int k,
                                                     int metric, const int64_t* __restrict__ ids,
                                                     float* __restrict__ D, int64_t* __restrict__ I,
                                                     int64_t* __restrict__ rows, const int32_t* __restrict__ nq_dev) {
     extern __shared__ __align__(16) unsigned char sm[];
     uint64_t* a = reinterpret_cast<uint64_t*>(sm);
-    const size_t qi = blockIdx.x;
-    if (nq_dev && static_cast<int>(qi) >= *nq_dev) return;
+    // Query blockIdx.x, then every gridDim.x-th after it, below the device
+    // count when one is given.
+    const int nq_eff = nq_dev ? min(*nq_dev, nq) : nq;
+    for (size_t qi = blockIdx.x; qi < static_cast<size_t>(nq_eff); qi += gridDim.x) {
     const int n = nparts * kp;
     const uint64_t* src = parts + qi * n;
     const uint64_t* best = src;
     if (nparts > 1) {
         const int P = next_pow2(n);
+        __syncthreads();  // the previous query's keys have been read
         for (int i = threadIdx.x; i < P; i += blockDim.x) a[i] = i < n ? src[i] : KEY_MAX;
         __syncthreads();
         cta_bitonic_sort(a, P);
@@ -745,6 +760,7 @@ __global__ void __launch_bounds__(256) merge_kernel(const uint64_t* __restrict__
         I[qi * k + i] = iv;
         if (rows) rows[qi * k + i] = key == KEY_MAX ? -1 : static_cast<int64_t>(key & 0xffffffffu);
     }
+    }  // queries of this CTA
 }
 
 // ---------------------------------------------------------------------------
@@ -988,7 +1004,10 @@ static cudaError_t launch_scan_t(const ScanParams& p, int W, int* smem_out, cuda
     cudaError_t e = cudaFuncSetAttribute(scan_plain_kernel<KR, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    scan_plain_kernel<KR, S><<<p.nq * p.nsplit, W * 32, smem, s>>>(p);
+    // With a device count and a query grid, the CTAs loop over the queries.
+    const int gq = (p.nq_dev && p.qgrid > 0) ? std::min(p.nq, p.qgrid) : p.nq;
+    if (gq < 1) return cudaSuccess;
+    scan_plain_kernel<KR, S><<<gq * p.nsplit, W * 32, smem, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -1018,7 +1037,10 @@ cudaError_t launch_merge(const uint64_t* parts, int nq, int nparts, int kp, int 
     const size_t smem = nparts > 1 ? static_cast<size_t>(next_pow2(nparts * kp)) * 8 : 0;
     cudaError_t e = cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return e;
-    merge_kernel<<<nq, 256, smem, s>>>(parts, nparts, kp, k, metric, ids, D, I, rows, nq_dev);
+    // With a device count the grid is capped and the CTAs loop over queries.
+    const int grid = nq_dev ? std::min(nq, 1024) : nq;
+    if (grid < 1) return cudaSuccess;
+    merge_kernel<<<grid, 256, smem, s>>>(parts, nq, nparts, kp, k, metric, ids, D, I, rows, nq_dev);
     return cudaGetLastError();
 }
 

@@ -50,6 +50,9 @@ struct ScanParams {
     int* err;
     int nq, nprobe, nsplit, k, metric, prune;
     const int32_t* nq_dev = nullptr;  // optional device count: queries at or past it are skipped
+    // With nq_dev: the launch has min(nq, qgrid) query slots (qgrid > 0) whose
+    // CTAs loop over the queries below the device count.
+    int qgrid = 0;
 };
 
 cudaError_t launch_coarse_scores(const float* q, int nq, const float* cent, int nlist, int d, int metric, float* out,

@@ -14,7 +14,9 @@
 // contents; the entry point clears what must start at zero (status word,
 // counters, per-query thresholds) at the start of each call.  Calls whose GPU
 // work overlaps (two host threads, or two streams) race on the array and must
-// be serialised by the caller.
+// be serialised by the caller.  A call holds the index's call lock from its
+// first read of the index until its work has completed on the device, so
+// add / load / reset on the same index from another thread wait for it.
 #include <mutex>
 
 #include "../../include/hy.h"
@@ -34,6 +36,7 @@ struct IndexView {
 };
 int index_view(const hy_index* h, IndexView* v);
 int set_error(int code, const char* msg);
+std::mutex& index_mutex(hy_index* h);
 }  // namespace hy
 
 namespace {
@@ -89,6 +92,9 @@ extern "C" int hy_index_search_preassigned_noalloc(hy_index* h, size_t n, const 
     if (n == 0) return HY_OK;
     if (k < 1 || k > HY_MAX_K) return hy::set_error(HY_ERR_ARG, "search_preassigned_noalloc: k must be in [1, 256]");
     if (nprobe < 1) return hy::set_error(HY_ERR_ARG, "search_preassigned_noalloc: nprobe must be >= 1");
+    // Held until the final synchronisation: the scan and merge read the
+    // index's arena, list tables and ids, which add / load / reset replace.
+    std::lock_guard<std::mutex> index_lock(hy::index_mutex(h));
     hy::IndexView v;
     int rc = hy::index_view(h, &v);
     if (rc != HY_OK) return rc;

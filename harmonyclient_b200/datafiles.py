@@ -88,12 +88,39 @@ def load_bvecs(path, bounds=(1, 0), bvecs_records=False):
         bmax, start = (size - 4) // rec, 8
     a, b = _bounds(bounds[0], bounds[1], bmax)
     n = b - a + 1
-    out = np.empty((n, d), np.uint8)
-    raw = np.fromfile(path, np.uint8)
-    for i in range(n):
-        o = start + (a - 1 + i) * rec
-        out[i] = raw[o:o + d]
-    return out
+    # Only the bytes of rows a..b are read: record i's d bytes sit at
+    # start + i*rec, so rows a..b span n records from start + (a-1)*rec (the
+    # last record's trailing 4 bytes may lie past the end of the file).
+    off = start + (a - 1) * rec
+    want = n * rec
+    raw = np.fromfile(path, np.uint8, count=min(want, size - off), offset=off)
+    if raw.size < want:
+        raw = np.concatenate([raw, np.zeros(want - raw.size, np.uint8)])
+    return raw.reshape(n, rec)[:, :d].copy()
+
+
+def bvecs_is_records(path):
+    """True when a .bvecs file holds plain ``[int32 d][d uint8]`` records
+    (size a multiple of 4 + d, the layout of the public BIGANN files), False
+    when it has the reference loader's extra 4-byte header (size - 4 a
+    multiple of 4 + d).  Raises ValueError when it is neither."""
+    d = _first_int(path)
+    size = os.path.getsize(path)
+    if d <= 0:
+        raise ValueError(f"{path}: first int32 {d} is not a dimension")
+    if size % (4 + d) == 0:
+        return True
+    if (size - 4) % (4 + d) == 0:
+        return False
+    raise ValueError(f"{path}: size {size} fits neither [int32 d][d bytes] records nor the reference's "
+                     f"4-byte header before them (d = {d})")
+
+
+def bvecs_rows(path, bvecs_records):
+    """Rows in a .bvecs file of the given layout."""
+    d = _first_int(path)
+    size = os.path.getsize(path)
+    return size // (4 + d) if bvecs_records else (size - 4) // (4 + d)
 
 
 def load_tvecs(path, bounds=(1, 0)):
@@ -110,15 +137,15 @@ def load_tvecs(path, bounds=(1, 0)):
     return np.array([r[:d] for r in rows[a - 1:b]], np.float32).reshape(b - a + 1, d)
 
 
-def load_xvecs(path, bounds=(1, 0)):
+def load_xvecs(path, bounds=(1, 0), bvecs_records=False):
     """float32 rows of .fvecs, .bvecs (converted) or .txt (every row: the
     reference's loadXvecs passes no bounds to the text loader)
-    (src/utils.h:388-399)."""
+    (src/utils.h:388-399).  bvecs_records as in load_bvecs."""
     path = str(path)
     if path.endswith(".fvecs"):
         return load_fvecs(path, bounds)
     if path.endswith(".bvecs"):
-        return load_bvecs(path, bounds).astype(np.float32)
+        return load_bvecs(path, bounds, bvecs_records).astype(np.float32)
     if path.endswith(".txt"):
         return load_tvecs(path)
     raise ValueError("no support file")

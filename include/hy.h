@@ -91,7 +91,8 @@ typedef struct {
     double scan_ms;           /* device time of the list scan */
     double merge_ms;          /* device time of the top-k merge */
     uint64_t launches;        /* kernels this library launched for the call */
-    uint64_t fallback_queries; /* bf16 form: queries answered again by the plain scan */
+    uint64_t fallback_queries; /* bf16 / e4m3 forms: queries whose candidates overflowed, every one
+                                  answered again exactly by the plain scan on the device */
     double mean_nprobe;       /* lists probed per query (learned: the predicted mean) */
     double judge_recall;      /* learned: recall@10 of the judged sample vs fixed nprobe (-1: not judged) */
     uint64_t learned_fallback; /* learned: 1 when the batch was searched again with fixed nprobe */
@@ -99,9 +100,6 @@ typedef struct {
                                  bf16: batched_scan_kernel, both passes) in the last query chunk */
     uint64_t kernel_launches; /* launches kernel_ms covers */
     uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
-    uint64_t unresolved_queries; /* bf16 device-pointer search: overflowed queries beyond the device
-                                    fallback's capacity (296 per chunk), left with the bf16 re-rank's
-                                    answer; the host-pointer search re-runs such batches exactly */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -142,8 +140,7 @@ HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
  * queries per list on the tensor cores and re-ranks candidates with exact FP32
  * distances chosen by rigorous error bounds, so its results equal the plain
  * form's.  Queries whose candidates overflow their buffers are answered again
- * by the plain scan on the device (up to 296 per chunk of queries; the
- * host-pointer search re-runs a batch with more in the plain form). */
+ * by the plain scan on the device, however many overflow. */
 HY_API int hy_index_set_form(hy_index* h, int form);
 
 /* bf16 form parameters (0 keeps the current value): candidate slots per
@@ -273,7 +270,9 @@ HY_API int hy_file_inspect(const char* path, size_t* d, size_t* nlist, int* metr
  * on `stream` and waits for it; its first call on a device looks up the
  * array's device address, so make that call before any stream capture.  The
  * array is shared by every call on a device: calls whose GPU work overlaps
- * race and must be serialised by the caller. */
+ * race and must be serialised by the caller.  The call holds the index's lock
+ * until its work has completed, like the other entry points, so an add, load
+ * or reset of the same index from another thread waits for it. */
 HY_API int hy_index_search_preassigned_noalloc(hy_index* h, size_t n, const float* dq, size_t k, size_t nprobe,
                                                const int64_t* dprobes, float* dD, int64_t* dI, void* stream);
 

@@ -95,3 +95,33 @@ def test_bench_reads_vector_files(tmp_path):
     xb, qb = bench.file_workload(str(tmp_path / "b.fvecs"), str(tmp_path / "q.bvecs"), 7, 0)
     np.testing.assert_array_equal(xb, x[:7])
     np.testing.assert_array_equal(qb, q)
+
+
+def test_bench_reads_plain_record_bvecs(tmp_path):
+    """A .bvecs file without the reference loader's extra header (the public
+    BIGANN layout) is told apart by its size and read whole and in bounds."""
+    import bench
+
+    x = np.arange(60, dtype=np.float32).reshape(10, 6)
+    q = (np.arange(18, dtype=np.float32).reshape(3, 6) * 7) % 251
+    io.write_fvecs(str(tmp_path / "b.fvecs"), x)
+    qp = str(tmp_path / "q.bvecs")
+    io.write_bvecs(qp, q.astype(np.uint8), bvecs_records=True)
+    assert io.bvecs_is_records(qp)
+    assert bench._file_info(qp) == (3, 6)
+    xb, qb = bench.file_workload(str(tmp_path / "b.fvecs"), qp, 0, 2)
+    np.testing.assert_array_equal(qb, q[:2])
+    np.testing.assert_array_equal(xb, x)
+    rp = str(tmp_path / "r.bvecs")
+    io.write_bvecs(rp, q.astype(np.uint8))
+    assert not io.bvecs_is_records(rp)
+    assert bench._file_info(rp) == (3, 6)
+
+
+def test_bvecs_bounded_read_matches_whole_read(tmp_path):
+    x = (np.arange(7 * 12) % 256).astype(np.uint8).reshape(7, 12)
+    for records in (False, True):
+        p = str(tmp_path / f"x{int(records)}.bvecs")
+        io.write_bvecs(p, x, bvecs_records=records)
+        np.testing.assert_array_equal(io.load_bvecs(p, (3, 7), records), x[2:7])
+        np.testing.assert_array_equal(io.load_bvecs(p, (1, 1), records), x[:1])

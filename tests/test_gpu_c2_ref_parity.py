@@ -1,0 +1,76 @@
+"""Parity with the reference itself on a C2-shaped index: 200,000 x 128
+integer-valued vectors in [0,255] from a 4,096-component mixture (sigma 20),
+nlist 1024, k 100, 1,000 queries, nprobe 16, 64 and 256.
+
+The reference's own Index::add and Index::search (ORIGINAL mode, compiled
+from its sources into oracle/_ref) run live on the host cores with the
+centroids the GPU trained, and the GPU's plain and bf16 forms must return
+the same answers: on this integer data every distance is exact in FP32
+(128 * 255^2 < 2^24), so distances must be bit-equal (rtol 0) and ids equal
+apart from ties at the k-th distance (tests/topk_check.py).  Queries whose
+nprobe-th and (nprobe+1)-th centroid distances are tied within 1e-5 in FP64
+may legitimately probe different lists and are left out; they must be rare.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import harmonyclient_b200 as hb
+from harmonyclient_b200 import datasets
+from oracle import ref
+from tests.topk_check import assert_topk_equal, probe_tied_rows
+
+pytestmark = pytest.mark.gpu
+
+NB, NQ, NLIST, K = 200_000, 1_000, 1024, 100
+
+
+@pytest.fixture(scope="module")
+def c2_shape():
+    assert ref.available(), "oracle/_ref (the reference built from its sources) is missing"
+    x, q = datasets.gmm_uint8(NB, NQ, seed=3)
+    idx = hb.Index(128, NLIST, 64)
+    idx.train(x)
+    idx.add(x)
+    cent = idx.centroid_codes
+    ref.set_threads(os.cpu_count() or 1)
+    R = ref.RefIndex(128, NLIST, 64)
+    R.set_centroids(cent)
+    R.add(x)
+    return {"idx": idx, "R": R, "x": x, "q": q, "cent": cent, "ref": {}}
+
+
+def _reference(c, nprobe):
+    if nprobe not in c["ref"]:
+        c["R"].set_nprobe(nprobe)
+        c["ref"][nprobe] = c["R"].search(c["q"], K)
+    return c["ref"][nprobe]
+
+
+def test_lists_equal_the_references(c2_shape):
+    c = c2_shape
+    for l in range(0, NLIST, 37):
+        ids, _, _ = c["idx"].get_list(l)
+        rids, _, _ = c["R"].get_list(l)
+        assert sorted(ids.tolist()) == sorted(rids.tolist())
+
+
+@pytest.mark.parametrize("nprobe", [16, 64, 256])
+@pytest.mark.parametrize("form", ["plain", "bf16"])
+def test_c2_shape_equals_reference(c2_shape, form, nprobe):
+    c = c2_shape
+    Dr, Ir = _reference(c, nprobe)
+    idx = c["idx"]
+    idx.nprobe = nprobe
+    idx.set_form(form)
+    try:
+        D, I = idx.search(c["q"], K)
+        st = idx.last_stats()
+    finally:
+        idx.set_form("plain")
+        idx.nprobe = 64
+    tied = probe_tied_rows(c["q"], c["cent"], np.zeros((1, nprobe)), 1)
+    assert len(tied) <= NQ // 50, f"{len(tied)} probe-tied queries"
+    assert_topk_equal(Dr, Ir, D, I, rtol=0.0, skip_rows=tied)
+    assert st["nq"] == NQ

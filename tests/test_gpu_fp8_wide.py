@@ -92,7 +92,6 @@ def test_fp8_oversampled_recall_on_420d(wide):
     # every returned distance is the exact FP32 distance of its row
     same = I == Ip
     np.testing.assert_array_equal(D[same], Dp[same])
-    assert st["unresolved_queries"] == 0
 
 
 @pytest.mark.parametrize("d", [200, 420])

@@ -3,9 +3,8 @@
 * search_nprobes (host and device pointers) returns what a preassigned search
   over each query's first nprobes[i] lists returns, in both forms.
 * Queries whose bf16 candidate buffers overflow are answered again by the
-  plain scan on the device (device-pointer search included); a batch with
-  more overflowing queries than the device fallback holds per chunk is
-  searched again in the plain form by the host-pointer search.
+  plain scan on the device (device-pointer search included), however many
+  of a batch's queries overflow.
 """
 import numpy as np
 import pytest
@@ -99,24 +98,36 @@ def test_device_fallback_answers_overflowed_queries_exactly(skewed):
     finally:
         idx.set_batch_params(capq=8192)
         idx.set_form("plain")
-    assert st["fallback_queries"] > 0 and st["unresolved_queries"] == 0
+    assert st["fallback_queries"] > 0
     np.testing.assert_array_equal(dI.cpu().numpy(), Ip)
     np.testing.assert_array_equal(dD.cpu().numpy(), Dp)
 
 
-def test_host_search_reruns_batch_beyond_device_fallback(skewed):
-    """More overflowing queries than the device fallback holds: the host
-    search re-runs the batch in the plain form and reports it."""
+def test_device_fallback_has_no_cap(skewed):
+    """All 1,000 queries overflow capq 256 (far more than one wave of the
+    fallback's query slots, 148): the device-pointer search answers every
+    one exactly with the plain scan on the device, and so does the
+    host-pointer search."""
     idx, x, q = skewed
     Dp, Ip = idx.search(q, 100)
     idx.set_form("bf16")
     idx.set_batch_params(capq=256)
     try:
+        dq = torch.from_numpy(q).cuda()
+        dD = torch.empty((q.shape[0], 100), dtype=torch.float32, device="cuda")
+        dI = torch.empty((q.shape[0], 100), dtype=torch.int64, device="cuda")
+        idx.search_device(q.shape[0], dq.data_ptr(), 100, dD.data_ptr(), dI.data_ptr(),
+                          torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        st_dev = idx.last_stats()
         D, I = idx.search(q, 100)
         st = idx.last_stats()
     finally:
         idx.set_batch_params(capq=8192)
         idx.set_form("plain")
-    assert st["fallback_queries"] == q.shape[0]
+    assert st_dev["fallback_queries"] > 296
+    assert st["fallback_queries"] == st_dev["fallback_queries"]
+    np.testing.assert_array_equal(dI.cpu().numpy(), Ip)
+    np.testing.assert_array_equal(dD.cpu().numpy(), Dp)
     np.testing.assert_array_equal(I, Ip)
     np.testing.assert_array_equal(D, Dp)
