@@ -14,6 +14,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "hy.h")
 HY_OK, HY_ERR_ARG, HY_ERR_OOM, HY_ERR_CUDA, HY_ERR_TIMEOUT, HY_ERR_STATE, HY_ERR_IO, HY_ERR_UNSUPPORTED = range(8)
 HY_FORM_PLAIN, HY_FORM_BF16, HY_FORM_FP8 = 0, 1, 2
 HY_COARSE_EXACT, HY_COARSE_TENSOR = 0, 1
+HY_PLAIN_AUTO, HY_PLAIN_QUERY_MAJOR, HY_PLAIN_LIST_MAJOR = 0, 1, 2
 HY_MAX_K = 256
 
 
@@ -35,7 +36,8 @@ class SearchStats(C.Structure):
                 ("tile_blocks_max", C.c_uint64), ("coarse_ms", C.c_double), ("scan_ms", C.c_double),
                 ("merge_ms", C.c_double), ("launches", C.c_uint64), ("fallback_queries", C.c_uint64),
                 ("mean_nprobe", C.c_double), ("judge_recall", C.c_double), ("learned_fallback", C.c_uint64),
-                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("graph_replayed", C.c_uint64)]
+                ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("graph_replayed", C.c_uint64),
+                ("block_sums", C.c_uint64), ("list_major", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -74,6 +76,7 @@ def load():
     L.hy_index_set_nprobe.argtypes = [H, sz]
     L.hy_index_presearch.argtypes = [H, sz, sz]
     L.hy_index_set_form.argtypes = [H, i]
+    L.hy_index_set_plain_scan.argtypes = [H, i]
     L.hy_index_set_batch_params.argtypes = [H, sz, sz, sz]
     L.hy_index_set_coarse.argtypes = [H, i]
     L.hy_index_search.argtypes = [H, sz, vp, sz, vp, vp]

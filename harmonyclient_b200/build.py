@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhy.so")
-SOURCES = ["hy_kernels.cu", "hy_batched.cu", "hy_capi.cu", "hy_selftest.cu", "hy_noalloc.cu", "hy_mlp.cu"]
-HEADERS = ["hy_device.cuh", "hy_kernels.cuh", "hy_tc.cuh", "hy_common.cuh", "hy_batched.cuh", "hy_mlp.cuh"]
+SOURCES = ["hy_kernels.cu", "hy_batched.cu", "hy_capi.cu", "hy_selftest.cu", "hy_noalloc.cu", "hy_mlp.cu", "hy_lists.cu"]
+HEADERS = ["hy_device.cuh", "hy_kernels.cuh", "hy_tc.cuh", "hy_common.cuh", "hy_batched.cuh", "hy_mlp.cuh", "hy_lists.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

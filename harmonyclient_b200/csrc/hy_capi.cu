@@ -20,6 +20,7 @@
 
 #include "../../include/hy.h"
 #include "hy_batched.cuh"
+#include "hy_lists.cuh"
 #include "hy_kernels.cuh"
 #include "hy_mlp.cuh"
 
@@ -116,7 +117,7 @@ ArenaLayout make_layout(int d, int nb) {
 // Device status of a host-pointer call, read back in one pinned block.
 struct HostStatus {
     int err = 0;
-    unsigned long long counters[2] = {0, 0};  // scan tile-block counters
+    unsigned long long counters[3] = {0, 0, 0};  // scan counters (block copies, blocks unpruned, block sums)
     unsigned long long learned_total = 0;     // sum of the learned nprobes
     unsigned long long fallback = 0;  // queries answered by the device fallback
 };
@@ -185,6 +186,9 @@ struct hy_index {
     hy_search_stats_t stats = {};
     uint64_t launches = 0;  // kernels launched since the last stats snapshot
 
+    // plain form: query-major or list-major scan (hy_index_set_plain_scan)
+    int plain_scan = HY_PLAIN_AUTO;
+    bool lm_last = false;  // the last plain search ran the list-major scan
     // batched tensor-core forms (bf16, e4m3)
     int form = HY_FORM_PLAIN;
     size_t capq = 8192;       // candidate slots per query
@@ -514,8 +518,127 @@ int scan_and_merge(hy_index* h, size_t n, const float* dq, size_t k, size_t npro
     return HY_OK;
 }
 
+// Rows per work item of the list-major scan (32 tiles: four per warp).
+constexpr int LM_ROW_SLICE = 1024;
+
+// Whether a plain search of m queries (per chunk) at nprobe runs the
+// list-major scan.
+bool use_list_major(const hy_index* h, size_t m, size_t nprobe) {
+    if (h->plain_scan == HY_PLAIN_QUERY_MAJOR || h->arena_rows == 0 || !hy::list_scan_fits(h->L)) return false;
+    if (h->plain_scan == HY_PLAIN_LIST_MAJOR) return true;
+    return m * nprobe >= 4 * h->nlist;
+}
+
+// The list-major plain scan of m device queries whose probe lists (m x
+// nprobe, -1 = skip) and ordered-key thresholds (thr: warm-up values or
+// 0xffffffff; lowered in place) are on the device, into D / I: first pass
+// over each query's nearest list, the k best keys kept and the threshold
+// lowered to the k-th, second pass over the other probed lists, final
+// top-k; queries whose candidates overflowed are searched again by the
+// query-major scan.  Runs on stream s.
+int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, const int64_t* probes, uint32_t* thr,
+               float* dD, int64_t* dI, cudaStream_t s, bool timed) {
+    if (h->nsm == 0) HY_CUDA(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const size_t nlist = h->nlist;
+    const size_t capq = h->capq;
+    const int rs = LM_ROW_SLICE;
+    HY_RET(h->b_pcnt.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_pfill.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_poff.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_RET(h->b_pairs.ensure(m * nprobe * sizeof(int32_t)));
+    HY_RET(h->b_icnt.ensure(nlist * sizeof(int32_t)));
+    HY_RET(h->b_ioff.ensure((nlist + 1) * sizeof(int64_t)));
+    HY_RET(h->b_work.ensure(sizeof(unsigned int)));
+    HY_RET(h->b_cand.ensure(m * capq * sizeof(uint64_t)));
+    HY_RET(h->b_ccnt.ensure(m * sizeof(int32_t)));
+    HY_RET(h->b_ovf.ensure((m + 1) * sizeof(int32_t)));
+    size_t max_slices = 1;
+    for (size_t l = 0; l < nlist; ++l)
+        max_slices = std::max(max_slices, ((size_t)h->h_list_size[l] + rs - 1) / rs);
+    const size_t item_cap = std::min<size_t>((m * nprobe / hy::LM_GROUP + nlist) * max_slices, size_t(4) << 20);
+    HY_RET(h->b_items.ensure(item_cap * sizeof(int4)));
+    HY_RET(h->b_fq.ensure(m * h->d * sizeof(float)));
+    HY_RET(h->b_fpr.ensure(m * nprobe * sizeof(int64_t)));
+    HY_RET(h->b_fD.ensure(m * k * sizeof(float)));
+    HY_RET(h->b_fI.ensure(m * k * sizeof(int64_t)));
+    HY_RET(h->b_fcnt.ensure(sizeof(int32_t)));
+    HY_RET(h->b_fbtot.ensure(sizeof(unsigned long long)));
+    hy::BatchWork w{};
+    w.items = h->b_items.as<int4>();
+    w.item_cap = (int64_t)item_cap;
+    w.pair_cnt = h->b_pcnt.as<int32_t>();
+    w.pair_fill = h->b_pfill.as<int32_t>();
+    w.pair_off = h->b_poff.as<int64_t>();
+    w.pairs = h->b_pairs.as<int32_t>();
+    w.item_cnt = h->b_icnt.as<int32_t>();
+    w.item_off = h->b_ioff.as<int64_t>();
+    w.work = h->b_work.as<unsigned int>();
+    int32_t* ovf = h->b_ovf.as<int32_t>();
+    HY_CUDA(cudaMemsetAsync(h->b_ccnt.p, 0, m * sizeof(int32_t), s));
+    HY_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
+    hy::ListScanParams p;
+    p.L = h->L;
+    p.codes = h->codes.as<float>();
+    p.list_off = h->list_off.as<int64_t>();
+    p.list_size = h->list_size.as<int32_t>();
+    p.q = qq;
+    p.item_off = w.item_off;
+    p.items = w.items;
+    p.item_cap = w.item_cap;
+    p.pair_off = w.pair_off;
+    p.pairs = w.pairs;
+    p.pair_cnt = w.pair_cnt;
+    p.thr = thr;
+    p.cand = h->b_cand.as<uint64_t>();
+    p.cand_cnt = h->b_ccnt.as<int32_t>();
+    p.work = w.work;
+    p.counters = h->w_counters.as<unsigned long long>();
+    p.err = h->w_err.as<int>();
+    p.nlist = (int)nlist;
+    p.rs = rs;
+    p.capq = (int)capq;
+    p.metric = h->metric;
+    p.prune = 1;
+    if (timed) HY_CUDA(ev_record(h->ev[2], s));
+    // Pass 1: each query's nearest list.
+    HY_CUDA(hy::launch_invert_probes(probes, (int)m, (int)nprobe, 0, 1, (int)nlist, h->list_size.as<int32_t>(), rs,
+                                     hy::LM_GROUP, w, s));
+    HY_CUDA(cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s));
+    if (timed) HY_CUDA(ev_record(h->ev[6], s));
+    HY_CUDA(hy::launch_list_scan(p, h->nsm, s));
+    if (timed) HY_CUDA(ev_record(h->ev[7], s));
+    if (timed) h->kev = 1;
+    HY_CUDA(hy::launch_list_topk(p.cand, p.cand_cnt, (int)m, (int)capq, (int)k, h->metric, 0, thr, nullptr, nullptr,
+                                 nullptr, nullptr, s));
+    h->launches += 8;
+    if (nprobe > 1) {
+        // Pass 2: the other probed lists under the lowered thresholds.
+        HY_CUDA(hy::launch_invert_probes(probes, (int)m, (int)nprobe, 1, (int)nprobe, (int)nlist,
+                                         h->list_size.as<int32_t>(), rs, hy::LM_GROUP, w, s));
+        HY_CUDA(cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s));
+        if (timed) HY_CUDA(ev_record(h->ev[8], s));
+        HY_CUDA(hy::launch_list_scan(p, h->nsm, s));
+        if (timed) HY_CUDA(ev_record(h->ev[9], s));
+        if (timed) h->kev = 2;
+        h->launches += 7;
+    }
+    if (timed) HY_CUDA(ev_record(h->ev[3], s));
+    HY_CUDA(hy::launch_list_topk(p.cand, p.cand_cnt, (int)m, (int)capq, (int)k, h->metric, 1, thr,
+                                 h->ids.as<int64_t>(), dD, dI, ovf, s));
+    // Overflowed queries: the query-major scan over the same probe lists.
+    HY_CUDA(hy::launch_fb_gather(ovf, qq, probes, (int)nprobe, (int)h->d, (int)m, h->b_fq.as<float>(),
+                                 h->b_fpr.as<int64_t>(), h->b_fcnt.as<int32_t>(), s));
+    HY_RET(scan_and_merge(h, m, h->b_fq.as<float>(), k, nprobe, h->b_fpr.as<int64_t>(), nullptr, h->b_fD.as<float>(),
+                          h->b_fI.as<int64_t>(), s, false, nullptr, h->b_fcnt.as<int32_t>()));
+    HY_CUDA(hy::launch_fb_scatter(ovf, h->b_fD.as<float>(), h->b_fI.as<int64_t>(), (int)k, (int)m, dD, dI,
+                                  h->b_fbtot.as<unsigned long long>(), s));
+    if (timed) HY_CUDA(ev_record(h->ev[4], s));
+    h->launches += 3;
+    return HY_OK;
+}
+
 int ensure_common(hy_index* h) {
-    HY_RET(h->w_counters.ensure(2 * sizeof(unsigned long long)));
+    HY_RET(h->w_counters.ensure(3 * sizeof(unsigned long long)));
     HY_RET(h->w_err.ensure(sizeof(int)));
     return HY_OK;
 }
@@ -547,17 +670,30 @@ int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, i
 // merge, in query chunks.
 int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
                        bool timed) {
+    HY_RET(ensure_common(h));
+    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 3 * sizeof(unsigned long long), s));
+    h->lm_last = false;
+    h->stats.list_major = 0;
     if (batched_form(h) && h->arena_rows > 0) return search_bf16_impl(h, n, dq, k, dD, dI, s, timed);
     const size_t nprobe = std::min(h->nprobe, h->nlist);
     HY_CHECK(nprobe >= 1, HY_ERR_ARG, "search: nprobe must be >= 1");
     HY_CHECK(h->nlist <= 40000, HY_ERR_ARG, "search: nlist above 40000 is not supported by the coarse selector");
     HY_RET(ensure_common(h));
-    const size_t qc = query_chunk(h->nlist, n);
+    size_t qc = query_chunk(h->nlist, n);
+    // List-major scan: chunks sized so the candidate buffers stay within 2 GiB.
+    const bool lm = use_list_major(h, qc, nprobe);
+    if (lm) qc = std::min(qc, std::max<size_t>(1, (size_t(2) << 30) / (h->capq * 8)));
+    h->lm_last = lm;
+    h->stats.list_major = lm ? 1 : 0;
     HY_RET(h->w_scores.ensure(qc * h->nlist * sizeof(float)));
     HY_RET(h->w_probes.ensure(qc * nprobe * sizeof(int64_t)));
     if (learned_on(h)) HY_RET(h->m_pscore.ensure(qc * nprobe * sizeof(float)));
     const bool warm = h->warmup_list > 0 && h->metric == HY_METRIC_L2;
-    if (warm) HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
+    if (warm || lm) HY_RET(h->w_thr.ensure(qc * sizeof(uint32_t)));
+    if (lm) {
+        HY_RET(h->b_fbtot.ensure(sizeof(unsigned long long)));
+        HY_CUDA(cudaMemsetAsync(h->b_fbtot.p, 0, sizeof(unsigned long long), s));
+    }
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
@@ -584,8 +720,14 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
             thr = h->w_thr.as<uint32_t>();
         }
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[1], s));
-        HY_RET(scan_and_merge(h, m, qq, k, nprobe, h->w_probes.as<int64_t>(), thr, dD + q0 * k, dI + q0 * k, s,
-                              timed && q0 + qc >= n));
+        if (lm) {
+            if (!warm) HY_CUDA(cudaMemsetAsync(h->w_thr.p, 0xff, m * sizeof(uint32_t), s));
+            HY_RET(scan_lists(h, m, qq, k, nprobe, h->w_probes.as<int64_t>(), h->w_thr.as<uint32_t>(), dD + q0 * k,
+                              dI + q0 * k, s, timed && q0 + qc >= n));
+        } else {
+            HY_RET(scan_and_merge(h, m, qq, k, nprobe, h->w_probes.as<int64_t>(), thr, dD + q0 * k, dI + q0 * k, s,
+                                  timed && q0 + qc >= n));
+        }
     }
     return HY_OK;
 }
@@ -991,6 +1133,7 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
     h->stats.pairs = n * nprobe;
     h->stats.tile_blocks = st->counters[0];
     h->stats.tile_blocks_max = st->counters[1];
+    h->stats.block_sums = st->counters[2];
     h->stats.launches = h->launches;
     h->launches = 0;
     if (timed) collect_times(h);
@@ -1003,7 +1146,7 @@ int reset_counters(hy_index* h, cudaStream_t s) {
     h->launches = 0;
     HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
     HY_CUDA(cudaMemsetAsync(h->m_total.p, 0, sizeof(unsigned long long), s));
-    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 2 * sizeof(unsigned long long), s));
+    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 3 * sizeof(unsigned long long), s));
     return HY_OK;
 }
 
@@ -1251,6 +1394,16 @@ int hy_index_set_form(hy_index* h, int form) {
     return HY_OK;
 }
 
+int hy_index_set_plain_scan(hy_index* h, int mode) {
+    HY_CHECK(h, HY_ERR_ARG, "set_plain_scan: NULL handle");
+    HY_CHECK(mode == HY_PLAIN_AUTO || mode == HY_PLAIN_QUERY_MAJOR || mode == HY_PLAIN_LIST_MAJOR, HY_ERR_ARG,
+             "set_plain_scan: unknown mode");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->epoch++;  // a captured search graph no longer matches
+    h->plain_scan = mode;
+    return HY_OK;
+}
+
 int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice) {
     HY_CHECK(h, HY_ERR_ARG, "set_batch_params: NULL handle");
     h->epoch++;  // a captured search graph no longer matches
@@ -1449,7 +1602,7 @@ int search_host(hy_index* h, size_t n, const float* q, size_t k, float* D, int64
     h->stats.fallback_queries = 0;
     h->stats.mean_nprobe = (double)std::min(h->nprobe, h->nlist);
     if (learned_on(h)) h->stats.mean_nprobe = (double)h->hstat->learned_total / (double)n;
-    if (batched_form(h) && h->arena_rows > 0) HY_RET(bf16_fallback(h));
+    if ((batched_form(h) || h->lm_last) && h->arena_rows > 0) HY_RET(bf16_fallback(h));
     return HY_OK;
 }
 
@@ -1926,10 +2079,17 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
         HY_RET(set_device(h));
         HY_CUDA(cudaEventSynchronize(h->ev[4]));
         collect_times(h);
-        if (batched_form(h) && h->b_fbtot.p) {
+        if ((batched_form(h) || h->lm_last) && h->b_fbtot.p) {
             unsigned long long c = 0;
             HY_CUDA(cudaMemcpy(&c, h->b_fbtot.p, sizeof(c), cudaMemcpyDeviceToHost));
             h->stats.fallback_queries = c;
+        }
+        if (h->w_counters.p) {
+            unsigned long long c[3] = {0, 0, 0};
+            HY_CUDA(cudaMemcpy(c, h->w_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+            h->stats.tile_blocks = c[0];
+            h->stats.tile_blocks_max = c[1];
+            h->stats.block_sums = c[2];
         }
     }
     *out = h->stats;

@@ -126,6 +126,15 @@ class Index:
         f = {"plain": _lib.HY_FORM_PLAIN, "bf16": _lib.HY_FORM_BF16, "fp8": _lib.HY_FORM_FP8}.get(form, form)
         check(self._L.hy_index_set_form(self._h, int(f)))
 
+    def set_plain_scan(self, mode):
+        """The plain form's scan: 'auto' (default: list-major when the batch
+        has at least 4 queries per list on average), 'query' (one CTA per
+        query streams its probed lists) or 'list' (queries probing a list
+        share one pass over it).  All give the same answer."""
+        m = {"auto": _lib.HY_PLAIN_AUTO, "query": _lib.HY_PLAIN_QUERY_MAJOR,
+             "list": _lib.HY_PLAIN_LIST_MAJOR}.get(mode, mode)
+        check(self._L.hy_index_set_plain_scan(self._h, int(m)))
+
     def set_coarse(self, mode):
         """The bf16 form's coarse step: 'tensor' (default; bf16 tensor-core
         scores with error bounds, exact FP32 scores only for the centroids

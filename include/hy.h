@@ -55,6 +55,14 @@ enum {
     HY_FORM_FP8 = 2    /* the same on e4m3 codes with per-list / per-query scales, oversampled re-rank */
 };
 
+/* How the plain form scans (hy_index_set_plain_scan).  Both return the same
+ * answer, bit for bit. */
+enum {
+    HY_PLAIN_AUTO = 0,        /* list-major when the batch shares lists (>= 4 queries per list on average) */
+    HY_PLAIN_QUERY_MAJOR = 1, /* one CTA per (query, probe split) streams that query's probed lists */
+    HY_PLAIN_LIST_MAJOR = 2   /* queries probing a list share one pass over it, 32 per group */
+};
+
 /* Largest k the scan kernels keep per query. The reference's distributed
  * modes assume k <= 100 (presumeK, src/node.h:89). */
 #define HY_MAX_K 256
@@ -100,6 +108,8 @@ typedef struct {
                                  bf16: batched_scan_kernel, both passes) in the last query chunk */
     uint64_t kernel_launches; /* launches kernel_ms covers */
     uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
+    uint64_t block_sums;      /* list-major plain scan: (query, 32-row x one-dim-block) partial sums computed */
+    uint64_t list_major;      /* plain form: 1 when the search ran the list-major scan */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
@@ -142,6 +152,17 @@ HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
  * form's.  Queries whose candidates overflow their buffers are answered again
  * by the plain scan on the device, however many overflow. */
 HY_API int hy_index_set_form(hy_index* h, int form);
+
+/* Plain form's scan (no counterpart in the reference): HY_PLAIN_AUTO (default),
+ * HY_PLAIN_QUERY_MAJOR or HY_PLAIN_LIST_MAJOR.  The list-major scan inverts
+ * the (query, probed list) pairs into per-list groups of 32 queries; each
+ * group reads a list once, dimension block by dimension block, pruning each
+ * (row, query) pair against the query's threshold between blocks, with the
+ * query-major scan's arithmetic.  Its two passes (each query's nearest list
+ * under the warm-up threshold, then the other probed lists under the k-th
+ * distance found so far) keep up to the bf16 form's candidate slots per
+ * query; a query with more is answered again by the query-major scan. */
+HY_API int hy_index_set_plain_scan(hy_index* h, int mode);
 
 /* bf16 form parameters (0 keeps the current value): candidate slots per
  * query (default 8192, at most 12288; the first pass scans each query's
