@@ -117,7 +117,7 @@ ArenaLayout make_layout(int d, int nb) {
 // Device status of a host-pointer call, read back in one pinned block.
 struct HostStatus {
     int err = 0;
-    unsigned long long counters[3] = {0, 0, 0};  // scan counters (block copies, blocks unpruned, block sums)
+    unsigned long long counters[4] = {0, 0, 0, 0};  // scan counters (block copies, blocks unpruned, block sums, sums unpruned)
     unsigned long long learned_total = 0;     // sum of the learned nprobes
     unsigned long long fallback = 0;  // queries answered by the device fallback
 };
@@ -214,6 +214,10 @@ struct hy_index {
     // and the work of one launch
     int coarse_mode = HY_COARSE_TENSOR;
     bool cimg_valid = false;
+    // Inner product with OPT_TRIANGLE: per arena row its inner product with
+    // its list's centroid and per 32-row tile {max, min} (built on first use).
+    DevBuf c2c, c2c_tile;
+    bool c2c_valid = false;
     DevBuf c_img, c_aux, c_taux, c_norm, c_off, c_size;
     DevBuf c_pcnt, c_poff, c_pairs, c_ioff, c_items, c_work, c_cand, c_ccnt;
 
@@ -388,6 +392,7 @@ int build_arena(hy_index* h, const float* x, size_t n, const int32_t* order, con
     const size_t rows_alloc = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
     h->abf_valid = false;
     h->a8_valid = false;
+    h->c2c_valid = false;
     HY_RET(h->codes.ensure(rows_alloc * h->L.row_pitch * sizeof(float)));
     HY_RET(h->ids.ensure(rows_alloc * sizeof(int64_t)));
     HY_RET(h->norms.ensure(rows_alloc * sizeof(float)));
@@ -599,6 +604,23 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
     p.capq = (int)capq;
     p.metric = h->metric;
     p.prune = 1;
+    if (h->metric == HY_METRIC_IP && (h->opt_level & 1)) {
+        // OPT_TRIANGLE (inner product): the cos-bound window of each
+        // (query, list), from each row's inner product with its centroid.
+        if (!h->c2c_valid) {
+            const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
+            HY_RET(h->c2c.ensure(rows * sizeof(float)));
+            HY_RET(h->c2c_tile.ensure(rows / 32 * sizeof(float2)));
+            HY_CUDA(hy::launch_row_centroid_ip(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(),
+                                               h->list_size.as<int32_t>(), (int)nlist, (int64_t)h->arena_rows,
+                                               h->cent.as<float>(), h->c2c.as<float>(), h->c2c_tile.as<float2>(), s));
+            h->c2c_valid = true;
+        }
+        p.triangle = 1;
+        p.c2c = h->c2c.as<float>();
+        p.c2c_tile = h->c2c_tile.as<float2>();
+        p.cent = h->cent.as<float>();
+    }
     if (timed) HY_CUDA(ev_record(h->ev[2], s));
     // Pass 1: each query's nearest list.
     HY_CUDA(hy::launch_invert_probes(probes, (int)m, (int)nprobe, 0, 1, (int)nlist, h->list_size.as<int32_t>(), rs,
@@ -638,7 +660,7 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
 }
 
 int ensure_common(hy_index* h) {
-    HY_RET(h->w_counters.ensure(3 * sizeof(unsigned long long)));
+    HY_RET(h->w_counters.ensure(4 * sizeof(unsigned long long)));
     HY_RET(h->w_err.ensure(sizeof(int)));
     return HY_OK;
 }
@@ -671,7 +693,7 @@ int apply_learned_probes(hy_index* h, size_t m, size_t nprobe, cudaStream_t s, i
 int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD, int64_t* dI, cudaStream_t s,
                        bool timed) {
     HY_RET(ensure_common(h));
-    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 3 * sizeof(unsigned long long), s));
+    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 4 * sizeof(unsigned long long), s));
     h->lm_last = false;
     h->stats.list_major = 0;
     if (batched_form(h) && h->arena_rows > 0) return search_bf16_impl(h, n, dq, k, dD, dI, s, timed);
@@ -1134,6 +1156,7 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
     h->stats.tile_blocks = st->counters[0];
     h->stats.tile_blocks_max = st->counters[1];
     h->stats.block_sums = st->counters[2];
+    h->stats.block_sums_max = st->counters[3];
     h->stats.launches = h->launches;
     h->launches = 0;
     if (timed) collect_times(h);
@@ -1146,7 +1169,7 @@ int reset_counters(hy_index* h, cudaStream_t s) {
     h->launches = 0;
     HY_RET(h->m_total.ensure(sizeof(unsigned long long)));
     HY_CUDA(cudaMemsetAsync(h->m_total.p, 0, sizeof(unsigned long long), s));
-    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 3 * sizeof(unsigned long long), s));
+    HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 4 * sizeof(unsigned long long), s));
     return HY_OK;
 }
 
@@ -1349,6 +1372,7 @@ int hy_index_set_centroids(hy_index* h, const float* c) {
     HY_CUDA(cudaMemcpy(h->cent.p, c, bytes, cudaMemcpyHostToDevice));
     h->trained = true;
     h->cimg_valid = false;
+    h->c2c_valid = false;
     return HY_OK;
 }
 
@@ -1373,6 +1397,15 @@ int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream) {
     std::lock_guard<std::mutex> g(h->mu);
     HY_RET(set_device(h));
     return add_impl(h, n, dx, true, static_cast<cudaStream_t>(stream));
+}
+
+int hy_index_set_opt_level(hy_index* h, int opt_level) {
+    HY_CHECK(h, HY_ERR_ARG, "set_opt_level: NULL handle");
+    HY_CHECK(opt_level >= 0 && opt_level <= 7, HY_ERR_ARG, "set_opt_level: invalid opt_level");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->epoch++;  // a captured search graph no longer matches
+    h->opt_level = opt_level;
+    return HY_OK;
 }
 
 int hy_index_set_nprobe(hy_index* h, size_t nprobe) {
@@ -2085,11 +2118,12 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
             h->stats.fallback_queries = c;
         }
         if (h->w_counters.p) {
-            unsigned long long c[3] = {0, 0, 0};
+            unsigned long long c[4] = {0, 0, 0, 0};
             HY_CUDA(cudaMemcpy(c, h->w_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
             h->stats.tile_blocks = c[0];
             h->stats.tile_blocks_max = c[1];
             h->stats.block_sums = c[2];
+            h->stats.block_sums_max = c[3];
         }
     }
     *out = h->stats;

@@ -152,8 +152,9 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     float* qs = bufs + static_cast<size_t>(LM_WARPS) * R * slot_floats;
     uint64_t* bars = reinterpret_cast<uint64_t*>(qs + static_cast<size_t>(QG) * L.row_pitch);
     __shared__ float s_thr[QG];
+    __shared__ float s_lo[QG], s_hi[QG];  // OPT_TRIANGLE: each query's candidate2centroid window
     __shared__ int s_qid[QG];
-    __shared__ int s_next, s_ntiles, s_nrows, s_nqv, s_done;
+    __shared__ int s_next, s_ntiles, s_nrows, s_nqv, s_done, s_list;
     __shared__ long long s_row0;
     // Per-warp ring tags: tile index within the item and block of each slot.
     __shared__ int s_tag_tile[LM_WARPS][R];
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     const bool l2 = p.metric == METRIC_L2;
     const bool prune = p.prune && l2;
     uint32_t iss = 0, con = 0;  // copies issued / consumed by this warp (ring position)
-    unsigned long long loaded = 0, computed = 0, possible = 0;
+    unsigned long long loaded = 0, computed = 0, possible = 0, possible_sums = 0;
     const int64_t nitems = p.item_off[p.nlist];
 
     for (;;) {
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                 s_nrows = min(p.rs, p.list_size[l] - lrow0);
                 s_ntiles = (s_nrows + 31) >> 5;
                 s_row0 = p.list_off[l] + lrow0;
+                s_list = l;
                 s_next = 0;
                 s_done = 0;
                 // query ids of the group
@@ -219,6 +221,32 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
             }
             qs[i] = v;
         }
+        if (p.triangle) {
+            // The reference's inner-product window (src/Index.cpp:1519-1542):
+            // with s = the query's k-th similarity so far and c = its inner
+            // product with the list's centroid, rows whose candidate2centroid
+            // lies outside [s c - sqrt(1-s^2) sqrt(1-c^2), s c + sqrt(1-s^2)
+            // sqrt(1-c^2)] (no upper limit when s < c) cannot reach s for
+            // unit-norm rows and queries, and are not scanned.  Without a
+            // threshold (s = -inf) or off the unit sphere the bounds are NaN
+            // and nothing is skipped, as in the reference.
+            const float* cl = p.cent + static_cast<size_t>(s_list) * L.d;
+            for (int j = warp; j < QG; j += LM_WARPS) {
+                float c = 0.0f;
+                if (j < nqv) {
+                    const float* qj = p.q + static_cast<size_t>(s_qid[j]) * L.d;
+                    for (int e = lane; e < L.d; e += 32) c = __fmaf_rn(qj[e], cl[e], c);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+                }
+                if (lane == 0) {
+                    const float sim = -s_thr[j];
+                    const float ss = sqrtf(1.0f - sim * sim), sc = sqrtf(1.0f - c * c);
+                    s_lo[j] = sim * c - ss * sc;
+                    s_hi[j] = sim < c ? INFINITY : sim * c + ss * sc;
+                }
+            }
+        }
         __syncthreads();
         const int ntiles = s_ntiles, nrows = s_nrows;
         const int64_t row0 = s_row0;
@@ -245,9 +273,17 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                         more = false;
                         return;
                     }
+                    possible += L.nb;
+                    possible_sums += static_cast<unsigned long long>(L.nb) * nqv;
+                    if (p.triangle) {
+                        // A tile whose rows lie outside every query's window
+                        // is not loaded.
+                        const float2 tr = p.c2c_tile[(row0 >> 5) + g];
+                        const bool hit = lane < nqv && !(tr.y > s_hi[lane]) && !(tr.x < s_lo[lane]);
+                        if (!__any_sync(FULL, hit)) continue;
+                    }
                     it_tile = g;
                     it_b = 0;
-                    possible += L.nb;
                 }
                 const int slot = static_cast<int>(iss % R);
                 const int b = it_b;
@@ -287,6 +323,12 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                 cur_tile = tile;
                 const int nv = min(32, nrows - 32 * tile);
                 alive = lane < nv ? qmask : 0u;
+                if (p.triangle && lane < nv) {
+                    const float cc = p.c2c[row0 + 32 * static_cast<int64_t>(tile) + lane];
+#pragma unroll
+                    for (int qi = 0; qi < QG; ++qi)
+                        if (cc > s_hi[qi] || cc < s_lo[qi]) alive &= ~(1u << qi);
+                }
             }
             if (tile != dead_tile) {
                 const uint32_t live = __reduce_or_sync(FULL, alive);
@@ -337,6 +379,7 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
         atomicAdd(&p.counters[0], loaded);
         atomicAdd(&p.counters[1], possible);
         atomicAdd(&p.counters[2], computed);
+        atomicAdd(&p.counters[3], possible_sums);
     }
 }
 
@@ -418,6 +461,50 @@ __global__ void __launch_bounds__(256) list_topk_kernel(uint64_t* __restrict__ c
     }
 }
 
+// Per arena row: the inner product with its list's centroid (the reference's
+// candidate2centroid, src/Index.cpp:659-667; rows of a list are ordered by it,
+// descending), and per 32-row tile {max, min} over its valid rows.  One warp
+// per tile; lane = row; dimensions in order.
+__global__ void row_centroid_ip_kernel(ArenaLayout L, const float* __restrict__ codes,
+                                       const int64_t* __restrict__ list_off, const int32_t* __restrict__ list_size,
+                                       int nlist, const float* __restrict__ cent, float* __restrict__ c2c,
+                                       float2* __restrict__ c2c_tile) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    // gw enumerates (list, tile of the list): find the list by binary search
+    // over the tile offsets list_off / 32.
+    const int64_t ntiles_all = list_off[nlist] >> 5;
+    if (gw >= ntiles_all) return;
+    int lo = 0, hi = nlist - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((list_off[mid] >> 5) <= gw)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int l = lo;
+    const int64_t r = gw * 32 + lane;
+    const bool valid = r - list_off[l] < list_size[l];
+    float v = 0.0f;
+    if (valid) {
+        const float* c = cent + static_cast<size_t>(l) * L.d;
+        for (int b = 0; b < L.nb; ++b) {
+            const int w = L.bstart[b + 1] - L.bstart[b];
+            for (int j = 0; j < w; ++j)
+                v = __fadd_rn(v, __fmul_rn(codes[arena_offset(L, r, b, j)], c[L.bstart[b] + j]));
+        }
+    }
+    c2c[r] = v;
+    float mx = valid ? v : -INFINITY, mn = valid ? v : INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(FULL, mn, o));
+    }
+    if (lane == 0) c2c_tile[gw] = make_float2(mx, mn);
+}
+
 template <int QG, int R, bool MULTI>
 size_t list_scan_smem(const ArenaLayout& L) {
     return static_cast<size_t>(LM_WARPS) * R * 32 * L.max_pitch * 4 + static_cast<size_t>(QG) * L.row_pitch * 4 +
@@ -460,6 +547,16 @@ cudaError_t launch_list_scan(const ListScanParams& p, int nsm, cudaStream_t s) {
     if (!list_scan_multi(p.L)) return launch_list_scan_t<LM_GROUP, 3, false>(p, nsm, s);
     if (p.L.max_pitch <= 64) return launch_list_scan_t<LM_GROUP, 2, true>(p, nsm, s);
     return launch_list_scan_t<LM_GROUP, 1, true>(p, nsm, s);
+}
+
+cudaError_t launch_row_centroid_ip(const ArenaLayout& L, const float* codes, const int64_t* list_off,
+                                   const int32_t* list_size, int nlist, int64_t arena_rows, const float* cent,
+                                   float* c2c, float2* c2c_tile, cudaStream_t s) {
+    const int64_t tiles = arena_rows / 32;
+    if (tiles < 1) return cudaSuccess;
+    row_centroid_ip_kernel<<<static_cast<int>((tiles * 32 + 255) / 256), 256, 0, s>>>(L, codes, list_off, list_size,
+                                                                                      nlist, cent, c2c, c2c_tile);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_list_topk(uint64_t* cand, int32_t* cnt, int nq, int capq, int k, int metric, int mode,

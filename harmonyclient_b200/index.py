@@ -80,6 +80,16 @@ class Index:
         return self.info().ntotal
 
     @property
+    def opt_level(self):
+        return self.info().opt_level
+
+    @opt_level.setter
+    def opt_level(self, v):
+        """OPT_TRIANGLE with inner product: the reference's cos-bound window
+        (see include/hy.h, hy_index_set_opt_level)."""
+        check(self._L.hy_index_set_opt_level(self._h, int(v)))
+
+    @property
     def nprobe(self):
         return self.info().nprobe
 

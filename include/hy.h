@@ -109,6 +109,7 @@ typedef struct {
     uint64_t kernel_launches; /* launches kernel_ms covers */
     uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
     uint64_t block_sums;      /* list-major plain scan: (query, 32-row x one-dim-block) partial sums computed */
+    uint64_t block_sums_max;  /* list-major plain scan: the partial sums a scan without pruning computes */
     uint64_t list_major;      /* plain form: 1 when the search ran the list-major scan */
 } hy_search_stats_t;
 
@@ -117,8 +118,8 @@ HY_API const char* hy_version(void);
 
 /* Index lifecycle.  Replaces harmony::Index::Index(d, nlist, nprobe, metric,
  * opt_level, ...) (src/Index.h:15-25, src/Index.cpp:24-43).  opt_level is
- * accepted for compatibility (callers pass OPT_ALL through sub_k,
- * src/query.cpp:460); only OPT_NONE scanning is implemented.  dim_blocks is
+ * the reference's OptLevel (see hy_index_set_opt_level; callers also pass
+ * OPT_ALL through sub_k, src/query.cpp:460, which is accepted).  dim_blocks is
  * the number of dimension blocks the partial-distance prune checks between
  * (the reference hard-codes 4, src/node.cpp:639); 0 selects 4. */
 HY_API int hy_index_create(size_t d, size_t nlist, size_t nprobe, int metric, int opt_level, size_t dim_blocks,
@@ -144,6 +145,19 @@ HY_API int hy_index_add(hy_index* h, size_t n, const float* x);
 HY_API int hy_index_add_device(hy_index* h, size_t n, const float* dx, void* stream);
 
 HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
+
+/* The public opt_level field (src/Index.h:108; callers set it between
+ * searches, src/main.cpp:61-70).  OPT_TRIANGLE with the inner-product
+ * metric scans, per (query, probed list), only the rows whose inner product
+ * with the list's centroid lies in the reference's cos-bound window
+ * (src/Index.cpp:1509-1546), built from the query's k-th similarity so far;
+ * for unit-norm rows and queries the skipped rows cannot reach the top-k, so
+ * the answer is the exact scan's, as in the reference.  The list-major scan
+ * applies the window; the query-major scan scans every row.  The L2 triangle
+ * and the sub-NN levels change nothing in the reference's search (their scan
+ * code is commented out, src/Index.cpp:1468-1492, src/IVFScan.hpp:223-427)
+ * and nothing here. */
+HY_API int hy_index_set_opt_level(hy_index* h, int opt_level);
 
 /* Scan form (no counterpart in the reference, whose only scan is the exact
  * FP32 one): HY_FORM_PLAIN or HY_FORM_BF16 (d <= 128).  The bf16 form batches

@@ -49,6 +49,7 @@ def load():
     L.ref_set_centroids.argtypes = [vp, fp]
     L.ref_get_centroids.argtypes = [vp, fp]
     L.ref_set_nprobe.argtypes = [vp, sz]
+    L.ref_set_opt_level.argtypes = [vp, C.c_int]
     L.ref_add.argtypes = [vp, sz, fp]
     L.ref_list_size.argtypes = [vp, sz, C.POINTER(C.c_size_t)]
     L.ref_get_list.argtypes = [vp, sz, ip64, fp, fp]
@@ -123,6 +124,9 @@ class RefIndex:
     def set_nprobe(self, nprobe):
         self.nprobe = nprobe
         _check(self.L.ref_set_nprobe(self.h, nprobe))
+
+    def set_opt_level(self, opt_level):
+        _check(self.L.ref_set_opt_level(self.h, int(opt_level)))
 
     def add(self, x):
         x = np.ascontiguousarray(x, np.float32)

@@ -13,6 +13,7 @@
 //   ref_set_centroids / ref_get_centroids the public centroid_codes field
 //   ref_add                               Index::add (src/Index.cpp:581-697)
 //   ref_list_size / ref_get_list          IVF lists (src/IVF.h:17-28)
+//   ref_set_opt_level                     the public opt_level field (src/Index.h:108)
 //   ref_search_original                   Index::search, ORIGINAL mode
 //                                         (src/Index.cpp:1638-1706 -> 1420-1554)
 //   ref_probes                            findNearNprobeOfCentroidIds (src/Index.cpp:967-995)
@@ -117,6 +118,13 @@ extern "C" int ref_get_centroids(void* h, float* c) {
 
 extern "C" int ref_set_nprobe(void* h, size_t nprobe) {
     REF_TRY({ static_cast<RefIndex*>(h)->idx->nprobe = nprobe; });
+}
+
+// The public opt_level field (src/Index.h:108): add() stores the per-row
+// candidate2centroid for OPT_TRIANGLE (src/Index.cpp:659-667) and the inner
+// product search scans the cos-bound window (src/Index.cpp:1509-1546).
+extern "C" int ref_set_opt_level(void* h, int opt_level) {
+    REF_TRY({ static_cast<RefIndex*>(h)->idx->opt_level = static_cast<harmony::OptLevel>(opt_level); });
 }
 
 extern "C" int ref_add(void* h, size_t n, const float* x) {

@@ -43,7 +43,7 @@ int main(int argc, char** argv) {
         std::ofstream(pre + ".D", std::ios::binary).write(reinterpret_cast<const char*>(D.data()), D.size() * 4);
         std::ofstream(pre + ".I", std::ios::binary).write(reinterpret_cast<const char*>(I.data()), I.size() * 8);
         std::ofstream(pre + ".C", std::ios::binary)
-            .write(reinterpret_cast<const char*>(index.centroid_codes.data()), index.centroid_codes.size() * 4);
+            .write(reinterpret_cast<const char*>(index.centroid_codes.get()), nlist * d * 4);
         std::cout << "searched " << st.nq << " queries, skip rate " << st.skip_rate() << "\n";
     } catch (const std::exception& e) {
         std::cerr << "error: " << e.what() << "\n";

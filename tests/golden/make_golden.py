@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this directory by running the REFERENCE's
 own code (oracle/_ref, compiled unmodified from the Harmony sources).
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [case ...]
 
 Inputs are not stored: every case regenerates its data from a numpy seed
 (harmonyclient_b200.datasets / numpy.random.default_rng), and the fixture
@@ -41,6 +41,8 @@ def ivf_case(name):
     R = ref.RefIndex(c["d"], c["nlist"], c["nprobe"], c["metric"])
     R.train(x)
     cent = R.centroids()
+    if c.get("opt_level"):
+        R.set_opt_level(c["opt_level"])
     R.add(x)
     D, I = R.search(q, c["k"])
     P = R.probes(q)
@@ -71,11 +73,15 @@ def index_file():
 
 
 if __name__ == "__main__":
+    # With case names as arguments only those fixtures are written.
     ref.set_threads(1)
-    heap_kat()
+    only = sys.argv[1:]
+    if not only:
+        heap_kat()
     for n in cases.CASES:
-        if n != "tiny_file":
+        if n != "tiny_file" and (not only or n in only):
             ivf_case(n)
             print("wrote", n)
-    index_file()
+    if not only:
+        index_file()
     print("done")

@@ -61,8 +61,11 @@ def test_file_inspect_rejects_truncated(tmp_path):
         file_inspect(tmp_path / "missing.index")
 
 
-def test_cpp_facade_compiles(tmp_path):
-    """include/harmony/Index.h compiles as C++17 and links against libhy.so."""
+@pytest.mark.parametrize("name", ["facade_demo", "benchmark_caller"])
+def test_cpp_facade_compiles(tmp_path, name):
+    """include/harmony/Index.h compiles as C++17 (warnings as errors) and
+    links against libhy.so, for a minimal caller and for one that uses every
+    public member the reference's drivers touch."""
     from tests.cpp_facade import build
-    exe = build(tmp_path)
+    exe = build(tmp_path, name)
     assert os.path.exists(exe)

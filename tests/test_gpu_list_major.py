@@ -86,7 +86,7 @@ def test_k_range_with_warmup(k):
     # the warm-up and first-pass thresholds prune: fewer block sums than
     # (query, tile, block) triples
     st = lm[2]
-    assert st["tile_blocks"] < st["tile_blocks_max"]
+    assert 0 < st["block_sums"] < st["block_sums_max"]
 
 
 def test_per_query_nprobe():
@@ -141,3 +141,29 @@ def test_device_api_in_graph_mode():
     finally:
         idx.set_graph(False)
         idx.set_plain_scan("auto")
+
+
+def test_ip_triangle_window_matches_reference():
+    """OPT_TRIANGLE on clustered unit-norm data (tests/golden/ip_tri.npz, the
+    reference's own answer at that opt level): the list-major scan skips the
+    rows outside each (query, list) window and returns the reference's
+    answer, which is also the exact (OPT_NONE) one."""
+    from tests.topk_check import assert_topk_equal, probe_tied_rows
+    idx, q, c = _golden_index("ip_tri")
+    g = np.load(os.path.join(GOLD, "ip_tri.npz"))
+    idx.set_plain_scan("list")
+    try:
+        D0, I0 = idx.search(q, c["k"])
+        st0 = idx.last_stats()
+        idx.opt_level = hb.OPT_TRIANGLE
+        D1, I1 = idx.search(q, c["k"])
+        st1 = idx.last_stats()
+    finally:
+        idx.opt_level = hb.OPT_NONE
+        idx.set_plain_scan("auto")
+    tied = probe_tied_rows(q, g["centroids"], g["probes"], 0)
+    assert_topk_equal(g["D"], g["I"], D1, I1, rtol=1e-5, metric=0, skip_rows=tied)
+    assert_topk_equal(D0, I0, D1, I1, rtol=1e-5, metric=0)
+    # the window skipped most of the probed rows' work
+    assert st1["block_sums"] < 0.5 * st0["block_sums"], (st1["block_sums"], st0["block_sums"])
+    assert st1["tile_blocks"] < st0["tile_blocks"]
