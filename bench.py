@@ -50,6 +50,15 @@ KNOWN_TRAFFIC = {
 }
 
 
+def idx_layout_pitches(d, nb=4):
+    """Padded width (floats, a multiple of 32) of each of the arena's nb
+    dimension blocks: block b spans d // nb dimensions, the last one the
+    remainder."""
+    w = [d // nb] * nb
+    w[-1] += d - sum(w)
+    return [(x + 31) // 32 * 32 for x in w]
+
+
 def peaks():
     """(HBM GB/s, dense bf16 TFLOP/s burst, which) from MEASURED_PEAKS.json,
     else the pool's earlier fallback measurement."""
@@ -400,8 +409,9 @@ def run_ours(args, rank, world, dist):
         idx.set_form("plain")
         _search(idx, dq, dD, dI, k, stream, npq)
         pms, pst, pclk = _time_device(idx, dq, dD, dI, k, args.plain_steps, stream, dist, dev, npq)
-        pk_ms, _ = _kernel_ms(idx, dq, dD, dI, k, 1, stream, npq)
-        plain = {"ms": pms, "kernel_ms": pk_ms, "I": dI.cpu().numpy(), "D": dD.cpu().numpy(), "clocks": pclk}
+        pk_ms, pk_launches = _kernel_ms(idx, dq, dD, dI, k, 1, stream, npq)
+        plain = {"ms": pms, "kernel_ms": pk_ms, "launches": pk_launches, "stats": idx.last_stats(),
+                 "I": dI.cpu().numpy(), "D": dD.cpu().numpy(), "clocks": pclk}
         idx.set_form(base)
         if learned:
             idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
@@ -464,19 +474,41 @@ def run_ours(args, rank, world, dist):
             P_plain[np.arange(P_plain.shape[1])[None, :] >= npq_host[:, None]] = -1
         prow = pair_rows(P_plain)
         palg = prow * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
-        pach = palg / (plain["kernel_ms"] / 1e3) / 1e9
+        pst = plain["stats"]
+        scan_ms = plain["kernel_ms"] * plain["launches"]  # every scan launch of one search
         sc_plain, _ = _score(x, q, plain["D"], plain["I"], args.recall_sample, truth)
         pv = world * q.shape[0] * args.plain_steps / (plain["ms"] / 1e3)
+        if pst.get("list_major"):
+            # The list-major scan reads each list once per group of 32
+            # queries, so its bound is FP32 issue: 3 FP32 operations (sub,
+            # mul, add) per (query, row, dimension) of every block sum it
+            # executed (32 rows x a block's padded width), against 148 SMs x
+            # 128 FP32 lanes x the SM clock measured during the run.
+            width = sum(idx_layout_pitches(d)) / len(idx_layout_pitches(d))
+            ops = pst["block_sums"] * 32 * width * 3
+            sm_mhz = (plain["clocks"] or {}).get("sm_mhz") or 1965.0
+            fpeak = 148 * 128 * sm_mhz * 1e6 / 1e12
+            fach = ops / (scan_ms / 1e3) / 1e12
+            proof = {"bound": "fp32", "achieved": round(fach, 2), "peak": round(fpeak, 2), "unit": "TFLOP/s",
+                     "frac": round(fach / fpeak, 4),
+                     "peak_kind": "nominal FP32 issue (148 SMs x 128 lanes x measured SM clock)",
+                     "kernel": "list_scan_kernel", "kernel_ms": round(scan_ms, 4),
+                     "launches_per_search": plain["launches"], "executed_ops": int(ops),
+                     "block_sums_executed": round(pst["block_sums"] / max(pst["block_sums_max"], 1), 4),
+                     "pair_bytes": palg, "pair_bytes_rate_gbs": round(palg / (scan_ms / 1e3) / 1e9, 1),
+                     "traffic": KNOWN_TRAFFIC.get((args.workload, "plain-lm", args.nb, args.nq, args.nprobe))}
+        else:
+            pach = palg / (scan_ms / 1e3) / 1e9
+            proof = {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
+                     "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb, args.nq, args.nprobe)),
+                     "kernel": "scan_plain_kernel", "kernel_ms": round(scan_ms, 4), "algorithmic_bytes": palg}
         plain_line = {"value": round(pv, 1), "unit": "queries/s", "steps": args.plain_steps,
                       "ms_per_step": round(plain["ms"] / args.plain_steps, 3),
                       "recall_at_10": round(sc_plain["recall"], 4),
                       "dist_rel_err_max": sc_plain["dist_rel_err_max"],
                       "nprobe": args.nprobe, "speedup_of_headline": round(value / pv, 2),
-                      "roofline": {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
-                                   "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
-                                   "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb, args.nq, args.nprobe)),
-                                   "kernel": "scan_plain_kernel", "kernel_ms": round(plain["kernel_ms"], 4),
-                                   "algorithmic_bytes": palg},
+                      "roofline": proof, "fallback_queries": pst.get("fallback_queries", 0),
                       "clocks": plain["clocks"]}
 
     parity = None
@@ -548,6 +580,21 @@ def run_ours(args, rank, world, dist):
         "clocks": clocks,
         "build_s": round(build_s, 2),
     }
+    if args.extras and world == 1:
+        # The main index's other nprobes, then two other workloads (each
+        # failure is recorded in the line rather than losing it).
+        extras = {}
+        for name, fn in (("c2_nprobe", lambda: extra_nprobe_sweep(idx, x, q, k, (16, 64, 256), 3, stream, dev,
+                                                                     args.nprobe)),
+                         ("c2_sigma60", lambda: extra_c2_hard(args, stream, dev, 3)),
+                         ("c3", lambda: extra_c3(args, stream, dev, 3))):
+            t0 = time.perf_counter()
+            try:
+                extras[name] = fn()
+            except Exception as e:  # noqa: BLE001 - reported in the line
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+            extras[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+        line["extras"] = extras
     if learned:
         line["probe_model"] = {"train_queries": args.train_queries, "epochs": args.epochs,
                                "coverage_target": args.coverage, "train_s": round(train_s, 2),
@@ -556,6 +603,161 @@ def run_ours(args, rank, world, dist):
                                "judge_recall_min": round(min(judge), 4) if judge else None,
                                "judge_fallbacks": learned_fb}
     return line
+
+
+# ---------------------------------------------------------------------------
+# Extra measurements of the one-GPU line: the other nprobes of the 1M x 128
+# workload, a harder mixture on which the learned predictor has work to do,
+# and the 1M x 420 precision workload at k 10 and 100.  Each is timed with
+# CUDA events on the device-pointer API (graph mode) and scored against a
+# float64 brute force over every query.
+def _device_qps(idx, q, k, steps, ts, dev):
+    """queries/s of `steps` device-pointer searches after two untimed ones,
+    with the last answer, the stats of the last search and ms per step."""
+    import torch
+    dq = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    dD = torch.empty((q.shape[0], k), dtype=torch.float32, device="cuda")
+    dI = torch.empty((q.shape[0], k), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        _search(idx, dq, dD, dI, k, ts)
+    torch.cuda.synchronize()
+    ms, st, _ = _time_device(idx, dq, dD, dI, k, steps, ts, None, dev)
+    kern_ms, launches = _kernel_ms(idx, dq, dD, dI, k, 1, ts)
+    st = idx.last_stats()
+    return {"qps": round(q.shape[0] * steps / (ms / 1e3), 1), "ms_per_step": round(ms / steps, 4),
+            "kernel_ms": round(kern_ms * launches, 4)}, dD.cpu().numpy(), dI.cpu().numpy(), st
+
+
+def _scored(x, q, D, I, truth, at, metric=1):
+    from oracle import gpu_bruteforce as gb
+    sc = gb.score(D, I, truth["D"], truth["I"], x, q, at=at, metric=metric)
+    return {"recall_at_%d" % at: round(sc["recall"], 4), "dist_rel_err_max": sc["dist_rel_err_max"]}
+
+
+def _plain_work(st):
+    """The list-major plain scan's executed share of its unpruned block sums."""
+    if st.get("list_major") and st.get("block_sums_max"):
+        return {"scan": "list-major", "block_sums_executed": round(st["block_sums"] / st["block_sums_max"], 4)}
+    return {"scan": "query-major"}
+
+
+def extra_nprobe_sweep(idx, x, q, k, nprobes, steps, ts, dev, main_nprobe):
+    """bf16 (fixed nprobe) and plain FP32 at each nprobe on the main index."""
+    from oracle import gpu_bruteforce as gb
+    truth = {}
+    truth["D"], truth["I"] = gb.topk(x, q, 10)
+    out = {}
+    idx.set_learned(False)
+    for npb in nprobes:
+        idx.nprobe = npb
+        row = {}
+        for form in ("bf16", "plain"):
+            idx.set_form(form)
+            r, D, I, st = _device_qps(idx, q, k, steps, ts, dev)
+            r.update(_scored(x, q, D, I, truth, 10))
+            if form == "plain":
+                r.update(_plain_work(st))
+            row[form] = r
+        row["bf16_over_plain"] = round(row["bf16"]["qps"] / row["plain"]["qps"], 2)
+        out[str(npb)] = row
+    idx.nprobe = main_nprobe
+    return out
+
+
+def extra_c2_hard(args, ts, dev, steps):
+    """1M x 128 integer-valued mixture with sigma 60 (neighbours straddle
+    lists; nprobe 1 misses much of the top-10): the learned probes + bf16,
+    the bf16 form at a fixed nprobe equal to the learned mean, the smallest
+    fixed nprobe that reaches recall@10 0.95, and the plain FP32 scan there."""
+    import harmonyclient_b200 as hb
+    from harmonyclient_b200 import datasets
+    from oracle import gpu_bruteforce as gb
+    nb = args.nb
+    x, q = datasets.gmm_uint8(nb, args.nq, sigma=60.0, seed=0)
+    tq = datasets.gmm_uint8(0, args.train_queries, sigma=60.0, seed=0, query_seed=777)[1]
+    k = 10
+    idx = hb.Index(128, 1024, 64, hb.METRIC_L2, device=dev)
+    idx.train(x)
+    idx.add(x)
+    idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
+    truth = {}
+    truth["D"], truth["I"] = gb.topk(x, q, 10)
+    idx.set_form("bf16")
+    sweep = {}
+    for npb in (1, 2, 4, 8, 16, 32, 64):
+        idx.nprobe = npb
+        r, D, I, _ = _device_qps(idx, q, k, steps, ts, dev)
+        r.update(_scored(x, q, D, I, truth, 10))
+        sweep[str(npb)] = r
+    reach = [int(n) for n, r in sweep.items() if r["recall_at_10"] >= 0.95]
+    target = min(reach) if reach else 64
+    idx.nprobe = 64
+    t0 = time.perf_counter()
+    rep = idx.train_probe_model(tq, max_nprobe=64, k_label=10, epochs=args.epochs, lr=1e-3, coverage=args.coverage)
+    train_s = time.perf_counter() - t0
+    idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
+    learned, D, I, _ = _device_qps(idx, q, k, steps, ts, dev)
+    learned.update(_scored(x, q, D, I, truth, 10))
+    mean_np = float((idx.probes(q) >= 0).sum()) / q.shape[0]
+    learned["mean_nprobe"] = round(mean_np, 3)
+    idx.set_learned(False)
+    idx.nprobe = max(1, int(round(mean_np)))
+    same_np, D, I, _ = _device_qps(idx, q, k, steps, ts, dev)
+    same_np.update(_scored(x, q, D, I, truth, 10))
+    same_np["nprobe"] = idx.nprobe
+    idx.nprobe = target
+    idx.set_form("plain")
+    plain, D, I, st = _device_qps(idx, q, k, max(1, steps // 2), ts, dev)
+    plain.update(_scored(x, q, D, I, truth, 10))
+    plain.update(_plain_work(st))
+    plain["nprobe"] = target
+    at_target = sweep[str(target)]
+    return {
+        "workload": f"{nb} x 128 uint8-valued gmm (4096 components, sigma 60), nlist 1024, k 10, "
+                    f"{q.shape[0]} queries; probe network trained on {tq.shape[0]} other queries "
+                    f"({round(train_s, 2)} s)",
+        "bf16_fixed_nprobe": sweep,
+        "smallest_fixed_nprobe_at_recall_0.95": target,
+        "learned_bf16": learned,
+        "bf16_at_learned_mean_nprobe": same_np,
+        "plain_fp32_at_that_nprobe": plain,
+        "learned_speedup_at_equal_recall": round(learned["qps"] / at_target["qps"], 2),
+        "learned_speedup_over_plain": round(learned["qps"] / plain["qps"], 2),
+        "probe_model_heldout": {kk: round(v, 4) for kk, v in rep.items()},
+    }
+
+
+def extra_c3(args, ts, dev, steps):
+    """1M x 420 float mixture (nlist 2048, nprobe 64): the e4m3 form (4 x k
+    exact re-rank), the bf16 form and the plain FP32 scan at k 10 and 100."""
+    import harmonyclient_b200 as hb
+    from harmonyclient_b200 import datasets
+    from oracle import gpu_bruteforce as gb
+    nb = args.nb
+    x, q = datasets.gmm_dense(nb, args.nq, seed=0)
+    idx = hb.Index(420, 2048, 64, hb.METRIC_L2, device=dev)
+    idx.train(x)
+    idx.add(x)
+    truth = {}
+    truth["D"], truth["I"] = gb.topk(x, q, 100)
+    out = {"workload": f"{nb} x 420 float gmm (2048 components, per-dim mean U[-1,1], sigma 0.3), nlist 2048, "
+                       f"nprobe 64, {q.shape[0]} queries"}
+    for k in (10, 100):
+        idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
+        row = {}
+        for form in ("fp8", "bf16", "plain"):
+            idx.set_form(form)
+            if form == "fp8":
+                idx.set_batch_params(oversample=4)
+            r, D, I, st = _device_qps(idx, q, k, steps if form != "plain" else max(1, steps // 2), ts, dev)
+            r.update(_scored(x, q, D, I, truth, 10))
+            if k > 10:
+                r.update(_scored(x, q, D, I, truth, k))
+            if form == "plain":
+                r.update(_plain_work(st))
+            row[form] = r
+        out[f"k{k}"] = row
+    return out
 
 
 def run_lists(args, rank, world, dist):
@@ -677,6 +879,8 @@ def main():
     ap.add_argument("--judge-fraction", type=float, default=0.01)
     ap.add_argument("--no-graph", dest="graph", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the other nprobes, the sigma-60 mixture and the 1M x 420 workload")
     ap.add_argument("--nb", type=int, default=None, help="default: the workload's")
     ap.add_argument("--nq", type=int, default=None, help="default: the workload's")
     ap.add_argument("--recall-sample", type=int, default=0, help="queries scored for recall (0: all)")

@@ -1,4 +1,5 @@
-"""Builds libhy.so (the CUDA engine behind include/hy.h) in-tree for sm_100a.
+"""Builds libhy.so (the CUDA engine behind include/hy.h) in-tree for sm_100a,
+and harmony_serve (the TCP query server over it).
 
     python -m harmonyclient_b200.build          # build if sources changed
     python -m harmonyclient_b200.build --force  # rebuild
@@ -16,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhy.so")
+SERVER = os.path.join(HERE, "harmony_serve")
 SOURCES = ["hy_kernels.cu", "hy_batched.cu", "hy_capi.cu", "hy_selftest.cu", "hy_noalloc.cu", "hy_mlp.cu", "hy_lists.cu"]
 HEADERS = ["hy_device.cuh", "hy_kernels.cuh", "hy_tc.cuh", "hy_common.cuh", "hy_batched.cuh", "hy_mlp.cuh", "hy_lists.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -29,14 +31,15 @@ def nvcc():
 
 
 def _inputs():
-    files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "hy.h")]
+    files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS + ["hy_serve.cpp"]] + [
+        os.path.join(ROOT, "include", "hy.h")]
     return files
 
 
 def stale():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(SERVER):
         return True
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(SERVER))
     return any(os.path.getmtime(f) > t for f in _inputs())
 
 
@@ -57,7 +60,19 @@ def build(force=False, verbose=False):
     tmp = LIB + ".tmp"
     subprocess.run([nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp] + objs, check=True)
     os.replace(tmp, LIB)
+    build_server()
     return LIB
+
+
+def build_server():
+    """harmony_serve: the TCP query server (csrc/hy_serve.cpp), a host
+    program over libhy.so found next to it."""
+    tmp = SERVER + ".tmp"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(CSRC, "hy_serve.cpp"), "-o", tmp, "-L", HERE, "-lhy", "-Wl,-rpath,$ORIGIN"],
+                   check=True)
+    os.replace(tmp, SERVER)
+    return SERVER
 
 
 if __name__ == "__main__":

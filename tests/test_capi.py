@@ -69,3 +69,16 @@ def test_cpp_facade_compiles(tmp_path, name):
     from tests.cpp_facade import build
     exe = build(tmp_path, name)
     assert os.path.exists(exe)
+
+
+def test_server_builds_and_checks_its_arguments():
+    """harmony_serve is built next to libhy.so and refuses a call without
+    exactly one of --index / --train_data (no GPU needed)."""
+    import subprocess
+
+    from harmonyclient_b200 import build
+    exe = build.build_server()
+    r = subprocess.run([exe, "--port", "1"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "exactly one of" in r.stderr
+    r = subprocess.run([exe, "--index", "a", "--train_data", "b"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1

@@ -92,17 +92,27 @@ def test_warmup_tops_match_reference(name):
 
 
 @pytest.mark.parametrize("name", ["c1", "int_small"])
-def test_search_with_warmup_threshold_is_exact(name):
+@pytest.mark.parametrize("scan", ["query", "list"])
+def test_search_with_warmup_threshold_is_exact(name, scan):
     """Pruning against the warm-up threshold (the GROUP/IVF mode semantics)
-    gives the same answer as the reference's unpruned search."""
+    gives the same answer as the reference's unpruned search, with either
+    plain scan.  The query-major scan skips whole dimension blocks of a tile;
+    the list-major one skips a query's partial sums for a tile (the tile is
+    loaded while any query of the group still needs it)."""
     idx, x, q, c = gpu_index(name)
     g = load(name)
     idx.preSearch(warmUpSearchList=10, warmUpSearchListSize=c["k"])
+    idx.set_plain_scan(scan)
     D, I = idx.search(q, c["k"])
+    st = idx.last_stats()
     tied = probe_tied_rows(q, g["centroids"], g["probes"])
     assert_topk_equal(g["D"], g["I"], D, I, rtol=0.0 if name == "int_small" else 1e-5, skip_rows=tied)
-    st = idx.last_stats()
-    assert st["tile_blocks"] < st["tile_blocks_max"], "pruning should skip some dimension blocks"
+    if scan == "list":
+        assert st["list_major"] == 1
+        assert st["block_sums"] < st["block_sums_max"], "pruning should skip some partial sums"
+    else:
+        assert st["list_major"] == 0
+        assert st["tile_blocks"] < st["tile_blocks_max"], "pruning should skip some dimension blocks"
 
 
 def test_exhaustive_recall_is_one():
