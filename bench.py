@@ -221,7 +221,36 @@ def cpu_baseline_ref(x, q, cent, nprobe, k, budget_s):
     dt = time.perf_counter() - t0
     info = {"value": m2 / dt, "unit": "queries/s", "cores": nt, "kind": "reference",
             "sample": f"{m2} of {q.shape[0]} queries, reference Index::search ORIGINAL mode, OpenMP x{nt}"}
+    info["group"] = cpu_baseline_group(R, q[:m2], k, Dr, Ir, nt)
     return info, Dr, Ir
+
+
+def cpu_baseline_group(R, q, k, Dr, Ir, cores):
+    """The reference's default distributed mode (GROUP with pruning,
+    src/Index.cpp:1053-1187, src/node.cpp:679-1203) in its documented
+    configuration (--group 2 --team 2 --block 4 on 5 MPI ranks), the ranks
+    run as threads of this process (oracle/ref_mpi_threads.cpp) with the host
+    cores split between them; timed as the reference times it (the master's
+    Index::search), with every row compared to the ORIGINAL search's."""
+    from tests.topk_check import row_agree
+    workers, group, team, block = 4, 2, 2, 4
+    m = min(q.shape[0], 10_000) // (group * block) * (group * block)
+    if m == 0 or k > 100:
+        return {"unavailable": "GROUP mode needs k <= 100 and nq divisible by group x block"}
+    try:
+        import psutil
+        if psutil.virtual_memory().available < 48 << 30:
+            return {"unavailable": "GROUP mode's per-worker distance buffers need ~20 GB of host memory here"}
+    except ImportError:
+        pass
+    tpr = max(1, cores // (workers + 1))
+    D, I, secs = R.search_group(q[:m], k, workers=workers, group=group, team=team, block=block,
+                                threads_per_rank=tpr)
+    eq = sum(1 for r in range(m) if row_agree(Dr[r], Ir[r], D[r], I[r], 0.0)[0])
+    return {"value": round(m / secs, 2), "unit": "queries/s", "cores": tpr * (workers + 1),
+            "ranks": workers + 1, "config": "group 2, team 2, block 4, pruning on, warm-up 10 lists x k rows",
+            "ranks_as": "threads of one process (no MPI on this host)", "queries": m,
+            "rows_equal_to_original": eq}
 
 
 def parity_block(Dr, Ir, answers, q, cent, nprobe, k, integral):

@@ -58,6 +58,8 @@ def load():
     L.ref_warmup_tops.argtypes = [vp, sz, fp, sz, sz, sz, ip64, fp]
     L.ref_search_prune.argtypes = [vp, sz, fp, sz, ip64, fp, fp, ip64]
     L.ref_heap_topk.argtypes = [C.c_int, sz, fp, ip64, sz, fp, ip64]
+    L.ref_search_group.argtypes = [vp, sz, fp, sz, C.c_int, C.c_int, C.c_int, C.c_int, sz, sz, C.c_int, C.c_int,
+                                   C.c_char_p, fp, ip64, C.POINTER(C.c_double)]
     L.ref_save.argtypes = [vp, C.c_char_p]
     L.ref_load.argtypes = [vp, C.c_char_p]
     L.ref_info.argtypes = [vp] + [C.POINTER(C.c_size_t)] * 3 + [C.POINTER(C.c_int)]
@@ -152,6 +154,29 @@ class RefIndex:
         I = np.empty((q.shape[0], k), np.int64)
         _check(self.L.ref_search_original(self.h, q.shape[0], _p(q), k, _p(D), _p(I)))
         return D, I
+
+    def search_group(self, q, k, workers=4, group=2, team=2, block=4, warmup_list=10, warmup_list_size=None,
+                     cut=True, threads_per_rank=None, scratch_path=None):
+        """The reference's GROUP mode with pruning (its default distributed
+        mode), 1 master + `workers` ranks run as threads of this process.
+        Returns (D, I, seconds of the master's search).  The reference needs
+        nq <= 10000, divisible by group * block, and k <= 100."""
+        import os
+        import tempfile
+        q = np.ascontiguousarray(q, np.float32)
+        if warmup_list_size is None:
+            warmup_list_size = k
+        if threads_per_rank is None:
+            threads_per_rank = max(1, (os.cpu_count() or 1) // (workers + 1))
+        D = np.empty((q.shape[0], k), np.float32)
+        I = np.empty((q.shape[0], k), np.int64)
+        secs = C.c_double()
+        with tempfile.TemporaryDirectory() as tmp:
+            path = scratch_path or os.path.join(tmp, "group.index")
+            _check(self.L.ref_search_group(self.h, q.shape[0], _p(q), k, workers, group, team, block, warmup_list,
+                                           warmup_list_size, int(cut), threads_per_rank, path.encode(), _p(D), _p(I),
+                                           C.byref(secs)))
+        return D, I, secs.value
 
     def probes(self, q):
         q = np.ascontiguousarray(q, np.float32)

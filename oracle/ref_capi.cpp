@@ -22,6 +22,8 @@
 //                                         cut=true (src/node.cpp:606-678), heaps initialised
 //                                         and sorted as the master does (src/Index.cpp:1309,1340)
 //   ref_heap_topk                         heap_replace_top + heap_sort (src/heap.hpp:35-82)
+//   ref_search_group                      GROUP mode with pruning, MPI ranks as threads
+//                                         (src/Index.cpp:1053-1187, src/node.cpp:679-1203)
 //   ref_save / ref_load                   Index::save_index / load_index (src/Index.cpp:1708-1770)
 #include <algorithm>
 #include <chrono>
@@ -36,6 +38,7 @@
 #include <random>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 #include <omp.h>
 
@@ -66,6 +69,20 @@ extern "C" const char* ref_last_error(void) { return g_err.c_str(); }
 struct RefIndex {
     std::unique_ptr<harmony::Index> idx;
     harmony::Index::Param param;
+};
+
+// Discards everything written to it, from any thread (no buffer, so no
+// shared put area between threads).
+struct NullBuf : std::streambuf {
+    int overflow(int c) override { return c == EOF ? 0 : c; }
+};
+
+// Silence std::cout while ranks on several threads write to it.
+struct QuietAll {
+    std::streambuf* old;
+    NullBuf sink;
+    QuietAll() : old(std::cout.rdbuf(&sink)) {}
+    ~QuietAll() { std::cout.rdbuf(old); }
 };
 
 // Silence the reference's chatty std::cout while it runs.
@@ -230,6 +247,86 @@ extern "C" int ref_heap_topk(int metric, size_t n, const float* vals, const int6
             }
         }
         harmony::sort_result(static_cast<harmony::MetricType>(metric), k, out_v, reinterpret_cast<idx_t*>(out_i));
+    });
+}
+
+// The reference's default distributed mode, GROUP with pruning
+// (src/Index.cpp:1053-1187 master, src/node.cpp:679-1203 GroupWorker), with
+// its MPI ranks as threads of this process (ref_mpi_threads.cpp): rank 0 is
+// the calling thread and runs preSearch + search as the benchmark driver's
+// master does (src/query.cpp:900-923); ranks 1..workers run what its
+// workers run in benchmark mode (src/query.cpp:98-114, 252-255: a barrier,
+// then GroupWorker init, receiveQuery, search).  teamSize = workers /
+// teamCount as the driver computes it (src/query.cpp:231).  Each worker's
+// OpenMP regions use threads_per_rank threads, the master's at least
+// team_count.  *seconds receives the wall
+// time of the master's Index::search alone (what the reference times).
+extern "C" void ref_mpi_threads_init(int size);
+extern "C" void ref_mpi_threads_bind(int rank);
+
+extern "C" int ref_search_group(void* h, size_t n, const float* q, size_t k, int workers, int group_count,
+                                int team_count, int block_count, size_t warmup_list, size_t warmup_list_size,
+                                int cut, int threads_per_rank, const char* scratch_path, float* D, int64_t* I,
+                                double* seconds) {
+    REF_TRY({
+        if (workers < 1 || team_count < 1 || group_count < 1 || block_count < 1 || workers % team_count)
+            throw std::runtime_error("ref_search_group: need workers divisible by team_count, all >= 1");
+        QuietAll qq;
+        auto* r = static_cast<RefIndex*>(h);
+        ref_mpi_threads_init(workers + 1);
+        std::vector<std::thread> ranks;
+        std::vector<std::string> errs(workers + 1);
+        for (int rank = 1; rank <= workers; ++rank) {
+            ranks.emplace_back([=, &errs] {
+                try {
+                    ref_mpi_threads_bind(rank);
+                    omp_set_num_threads(threads_per_rank);
+                    MPI_Barrier(MPI_COMM_WORLD);
+                    harmony::GroupWorker w;
+                    w.init(rank, false);
+                    w.receiveQuery();
+                    w.search(cut != 0, false);
+                } catch (const std::exception& e) {
+                    errs[rank] = e.what();
+                }
+            });
+        }
+        ref_mpi_threads_bind(0);
+        // The master receives each team's results in an OpenMP loop over the
+        // teams and forwards a group's heaps to the next team from inside it
+        // (src/Index.cpp:1133-1176): with fewer threads than teams, a team
+        // would wait on heaps the master has not reached yet.
+        omp_set_num_threads(std::max(threads_per_rank, team_count));
+        harmony::Index::Param& p = r->param;
+        p.mode = harmony::Index::SearchMode::DIVIDE_GROUP;
+        p.orderOptimize = true;
+        p.pruning = cut != 0;
+        p.fullWarmUp = false;
+        p.groupCount = group_count;
+        p.teamCount = team_count;
+        p.teamSize = workers / team_count;
+        p.hardInBalance = false;
+        size_t nb = 0;
+        for (size_t l = 0; l < r->idx->nlist; ++l) nb += r->idx->lists[l].get_list_size();
+        try {
+            // The driver's barrier before preSearch (src/query.cpp:900) meets
+            // the workers' first one; preSearch's own closing barrier meets
+            // the one that opens GroupWorker::receiveQuery (src/node.cpp:766).
+            if (MPI_Barrier(MPI_COMM_WORLD) != 0) throw std::runtime_error("GROUP: barrier before preSearch");
+            r->idx->preSearch(nb, workers, block_count, warmup_list, warmup_list_size, &p, scratch_path);
+            const auto t0 = std::chrono::steady_clock::now();
+            r->idx->search(n, q, k, D, reinterpret_cast<idx_t*>(I));
+            *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        } catch (...) {
+            for (auto& t : ranks) t.join();
+            ref_mpi_threads_init(1);
+            throw;
+        }
+        for (auto& t : ranks) t.join();
+        ref_mpi_threads_init(1);
+        omp_set_num_threads(omp_get_num_procs());
+        for (const auto& e : errs)
+            if (!e.empty()) throw std::runtime_error("GROUP worker: " + e);
     });
 }
 

@@ -1,8 +1,7 @@
-// Declarations-only stand-in for MPI, used only to compile the reference's
-// Index.cpp / node.cpp into the oracle library.  The oracle drives the
-// reference's single-process code (ORIGINAL search, add, train, warm-up and
-// the BaseWorker 4-chunk pruning loop); none of those call MPI.  The bodies
-// in ref_mpi_stub.cpp report an error if any MPI routine is reached.
+// Declarations of the MPI subset the reference's Index.cpp / node.cpp call,
+// for compiling them into the oracle library.  The bodies in
+// ref_mpi_threads.cpp run the ranks as threads of one process (the oracle's
+// GROUP-mode baseline); single-process code paths see a one-rank world.
 #pragma once
 typedef int MPI_Comm;
 typedef int MPI_Datatype;
