@@ -604,16 +604,19 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
     p.capq = (int)capq;
     p.metric = h->metric;
     p.prune = 1;
-    if (h->metric == HY_METRIC_IP && (h->opt_level & 1)) {
-        // OPT_TRIANGLE (inner product): the cos-bound window of each
-        // (query, list), from each row's inner product with its centroid.
+    if (h->metric == HY_METRIC_L2 || (h->opt_level & 1)) {
+        // Centroid windows of each (query, list): for L2 always (rows whose
+        // distance to the centroid differs from the query's by more than the
+        // square root of its threshold cannot reach it: an exact prune); for
+        // inner product with OPT_TRIANGLE, the reference's cos-bound window.
         if (!h->c2c_valid) {
             const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
             HY_RET(h->c2c.ensure(rows * sizeof(float)));
             HY_RET(h->c2c_tile.ensure(rows / 32 * sizeof(float2)));
-            HY_CUDA(hy::launch_row_centroid_ip(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(),
-                                               h->list_size.as<int32_t>(), (int)nlist, (int64_t)h->arena_rows,
-                                               h->cent.as<float>(), h->c2c.as<float>(), h->c2c_tile.as<float2>(), s));
+            HY_CUDA(hy::launch_row_centroid(h->L, h->codes.as<float>(), h->list_off.as<int64_t>(),
+                                            h->list_size.as<int32_t>(), (int)nlist, (int64_t)h->arena_rows,
+                                            h->cent.as<float>(), h->metric, h->c2c.as<float>(),
+                                            h->c2c_tile.as<float2>(), s));
             h->c2c_valid = true;
         }
         p.triangle = 1;

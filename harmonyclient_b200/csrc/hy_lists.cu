@@ -139,9 +139,67 @@ __device__ __forceinline__ void block_compute(const float* rowp, const float* qs
     }
 }
 
+// One 32-dimension block sum of one query (qb: its 32 block values) against
+// this lane's row (xr), in dimension order; and of two queries at once, as
+// two independent dependency chains.
+template <bool L2>
+__device__ __forceinline__ float chain1(const float* qb, const float4 (&xr)[8]) {
+    float a = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float4 y = *reinterpret_cast<const float4*>(qb + 4 * c);
+        if (L2) {
+            a = sq_add(a, y.x, xr[c].x);
+            a = sq_add(a, y.y, xr[c].y);
+            a = sq_add(a, y.z, xr[c].z);
+            a = sq_add(a, y.w, xr[c].w);
+        } else {
+            a = ip_add(a, y.x, xr[c].x);
+            a = ip_add(a, y.y, xr[c].y);
+            a = ip_add(a, y.z, xr[c].z);
+            a = ip_add(a, y.w, xr[c].w);
+        }
+    }
+    return a;
+}
+
+template <bool L2>
+__device__ __forceinline__ void chain2(const float* qa, const float* qb, const float4 (&xr)[8], float& a0,
+                                       float& a1) {
+    float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float4 y0 = *reinterpret_cast<const float4*>(qa + 4 * c);
+        const float4 y1 = *reinterpret_cast<const float4*>(qb + 4 * c);
+        if (L2) {
+            s0 = sq_add(s0, y0.x, xr[c].x);
+            s1 = sq_add(s1, y1.x, xr[c].x);
+            s0 = sq_add(s0, y0.y, xr[c].y);
+            s1 = sq_add(s1, y1.y, xr[c].y);
+            s0 = sq_add(s0, y0.z, xr[c].z);
+            s1 = sq_add(s1, y1.z, xr[c].z);
+            s0 = sq_add(s0, y0.w, xr[c].w);
+            s1 = sq_add(s1, y1.w, xr[c].w);
+        } else {
+            s0 = ip_add(s0, y0.x, xr[c].x);
+            s1 = ip_add(s1, y1.x, xr[c].x);
+            s0 = ip_add(s0, y0.y, xr[c].y);
+            s1 = ip_add(s1, y1.y, xr[c].y);
+            s0 = ip_add(s0, y0.z, xr[c].z);
+            s1 = ip_add(s1, y1.z, xr[c].z);
+            s0 = ip_add(s0, y0.w, xr[c].w);
+            s1 = ip_add(s1, y1.w, xr[c].w);
+        }
+    }
+    a0 = s0;
+    a1 = s1;
+}
+
 // Persistent list-major scan.  QG queries per group (<= 32), R bulk-copy
-// slots per warp, LM_WARPS warps.
-template <int QG, int R, bool MULTI>
+// slots per warp, LM_WARPS warps.  Blocks of pitch 32 (MULTI = false) keep
+// each (query, row) partial sum in shared memory and walk the live queries of
+// a tile two at a time; wider blocks keep them in registers.
+template <int QG, int R, bool MULTI, bool L2>
 __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     list_scan_kernel(const __grid_constant__ ListScanParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -150,7 +208,8 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     const size_t slot_floats = static_cast<size_t>(32) * L.max_pitch;
     float* bufs = reinterpret_cast<float*>(smem);
     float* qs = bufs + static_cast<size_t>(LM_WARPS) * R * slot_floats;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(qs + static_cast<size_t>(QG) * L.row_pitch);
+    float* sps = qs + static_cast<size_t>(QG) * L.row_pitch;  // [warp][query][lane] partial sums (pitch 32)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sps + (MULTI ? 0 : static_cast<size_t>(LM_WARPS) * QG * 32));
     __shared__ float s_thr[QG];
     __shared__ float s_lo[QG], s_hi[QG];  // OPT_TRIANGLE: each query's candidate2centroid window
     __shared__ int s_qid[QG];
@@ -166,8 +225,9 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     }
     float* wb = bufs + static_cast<size_t>(warp) * R * slot_floats;
     uint64_t* wbar = bars + warp * R;
-    const bool l2 = p.metric == METRIC_L2;
+    constexpr bool l2 = L2;
     const bool prune = p.prune && l2;
+    float* spw = sps + static_cast<size_t>(warp) * QG * 32 + lane;
     uint32_t iss = 0, con = 0;  // copies issued / consumed by this warp (ring position)
     unsigned long long loaded = 0, computed = 0, possible = 0, possible_sums = 0;
     const int64_t nitems = p.item_off[p.nlist];
@@ -222,28 +282,45 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
             qs[i] = v;
         }
         if (p.triangle) {
-            // The reference's inner-product window (src/Index.cpp:1519-1542):
-            // with s = the query's k-th similarity so far and c = its inner
-            // product with the list's centroid, rows whose candidate2centroid
-            // lies outside [s c - sqrt(1-s^2) sqrt(1-c^2), s c + sqrt(1-s^2)
-            // sqrt(1-c^2)] (no upper limit when s < c) cannot reach s for
-            // unit-norm rows and queries, and are not scanned.  Without a
-            // threshold (s = -inf) or off the unit sphere the bounds are NaN
-            // and nothing is skipped, as in the reference.
             const float* cl = p.cent + static_cast<size_t>(s_list) * L.d;
             for (int j = warp; j < QG; j += LM_WARPS) {
                 float c = 0.0f;
                 if (j < nqv) {
                     const float* qj = p.q + static_cast<size_t>(s_qid[j]) * L.d;
-                    for (int e = lane; e < L.d; e += 32) c = __fmaf_rn(qj[e], cl[e], c);
+                    for (int e = lane; e < L.d; e += 32)
+                        c = l2 ? __fmaf_rn(qj[e] - cl[e], qj[e] - cl[e], c) : __fmaf_rn(qj[e], cl[e], c);
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
                 }
                 if (lane == 0) {
-                    const float sim = -s_thr[j];
-                    const float ss = sqrtf(1.0f - sim * sim), sc = sqrtf(1.0f - c * c);
-                    s_lo[j] = sim * c - ss * sc;
-                    s_hi[j] = sim < c ? INFINITY : sim * c + ss * sc;
+                    if (l2) {
+                        // |q - x| >= | |q - c| - |x - c| |: a row whose distance
+                        // to the centroid lies outside [rq - t, rq + t], t =
+                        // sqrt(threshold), cannot reach the threshold.  Both
+                        // ends are widened by relative margins far above the
+                        // FP32 rounding of these norms and of the scan's
+                        // sums, so no row the exact scan would admit is
+                        // skipped.  No threshold: t = inf, nothing skipped.
+                        const float rq = sqrtf(c);
+                        const float t = sqrtf(s_thr[j]) * 1.0001f + rq * 1e-4f + 1e-6f;
+                        s_lo[j] = (rq - t) * (1.0f - 2e-4f);
+                        s_hi[j] = (rq + t) * (1.0f + 2e-4f);
+                    } else {
+                        // The reference's inner-product window
+                        // (src/Index.cpp:1519-1542): with s = the query's k-th
+                        // similarity so far and c = its inner product with
+                        // the centroid, rows whose candidate2centroid lies
+                        // outside [s c - sqrt(1-s^2) sqrt(1-c^2), s c +
+                        // sqrt(1-s^2) sqrt(1-c^2)] (no upper limit when
+                        // s < c) cannot reach s for unit-norm rows and
+                        // queries.  Without a threshold (s = -inf) or off the
+                        // unit sphere the bounds are NaN and nothing is
+                        // skipped, as in the reference.
+                        const float sim = -s_thr[j];
+                        const float ss = sqrtf(1.0f - sim * sim), sc = sqrtf(1.0f - c * c);
+                        s_lo[j] = sim * c - ss * sc;
+                        s_hi[j] = sim < c ? INFINITY : sim * c + ss * sc;
+                    }
                 }
             }
         }
@@ -335,6 +412,54 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                 if (live == 0u) {
                     dead_tile = tile;
                     if (it_tile == tile) it_tile = -1;  // issue none of its further blocks
+                } else if (!MULTI) {
+                    computed += static_cast<unsigned long long>(__popc(live));
+                    const float* rowp = wb + static_cast<size_t>(slot) * slot_floats + lane * 32;
+                    float4 xr[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        xr[c] = *reinterpret_cast<const float4*>(rowp + 4 * (c ^ (lane & 7)));
+                    const float* qbase = qs + L.boff[b];
+                    const bool first = b == 0, last = b + 1 == L.nb;
+                    const int64_t arow = row0 + 32 * static_cast<int64_t>(tile) + lane;
+                    // This block's sum of query qi is done: add it to the
+                    // running partial, then prune or emit.
+                    auto finish = [&](int qi, float a) {
+                        const float sv = first ? a : __fadd_rn(spw[qi * 32], a);
+                        if (!last) {
+                            spw[qi * 32] = sv;
+                            if (prune && sv > s_thr[qi]) alive &= ~(1u << qi);
+                            return;
+                        }
+                        const float score = l2 ? sv : -sv;
+                        const bool c = ((alive >> qi) & 1u) && score <= s_thr[qi];
+                        const uint32_t bal = __ballot_sync(FULL, c);
+                        if (bal) {
+                            const int qid = s_qid[qi];
+                            int base = 0;
+                            if (lane == 0) base = atomicAdd(&p.cand_cnt[qid], __popc(bal));
+                            base = __shfl_sync(FULL, base, 0);
+                            const int pos = base + __popc(bal & lanemask_lt());
+                            if (c && pos < p.capq)
+                                p.cand[static_cast<size_t>(qid) * p.capq + pos] =
+                                    (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
+                        }
+                    };
+                    uint32_t todo = live;
+                    while (todo) {
+                        const int qa = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        if (todo) {
+                            const int qb = __ffs(todo) - 1;
+                            todo &= todo - 1;
+                            float a0, a1;
+                            chain2<L2>(qbase + qa * L.row_pitch, qbase + qb * L.row_pitch, xr, a0, a1);
+                            finish(qa, a0);
+                            finish(qb, a1);
+                        } else {
+                            finish(qa, chain1<L2>(qbase + qa * L.row_pitch, xr));
+                        }
+                    }
                 } else {
                     computed += static_cast<unsigned long long>(__popc(live));
                     const int P = L.pitch[b];
@@ -461,14 +586,15 @@ __global__ void __launch_bounds__(256) list_topk_kernel(uint64_t* __restrict__ c
     }
 }
 
-// Per arena row: the inner product with its list's centroid (the reference's
-// candidate2centroid, src/Index.cpp:659-667; rows of a list are ordered by it,
-// descending), and per 32-row tile {max, min} over its valid rows.  One warp
-// per tile; lane = row; dimensions in order.
-__global__ void row_centroid_ip_kernel(ArenaLayout L, const float* __restrict__ codes,
-                                       const int64_t* __restrict__ list_off, const int32_t* __restrict__ list_size,
-                                       int nlist, const float* __restrict__ cent, float* __restrict__ c2c,
-                                       float2* __restrict__ c2c_tile) {
+// Per arena row: its inner product with its list's centroid (l2 = false; the
+// reference's candidate2centroid, src/Index.cpp:659-667, by which a list is
+// ordered, descending), or its L2 distance (not squared) to it (l2 = true; a
+// list is ordered by it, ascending); and per 32-row tile {max, min} over its
+// valid rows.  One warp per tile; lane = row.
+__global__ void row_centroid_kernel(ArenaLayout L, const float* __restrict__ codes,
+                                    const int64_t* __restrict__ list_off, const int32_t* __restrict__ list_size,
+                                    int nlist, const float* __restrict__ cent, bool l2, float* __restrict__ c2c,
+                                    float2* __restrict__ c2c_tile) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     // gw enumerates (list, tile of the list): find the list by binary search
@@ -491,9 +617,12 @@ __global__ void row_centroid_ip_kernel(ArenaLayout L, const float* __restrict__ 
         const float* c = cent + static_cast<size_t>(l) * L.d;
         for (int b = 0; b < L.nb; ++b) {
             const int w = L.bstart[b + 1] - L.bstart[b];
-            for (int j = 0; j < w; ++j)
-                v = __fadd_rn(v, __fmul_rn(codes[arena_offset(L, r, b, j)], c[L.bstart[b] + j]));
+            for (int j = 0; j < w; ++j) {
+                const float xv = codes[arena_offset(L, r, b, j)], cv = c[L.bstart[b] + j];
+                v = l2 ? __fmaf_rn(xv - cv, xv - cv, v) : __fadd_rn(v, __fmul_rn(xv, cv));
+            }
         }
+        if (l2) v = sqrtf(v);
     }
     c2c[r] = v;
     float mx = valid ? v : -INFINITY, mn = valid ? v : INFINITY;
@@ -508,22 +637,28 @@ __global__ void row_centroid_ip_kernel(ArenaLayout L, const float* __restrict__ 
 template <int QG, int R, bool MULTI>
 size_t list_scan_smem(const ArenaLayout& L) {
     return static_cast<size_t>(LM_WARPS) * R * 32 * L.max_pitch * 4 + static_cast<size_t>(QG) * L.row_pitch * 4 +
-           static_cast<size_t>(LM_WARPS) * R * 8;
+           (MULTI ? 0 : static_cast<size_t>(LM_WARPS) * QG * 32 * 4) + static_cast<size_t>(LM_WARPS) * R * 8;
+}
+
+template <int QG, int R, bool MULTI, bool L2>
+cudaError_t launch_list_scan_m(const ListScanParams& p, int nsm, cudaStream_t s) {
+    const size_t smem = list_scan_smem<QG, R, MULTI>(p.L);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    auto kern = list_scan_kernel<QG, R, MULTI, L2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LM_WARPS * 32, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = std::max(1, per_sm);
+    kern<<<nsm * per_sm, LM_WARPS * 32, smem, s>>>(p);
+    return cudaGetLastError();
 }
 
 template <int QG, int R, bool MULTI>
 cudaError_t launch_list_scan_t(const ListScanParams& p, int nsm, cudaStream_t s) {
-    const size_t smem = list_scan_smem<QG, R, MULTI>(p.L);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(list_scan_kernel<QG, R, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, list_scan_kernel<QG, R, MULTI>, LM_WARPS * 32, smem);
-    if (e != cudaSuccess) return e;
-    per_sm = std::max(1, per_sm);
-    list_scan_kernel<QG, R, MULTI><<<nsm * per_sm, LM_WARPS * 32, smem, s>>>(p);
-    return cudaGetLastError();
+    return p.metric == METRIC_L2 ? launch_list_scan_m<QG, R, MULTI, true>(p, nsm, s)
+                                 : launch_list_scan_m<QG, R, MULTI, false>(p, nsm, s);
 }
 
 }  // namespace
@@ -535,27 +670,28 @@ bool list_scan_multi(const ArenaLayout& L) {
 }
 
 bool list_scan_fits(const ArenaLayout& L) {
-    if (!list_scan_multi(L)) return list_scan_smem<LM_GROUP, 3, false>(L) <= 227 * 1024;
+    if (!list_scan_multi(L)) return list_scan_smem<LM_GROUP, 2, false>(L) <= 227 * 1024;
     if (L.max_pitch <= 64) return list_scan_smem<LM_GROUP, 2, true>(L) <= 227 * 1024;
     return list_scan_smem<LM_GROUP, 1, true>(L) <= 227 * 1024;
 }
 
 cudaError_t launch_list_scan(const ListScanParams& p, int nsm, cudaStream_t s) {
     if (p.qg != LM_GROUP) return cudaErrorInvalidValue;
-    // Two ring slots per warp while the slots fit (pitch <= 64 floats),
-    // else one; blocks wider than 32 floats take the multi-chunk path.
-    if (!list_scan_multi(p.L)) return launch_list_scan_t<LM_GROUP, 3, false>(p, nsm, s);
+    // Pitch-32 blocks: two ring slots per warp (with the shared-memory
+    // partial sums, two CTAs per SM); wider blocks: two slots while they fit
+    // (pitch <= 64 floats), else one.
+    if (!list_scan_multi(p.L)) return launch_list_scan_t<LM_GROUP, 2, false>(p, nsm, s);
     if (p.L.max_pitch <= 64) return launch_list_scan_t<LM_GROUP, 2, true>(p, nsm, s);
     return launch_list_scan_t<LM_GROUP, 1, true>(p, nsm, s);
 }
 
-cudaError_t launch_row_centroid_ip(const ArenaLayout& L, const float* codes, const int64_t* list_off,
-                                   const int32_t* list_size, int nlist, int64_t arena_rows, const float* cent,
-                                   float* c2c, float2* c2c_tile, cudaStream_t s) {
+cudaError_t launch_row_centroid(const ArenaLayout& L, const float* codes, const int64_t* list_off,
+                                const int32_t* list_size, int nlist, int64_t arena_rows, const float* cent, int metric,
+                                float* c2c, float2* c2c_tile, cudaStream_t s) {
     const int64_t tiles = arena_rows / 32;
     if (tiles < 1) return cudaSuccess;
-    row_centroid_ip_kernel<<<static_cast<int>((tiles * 32 + 255) / 256), 256, 0, s>>>(L, codes, list_off, list_size,
-                                                                                      nlist, cent, c2c, c2c_tile);
+    row_centroid_kernel<<<static_cast<int>((tiles * 32 + 255) / 256), 256, 0, s>>>(
+        L, codes, list_off, list_size, nlist, cent, metric == METRIC_L2, c2c, c2c_tile);
     return cudaGetLastError();
 }
 

@@ -31,8 +31,9 @@ struct ListScanParams {
     int* err;
     int nlist, rs, capq, metric, prune;
     int qg = LM_GROUP;          // queries per group the items were built with
-    // Inner product with OPT_TRIANGLE: per arena row its inner product with
-    // its list's centroid, per 32-row tile {max, min} of those, the centroids.
+    // Centroid windows: per arena row its L2 distance to (L2) or inner
+    // product with (inner product, OPT_TRIANGLE) its list's centroid, per
+    // 32-row tile {max, min} of those, the centroids.
     int triangle = 0;
     const float* c2c = nullptr;
     const float2* c2c_tile = nullptr;
@@ -47,12 +48,13 @@ bool list_scan_multi(const ArenaLayout& L);
 bool list_scan_fits(const ArenaLayout& L);
 // Persistent launch (nsm x the CTAs per SM that fit).
 cudaError_t launch_list_scan(const ListScanParams& p, int nsm, cudaStream_t s);
-// c2c [arena rows] := each valid row's inner product with its list's
-// centroid; c2c_tile [arena rows / 32] := {max, min} over each tile's valid
-// rows (lists start on 32-row tiles).
-cudaError_t launch_row_centroid_ip(const ArenaLayout& L, const float* codes, const int64_t* list_off,
-                                   const int32_t* list_size, int nlist, int64_t arena_rows, const float* cent,
-                                   float* c2c, float2* c2c_tile, cudaStream_t s);
+// c2c [arena rows] := each valid row's L2 distance to (metric L2, not
+// squared) or inner product with (inner product) its list's centroid;
+// c2c_tile [arena rows / 32] := {max, min} over each tile's valid rows
+// (lists start on 32-row tiles).
+cudaError_t launch_row_centroid(const ArenaLayout& L, const float* codes, const int64_t* list_off,
+                                const int32_t* list_size, int nlist, int64_t arena_rows, const float* cent, int metric,
+                                float* c2c, float2* c2c_tile, cudaStream_t s);
 // mode 0: keep each query's k best candidates and lower its threshold to the
 // k-th; mode 1: write the k best as (distance, id) into D / I, listing the
 // queries whose candidates overflowed in ovf (count first) instead.
