@@ -50,15 +50,6 @@ KNOWN_TRAFFIC = {
 }
 
 
-def idx_layout_pitches(d, nb=4):
-    """Padded width (floats, a multiple of 32) of each of the arena's nb
-    dimension blocks: block b spans d // nb dimensions, the last one the
-    remainder."""
-    w = [d // nb] * nb
-    w[-1] += d - sum(w)
-    return [(x + 31) // 32 * 32 for x in w]
-
-
 def peaks():
     """(HBM GB/s, dense bf16 TFLOP/s burst, which) from MEASURED_PEAKS.json,
     else the pool's earlier fallback measurement."""
@@ -510,11 +501,10 @@ def run_ours(args, rank, world, dist):
         if pst.get("list_major"):
             # The list-major scan reads each list once per group of 32
             # queries, so its bound is FP32 issue: 3 FP32 operations (sub,
-            # mul, add) per (query, row, dimension) of every block sum it
-            # executed (32 rows x a block's padded width), against 148 SMs x
-            # 128 FP32 lanes x the SM clock measured during the run.
-            width = sum(idx_layout_pitches(d)) / len(idx_layout_pitches(d))
-            ops = pst["block_sums"] * 32 * width * 3
+            # mul, add) per (query, row, dimension) of every 16-dimension
+            # segment sum it executed (32 rows x 16 dimensions), against
+            # 148 SMs x 128 FP32 lanes x the SM clock measured during the run.
+            ops = pst["seg_sums"] * 32 * 16 * 3
             sm_mhz = (plain["clocks"] or {}).get("sm_mhz") or 1965.0
             fpeak = 148 * 128 * sm_mhz * 1e6 / 1e12
             fach = ops / (scan_ms / 1e3) / 1e12
@@ -523,7 +513,7 @@ def run_ours(args, rank, world, dist):
                      "peak_kind": "nominal FP32 issue (148 SMs x 128 lanes x measured SM clock)",
                      "kernel": "list_scan_kernel", "kernel_ms": round(scan_ms, 4),
                      "launches_per_search": plain["launches"], "executed_ops": int(ops),
-                     "block_sums_executed": round(pst["block_sums"] / max(pst["block_sums_max"], 1), 4),
+                     "seg_sums_executed": round(pst["seg_sums"] / max(pst["seg_sums_max"], 1), 4),
                      "pair_bytes": palg, "pair_bytes_rate_gbs": round(palg / (scan_ms / 1e3) / 1e9, 1),
                      "traffic": KNOWN_TRAFFIC.get((args.workload, "plain-lm", args.nb, args.nq, args.nprobe))}
         else:
@@ -666,8 +656,8 @@ def _scored(x, q, D, I, truth, at, metric=1):
 
 def _plain_work(st):
     """The list-major plain scan's executed share of its unpruned block sums."""
-    if st.get("list_major") and st.get("block_sums_max"):
-        return {"scan": "list-major", "block_sums_executed": round(st["block_sums"] / st["block_sums_max"], 4)}
+    if st.get("list_major") and st.get("seg_sums_max"):
+        return {"scan": "list-major", "seg_sums_executed": round(st["seg_sums"] / st["seg_sums_max"], 4)}
     return {"scan": "query-major"}
 
 
@@ -708,7 +698,8 @@ def extra_c2_hard(args, ts, dev, steps, sigma):
     x, q = datasets.gmm_uint8(nb, args.nq, sigma=sigma, seed=0)
     tq = datasets.gmm_uint8(0, args.train_queries, sigma=sigma, seed=0, query_seed=777)[1]
     k = 10
-    idx = hb.Index(128, 1024, 64, hb.METRIC_L2, device=dev)
+    max_np = 256
+    idx = hb.Index(128, 1024, max_np, hb.METRIC_L2, device=dev)
     idx.train(x)
     idx.add(x)
     idx.preSearch(warmUpSearchList=args.warmup_list, warmUpSearchListSize=k)
@@ -716,16 +707,16 @@ def extra_c2_hard(args, ts, dev, steps, sigma):
     truth["D"], truth["I"] = gb.topk(x, q, 10)
     idx.set_form("bf16")
     sweep = {}
-    for npb in (1, 2, 4, 8, 16, 32, 64):
+    for npb in (1, 2, 4, 8, 16, 32, 64, 128, 256):
         idx.nprobe = npb
         r, D, I, _ = _device_qps(idx, q, k, steps, ts, dev)
         r.update(_scored(x, q, D, I, truth, 10))
         sweep[str(npb)] = r
-    idx.nprobe = 64
+    idx.nprobe = max_np
     learned = {}
     for cov in (0.5, 0.7, 0.8, 0.9, 0.97):
         t0 = time.perf_counter()
-        rep = idx.train_probe_model(tq, max_nprobe=64, k_label=10, epochs=args.epochs, lr=1e-3, coverage=cov)
+        rep = idx.train_probe_model(tq, max_nprobe=max_np, k_label=10, epochs=args.epochs, lr=1e-3, coverage=cov)
         train_s = time.perf_counter() - t0
         idx.set_learned(True, judge_fraction=args.judge_fraction, judge_recall=0.95)
         r, D, I, _ = _device_qps(idx, q, k, steps, ts, dev)
@@ -751,7 +742,8 @@ def extra_c2_hard(args, ts, dev, steps, sigma):
     plain["nprobe"] = target
     return {
         "workload": f"{nb} x 128 uint8-valued gmm (4096 components, sigma {sigma:g}), nlist 1024, k 10, "
-                    f"{q.shape[0]} queries; probe network (max nprobe 64) trained on {tq.shape[0]} other queries",
+                    f"{q.shape[0]} queries; probe network (max nprobe {max_np}) trained on {tq.shape[0]} other "
+                    f"queries",
         "bf16_fixed_nprobe": sweep,
         "learned_bf16_by_coverage": learned,
         "fastest_fixed_at_recall_0.95": {"nprobe": fkey, "qps": fq},
@@ -913,7 +905,7 @@ def main():
     ap.add_argument("--judge-fraction", type=float, default=0.01)
     ap.add_argument("--no-graph", dest="graph", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
-    ap.add_argument("--hard-sigma", type=float, default=120.0,
+    ap.add_argument("--hard-sigma", type=float, default=80.0,
                     help="sigma of the extra 1M x 128 mixture on which the learned probes are compared")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="skip the other nprobes, the sigma-60 mixture and the 1M x 420 workload")

@@ -604,11 +604,13 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
     p.capq = (int)capq;
     p.metric = h->metric;
     p.prune = 1;
-    if (h->metric == HY_METRIC_L2 || (h->opt_level & 1)) {
-        // Centroid windows of each (query, list): for L2 always (rows whose
+    if (h->opt_level & 1) {
+        // OPT_TRIANGLE: centroid windows of each (query, list).  Inner
+        // product: the reference's cos-bound window.  L2 (the reference's L2
+        // triangle is commented out, so its search is unpruned): rows whose
         // distance to the centroid differs from the query's by more than the
-        // square root of its threshold cannot reach it: an exact prune); for
-        // inner product with OPT_TRIANGLE, the reference's cos-bound window.
+        // square root of its threshold cannot reach it, an exact prune that
+        // pays when lists are tight balls around their centroids.
         if (!h->c2c_valid) {
             const size_t rows = std::max<size_t>(h->arena_rows, hy::BATCH_ROW_ALIGN);
             HY_RET(h->c2c.ensure(rows * sizeof(float)));
@@ -1158,8 +1160,8 @@ int finish_host_call(hy_index* h, cudaStream_t s, bool timed, size_t n, size_t n
     h->stats.pairs = n * nprobe;
     h->stats.tile_blocks = st->counters[0];
     h->stats.tile_blocks_max = st->counters[1];
-    h->stats.block_sums = st->counters[2];
-    h->stats.block_sums_max = st->counters[3];
+    h->stats.seg_sums = st->counters[2];
+    h->stats.seg_sums_max = st->counters[3];
     h->stats.launches = h->launches;
     h->launches = 0;
     if (timed) collect_times(h);
@@ -2125,8 +2127,8 @@ int hy_index_last_stats(const hy_index* hc, hy_search_stats_t* out) {
             HY_CUDA(cudaMemcpy(c, h->w_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
             h->stats.tile_blocks = c[0];
             h->stats.tile_blocks_max = c[1];
-            h->stats.block_sums = c[2];
-            h->stats.block_sums_max = c[3];
+            h->stats.seg_sums = c[2];
+            h->stats.seg_sums_max = c[3];
         }
     }
     *out = h->stats;

@@ -139,14 +139,14 @@ __device__ __forceinline__ void block_compute(const float* rowp, const float* qs
     }
 }
 
-// One 32-dimension block sum of one query (qb: its 32 block values) against
-// this lane's row (xr), in dimension order; and of two queries at once, as
-// two independent dependency chains.
-template <bool L2>
-__device__ __forceinline__ float chain1(const float* qb, const float4 (&xr)[8]) {
-    float a = 0.0f;
+// Chunks [C0, C1) (4 dimensions each) of one query's block sum (qb: its 32
+// block values) against this lane's row (xr), continuing from a, in
+// dimension order; and of two queries at once, as two independent
+// dependency chains.
+template <bool L2, int C0, int C1>
+__device__ __forceinline__ float chain1(const float* qb, const float4 (&xr)[8], float a) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+    for (int c = C0; c < C1; ++c) {
         const float4 y = *reinterpret_cast<const float4*>(qb + 4 * c);
         if (L2) {
             a = sq_add(a, y.x, xr[c].x);
@@ -163,12 +163,12 @@ __device__ __forceinline__ float chain1(const float* qb, const float4 (&xr)[8]) 
     return a;
 }
 
-template <bool L2>
+template <bool L2, int C0, int C1>
 __device__ __forceinline__ void chain2(const float* qa, const float* qb, const float4 (&xr)[8], float& a0,
                                        float& a1) {
-    float s0 = 0.0f, s1 = 0.0f;
+    float s0 = a0, s1 = a1;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+    for (int c = C0; c < C1; ++c) {
         const float4 y0 = *reinterpret_cast<const float4*>(qa + 4 * c);
         const float4 y1 = *reinterpret_cast<const float4*>(qb + 4 * c);
         if (L2) {
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                         return;
                     }
                     possible += L.nb;
-                    possible_sums += static_cast<unsigned long long>(L.nb) * nqv;
+                    possible_sums += static_cast<unsigned long long>(L.row_pitch >> 4) * nqv;
                     if (p.triangle) {
                         // A tile whose rows lie outside every query's window
                         // is not loaded.
@@ -413,7 +413,6 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                     dead_tile = tile;
                     if (it_tile == tile) it_tile = -1;  // issue none of its further blocks
                 } else if (!MULTI) {
-                    computed += static_cast<unsigned long long>(__popc(live));
                     const float* rowp = wb + static_cast<size_t>(slot) * slot_floats + lane * 32;
                     float4 xr[8];
 #pragma unroll
@@ -445,23 +444,49 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                                     (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(arow);
                         }
                     };
+                    // After the first 16 dimensions: a query none of whose
+                    // live rows can stay under its threshold (the partial,
+                    // which only grows, already exceeds it) is dropped from
+                    // the tile without the block's other 16 dimensions.
+                    auto half_dead = [&](int qi, float a) -> bool {
+                        if (!prune) return false;
+                        const float lb = first ? a : __fadd_rn(spw[qi * 32], a);
+                        const bool dead = !((alive >> qi) & 1u) || lb > s_thr[qi];
+                        if (!__all_sync(FULL, dead)) return false;
+                        alive &= ~(1u << qi);
+                        return true;
+                    };
                     uint32_t todo = live;
                     while (todo) {
                         const int qa = __ffs(todo) - 1;
                         todo &= todo - 1;
+                        const float* ya = qbase + qa * L.row_pitch;
                         if (todo) {
                             const int qb = __ffs(todo) - 1;
                             todo &= todo - 1;
-                            float a0, a1;
-                            chain2<L2>(qbase + qa * L.row_pitch, qbase + qb * L.row_pitch, xr, a0, a1);
-                            finish(qa, a0);
-                            finish(qb, a1);
+                            const float* yb = qbase + qb * L.row_pitch;
+                            float a0 = 0.0f, a1 = 0.0f;
+                            chain2<L2, 0, 4>(ya, yb, xr, a0, a1);
+                            const bool da = half_dead(qa, a0), db = half_dead(qb, a1);
+                            computed += 4 - (da ? 1 : 0) - (db ? 1 : 0);
+                            if (!da && !db) {
+                                chain2<L2, 4, 8>(ya, yb, xr, a0, a1);
+                                finish(qa, a0);
+                                finish(qb, a1);
+                            } else if (!da) {
+                                finish(qa, chain1<L2, 4, 8>(ya, xr, a0));
+                            } else if (!db) {
+                                finish(qb, chain1<L2, 4, 8>(yb, xr, a1));
+                            }
                         } else {
-                            finish(qa, chain1<L2>(qbase + qa * L.row_pitch, xr));
+                            const float a0 = chain1<L2, 0, 4>(ya, xr, 0.0f);
+                            const bool da = half_dead(qa, a0);
+                            computed += da ? 1 : 2;
+                            if (!da) finish(qa, chain1<L2, 4, 8>(ya, xr, a0));
                         }
                     }
                 } else {
-                    computed += static_cast<unsigned long long>(__popc(live));
+                    computed += static_cast<unsigned long long>(__popc(live)) * (L.pitch[b] >> 4);
                     const int P = L.pitch[b];
                     const float* rowp = wb + static_cast<size_t>(slot) * slot_floats + lane * P;
                     block_compute<QG, MULTI>(rowp, qs, L.row_pitch, L.boff[b], P, b == 0, l2, live, sp, lane);

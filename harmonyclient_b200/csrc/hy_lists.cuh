@@ -27,7 +27,9 @@ struct ListScanParams {
     uint64_t* cand;             // [nq][capq] candidate keys (ordered score << 32 | arena row)
     int32_t* cand_cnt;          // [nq]
     unsigned int* work;         // work-queue counter (zero before the launch)
-    unsigned long long* counters;  // [4]: block copies, blocks without pruning, (block, query) sums, sums without pruning
+    // [4]: block copies, block copies without pruning, executed (query,
+    // 32-row tile, 16-dimension segment) partial sums, and those without pruning
+    unsigned long long* counters;
     int* err;
     int nlist, rs, capq, metric, prune;
     int qg = LM_GROUP;          // queries per group the items were built with

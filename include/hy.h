@@ -108,8 +108,9 @@ typedef struct {
                                  bf16: batched_scan_kernel, both passes) in the last query chunk */
     uint64_t kernel_launches; /* launches kernel_ms covers */
     uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
-    uint64_t block_sums;      /* list-major plain scan: (query, 32-row x one-dim-block) partial sums computed */
-    uint64_t block_sums_max;  /* list-major plain scan: the partial sums a scan without pruning computes */
+    uint64_t seg_sums;        /* list-major plain scan: (query, 32-row tile, 16-dimension segment) partial
+                                 sums computed: 32 x 16 x 3 FP32 operations each */
+    uint64_t seg_sums_max;    /* list-major plain scan: the segment sums a scan without pruning computes */
     uint64_t list_major;      /* plain form: 1 when the search ran the list-major scan */
 } hy_search_stats_t;
 
@@ -153,9 +154,13 @@ HY_API int hy_index_set_nprobe(hy_index* h, size_t nprobe);
  * (src/Index.cpp:1509-1546), built from the query's k-th similarity so far;
  * for unit-norm rows and queries the skipped rows cannot reach the top-k, so
  * the answer is the exact scan's, as in the reference.  The list-major scan
- * applies the window; the query-major scan scans every row.  The L2 triangle
- * and the sub-NN levels change nothing in the reference's search (their scan
- * code is commented out, src/Index.cpp:1468-1492, src/IVFScan.hpp:223-427)
+ * applies the window; the query-major scan scans every row.  With L2,
+ * OPT_TRIANGLE makes the list-major scan skip the rows whose distance to
+ * their centroid differs from the query's by more than the square root of
+ * its threshold (|q - x| >= | |q - c| - |x - c| |, an exact prune with margins
+ * for FP32 rounding): the answer is unchanged, as in the reference, whose L2
+ * triangle code is commented out (src/Index.cpp:1468-1492).  The sub-NN
+ * levels change nothing in the reference's search (src/IVFScan.hpp:223-427)
  * and nothing here. */
 HY_API int hy_index_set_opt_level(hy_index* h, int opt_level);
 

@@ -57,7 +57,7 @@ def test_list_major_equals_query_major_on_golden_cases(name):
     qm, lm = _both(idx, q, c["k"])
     _equal(qm, lm)
     st = lm[2]
-    assert st["block_sums"] > 0 and st["tile_blocks"] > 0
+    assert st["seg_sums"] > 0 and st["tile_blocks"] > 0
 
 
 @pytest.mark.parametrize("d,metric", [(200, 1), (420, 1), (200, 0)])
@@ -86,7 +86,7 @@ def test_k_range_with_warmup(k):
     # the warm-up and first-pass thresholds prune: fewer block sums than
     # (query, tile, block) triples
     st = lm[2]
-    assert 0 < st["block_sums"] < st["block_sums_max"]
+    assert 0 < st["seg_sums"] < st["seg_sums_max"]
 
 
 def test_per_query_nprobe():
@@ -165,5 +165,29 @@ def test_ip_triangle_window_matches_reference():
     assert_topk_equal(g["D"], g["I"], D1, I1, rtol=1e-5, metric=0, skip_rows=tied)
     assert_topk_equal(D0, I0, D1, I1, rtol=1e-5, metric=0)
     # the window skipped most of the probed rows' work
-    assert st1["block_sums"] < 0.5 * st0["block_sums"], (st1["block_sums"], st0["block_sums"])
+    assert st1["seg_sums"] < 0.5 * st0["seg_sums"], (st1["seg_sums"], st0["seg_sums"])
+    assert st1["tile_blocks"] < st0["tile_blocks"]
+
+
+def test_l2_triangle_window_changes_no_answer():
+    """L2 with OPT_TRIANGLE: the list-major scan skips rows whose distance to
+    their centroid is too far from the query's (an exact prune); the answer
+    is the same bit for bit, and on tight clusters work is skipped."""
+    c = cases.CASES["ip_tri"]
+    x, q = cases.data("ip_tri")  # tight clusters, one per list
+    idx = hb.Index(c["d"], c["nlist"], c["nprobe"], hb.METRIC_L2)
+    idx.train(x)
+    idx.add(x)
+    idx.set_plain_scan("list")
+    try:
+        D0, I0 = idx.search(q, c["k"])
+        st0 = idx.last_stats()
+        idx.opt_level = hb.OPT_TRIANGLE
+        D1, I1 = idx.search(q, c["k"])
+        st1 = idx.last_stats()
+    finally:
+        idx.opt_level = hb.OPT_NONE
+        idx.set_plain_scan("auto")
+    np.testing.assert_array_equal(I1, I0)
+    np.testing.assert_array_equal(D1, D0)
     assert st1["tile_blocks"] < st0["tile_blocks"]

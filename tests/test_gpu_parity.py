@@ -109,7 +109,7 @@ def test_search_with_warmup_threshold_is_exact(name, scan):
     assert_topk_equal(g["D"], g["I"], D, I, rtol=0.0 if name == "int_small" else 1e-5, skip_rows=tied)
     if scan == "list":
         assert st["list_major"] == 1
-        assert st["block_sums"] < st["block_sums_max"], "pruning should skip some partial sums"
+        assert st["seg_sums"] < st["seg_sums_max"], "pruning should skip some partial sums"
     else:
         assert st["list_major"] == 0
         assert st["tile_blocks"] < st["tile_blocks_max"], "pruning should skip some dimension blocks"
