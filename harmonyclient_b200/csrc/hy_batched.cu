@@ -1371,13 +1371,6 @@ __global__ void coarse_items_kernel(int nq, int nlist, int64_t rows, int ngroups
 // Staging row pitch of coarse_refine_kernel (floats): d + 4 when d is a
 // multiple of 4 (16-byte rows), else d + 1 (conflict-free column reads).
 __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4 : d + 1; }
-// Shared memory of one refine warp: a 256-bin histogram and the query, plus
-// 32 staged centroid rows when d is not a multiple of 4 (with d a multiple
-// of 4 the rows are read from global memory, coarse_score_direct).
-__host__ __device__ inline size_t refine_warp_bytes(int d) {
-    const int pitch = refine_pitch(d);
-    return 1024 + static_cast<size_t>(pitch) * 4 + ((d & 3) == 0 ? 0 : static_cast<size_t>(32) * pitch * 4);
-}
 
 // Exact coarse selection from the tensor-core scores.  Per query (one warp):
 // cand holds nlist {score, error bound} pairs (held in registers, PER per
@@ -1397,63 +1390,6 @@ __host__ __device__ inline size_t refine_warp_bytes(int d) {
 // a multiple of 4 the copies and reads are 16 bytes wide, row pitch d + 4, so
 // a 512-byte warp read takes the minimum four wavefronts), then ordered by
 // (score, centroid) and written as select_warp_kernel writes them.
-// The exact coarse score of each of the c candidate centroids listed in
-// keys (written back as (score, centroid) keys), for d a multiple of 4: the
-// centroid rows are read from global memory (L1 / L2) with 16-byte loads,
-// and each lane runs up to four candidates (e, e + 32, e + 64, e + 96) as
-// independent dependency chains, each a sequential sum in dimension order
-// (the arithmetic of coarse_scores_kernel).  No shared-memory staging, so
-// many more warps fit on an SM than with the staged rounds.
-template <int METRIC>
-__device__ inline void coarse_score_direct(uint64_t* keys, int c, const float* qs, const float* __restrict__ cent,
-                                           int d, int lane) {
-    for (int g0 = 0; g0 < c; g0 += 128) {
-        int cid[4];
-        bool ok[4];
-        const float4* rowp[4];
-        float acc[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int e = g0 + r * 32 + lane;
-            ok[r] = e < c;
-            cid[r] = ok[r] ? static_cast<int>(keys[e]) : 0;
-            rowp[r] = reinterpret_cast<const float4*>(cent + static_cast<size_t>(cid[r]) * d);
-            acc[r] = 0.0f;
-        }
-        const int nr = min(4, (c - g0 + 31) >> 5);  // warp-uniform: rounds with a candidate
-#pragma unroll 2
-        for (int jj = 0; jj < (d >> 2); ++jj) {
-            const float4 a = *reinterpret_cast<const float4*>(qs + 4 * jj);
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                if (r < nr) {
-                    const float4 b = ok[r] ? __ldg(rowp[r] + jj) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (METRIC == METRIC_L2) {
-                        acc[r] = sq_add(acc[r], a.x, b.x);
-                        acc[r] = sq_add(acc[r], a.y, b.y);
-                        acc[r] = sq_add(acc[r], a.z, b.z);
-                        acc[r] = sq_add(acc[r], a.w, b.w);
-                    } else {
-                        acc[r] = ip_add(acc[r], a.x, b.x);
-                        acc[r] = ip_add(acc[r], a.y, b.y);
-                        acc[r] = ip_add(acc[r], a.z, b.z);
-                        acc[r] = ip_add(acc[r], a.w, b.w);
-                    }
-                }
-            }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            if (ok[r]) {
-                const float score = METRIC == METRIC_L2 ? acc[r] : -acc[r];
-                keys[g0 + r * 32 + lane] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cid[r]);
-            }
-        }
-        __syncwarp();
-    }
-}
-
 template <int METRIC>
 __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs, float* stage, int pitch,
                                          const float* __restrict__ cent, int d, int m, int qi,
@@ -1465,8 +1401,7 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
         if (out_score) out_score[static_cast<int64_t>(qi) * m + e] = FLT_MAX;
     }
     const bool v4 = (d & 3) == 0;
-    if (stage == nullptr) coarse_score_direct<METRIC>(keys, c, qs, cent, d, lane);
-    for (int c0 = 0; stage != nullptr && c0 < c; c0 += 32) {
+    for (int c0 = 0; c0 < c; c0 += 32) {
         const int nr = min(32, c - c0);
         const int cidr = lane < nr ? static_cast<int>(keys[c0 + lane]) : 0;
         for (int r = 0; r < nr; ++r) {
@@ -1578,11 +1513,11 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pitch = refine_pitch(d);
-    const size_t per_warp = refine_warp_bytes(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
     unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
     int* hist = reinterpret_cast<int*>(base);
     float* qs = reinterpret_cast<float*>(hist + 256);
-    float* stage = (d & 3) == 0 ? nullptr : qs + pitch;
+    float* stage = qs + pitch;
     const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
     if (qi >= nq) return;  // whole warp
     const float* qrow = q + static_cast<size_t>(qi) * d;
@@ -1667,11 +1602,11 @@ __global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __res
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pitch = refine_pitch(d);
-    const size_t per_warp = refine_warp_bytes(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
     unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
     int* hist = reinterpret_cast<int*>(base);
     float* qs = reinterpret_cast<float*>(hist + 256);
-    float* stage = (d & 3) == 0 ? nullptr : qs + pitch;
+    float* stage = qs + pitch;
     const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
     if (qi >= nq) return;  // whole warp
     const float* qrow = q + static_cast<size_t>(qi) * d;
@@ -2079,8 +2014,9 @@ cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int
 }
 
 size_t coarse_refine_smem(int nlist, int d, int warps) {
+    const int pitch = refine_pitch(d);
     (void)nlist;
-    const size_t per_warp = refine_warp_bytes(d);
+    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
     return static_cast<size_t>(warps) * ((per_warp + 15) & ~size_t(15));
 }
 
