@@ -1276,63 +1276,15 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
 }
 
 // Queries whose first-pass list was scanned densely, one warp each.
-// Dense tightening with the query's pairs cached in shared memory: one
-// coalesced read from global memory fills the warp's cache, and the minimum /
-// maximum, both radix passes and the rewrite read the cache (the rewrite
-// writes the keys to the global buffer, which the cache no longer aliases).
-// Queries with more than DENSE_CACHE pairs take tighten_dense_query's
-// streaming passes.
-constexpr int DENSE_CACHE = 2048;
-constexpr int DENSE_WARPS = 4;
-
-__global__ void __launch_bounds__(DENSE_WARPS * 32) tighten_dense_kernel(int nq, BatchWork w, int capq, int k,
-                                                                         float* __restrict__ thr, DenseFirst df) {
-    extern __shared__ __align__(16) unsigned char dsm[];
+__global__ void __launch_bounds__(256) tighten_dense_kernel(int nq, BatchWork w, int capq, int k,
+                                                            float* __restrict__ thr, DenseFirst df) {
+    __shared__ int hist[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* hist = reinterpret_cast<int*>(dsm) + warp * 256;
-    float2* cache = reinterpret_cast<float2*>(dsm + DENSE_WARPS * 256 * sizeof(int)) + warp * DENSE_CACHE;
-    const int qi = blockIdx.x * DENSE_WARPS + warp;
+    const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
     const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
     if (l0 < 0 || df.list_size[l0] > df.dense_max) return;
-    const int cnt = w.cand_cnt[qi];
-    const int64_t row0 = df.list_off[l0];
-    if (cnt > DENSE_CACHE) {
-        tighten_dense_query(qi, cnt, row0, w, capq, k, thr, hist, lane);
-        return;
-    }
-    uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
-    const float2* ce = reinterpret_cast<const float2*>(cq);
-    for (int base = 0; base < cnt; base += 256) {  // eight loads in flight per lane
-        float2 v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int e = base + i * 32 + lane;
-            v[i] = e < cnt ? ce[e] : make_float2(0.0f, 0.0f);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int e = base + i * 32 + lane;
-            if (e < cnt) cache[e] = v[i];
-        }
-    }
-    __syncwarp();
-    const float U = cnt >= k ? kth_bound_stream([cache](int e) { return cache[e]; }, cnt, k, hist, lane) : INFINITY;
-    int m = 0;
-    for (int base = 0; base < cnt; base += 32) {
-        const int e = base + lane;
-        const float2 v = e < cnt ? cache[e] : make_float2(0.0f, 0.0f);
-        const bool keep = e < cnt && v.x - v.y <= U;
-        const unsigned b = __ballot_sync(FULL, keep);
-        if (keep)
-            cq[m + __popc(b & ((1u << lane) - 1u))] =
-                (static_cast<uint64_t>(f2o(v.x)) << 32) | static_cast<uint32_t>(row0 + e);
-        m += __popc(b);
-    }
-    if (lane == 0) {
-        w.cand_cnt[qi] = m;
-        if (U < thr[qi]) thr[qi] = U;
-    }
+    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], w, capq, k, thr, hist[warp], lane);
 }
 
 // Queries with 1025..2048 candidates (w.big), one warp each.
@@ -2014,12 +1966,7 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.big2, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     if (df.dense_max > 0) {
-        const size_t dsmem = static_cast<size_t>(DENSE_WARPS) * (256 * sizeof(int) + DENSE_CACHE * sizeof(float2));
-        if ((e = cudaFuncSetAttribute(tighten_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(dsmem))) != cudaSuccess)
-            return e;
-        tighten_dense_kernel<<<(nq + DENSE_WARPS - 1) / DENSE_WARPS, DENSE_WARPS * 32, dsmem, s>>>(nq, w, capq, k,
-                                                                                                thr, df);
+        tighten_dense_kernel<<<(nq + 7) / 8, 256, 0, s>>>(nq, w, capq, k, thr, df);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
