@@ -37,16 +37,25 @@ METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan 
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu
-# captures of this script (dram__bytes_read.sum + dram__bytes_write.sum; the
-# capture commands are listed in profiles/), keyed by (workload, form, nb, nq,
-# nprobe).
-# The plain entry is a 1,000-query capture scaled by 10 to the 10,000-query
-# launch (traffic grows with the query count: every query streams its own
-# probed lists).
+# captures of this script (dram__bytes_read.sum + dram__bytes_write.sum),
+# keyed by (workload, form, nb, nq, nprobe), with the capture each comes
+# from (the summaries and commands are in profiles/).  A line whose
+# configuration has no capture reports traffic null.
 KNOWN_TRAFFIC = {
     ("c2", "plain", 1_000_000, 10_000, 64): 216_530_000_000,
+    ("c2", "plain-lm", 1_000_000, 10_000, 64): 492_300_000,
     ("c2", "learned", 1_000_000, 10_000, 64): 295_400_000,
     ("c2", "bf16", 1_000_000, 10_000, 64): 325_000_000,
+}
+TRAFFIC_SOURCE = {
+    "plain": "query-major scan_plain_kernel, 1,000-query ncu capture scaled x10 "
+             "(profiles/scan_plain_kernel_c2_1M_nprobe64.md)",
+    "plain-lm": "list_scan_kernel, average of the two passes of one 10,000-query search, ncu --set full "
+                "(profiles/list_scan_kernel_c2_1M_nprobe64.md)",
+    "learned": "batched_scan_kernel, average of the two passes of one 10,000-query search "
+               "(profiles/batched_scan_kernel_c2_learned.md)",
+    "bf16": "batched_scan_kernel, average of the two passes, nprobe 64 "
+            "(profiles/batched_scan_kernel_c2_bf16_nprobe64.md)",
 }
 
 
@@ -448,15 +457,9 @@ def run_ours(args, rank, world, dist):
     learned_probes = int((P_main >= 0).sum())
     rows_main = pair_rows(P_main)
     if base == "plain":
-        # Algorithmic bytes of one scan launch: every (query, probed row)
-        # pair's row, d x 4 bytes, plus the queries and the results.
         alg = rows_main * d * 4 + q.shape[0] * d * 4 + q.shape[0] * k * 12
-        ach = alg / (kern_ms / 1e3) / 1e9
-        roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb,
-                                                                               args.nq, args.nprobe)),
-                "peak_kind": peak_kind, "kernel": "scan_plain_kernel", "kernel_ms": round(kern_ms, 4),
-                "algorithmic_bytes": alg}
+        roof = plain_roofline(idx.last_stats(), kern_ms * kern_per_search, kern_per_search, alg, clocks, args,
+                              hbm_peak, peak_kind)
     else:
         # One batched-scan launch does a 2d-flop bf16 inner product per
         # (query, probed row) pair of its pass and reads each list that some
@@ -479,6 +482,7 @@ def run_ours(args, rank, world, dist):
             roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
                     "frac": round(ach / hbm_peak, 4)}
         roof.update({"traffic": KNOWN_TRAFFIC.get((args.workload, args.form, args.nb, args.nq, args.nprobe)),
+                     "traffic_source": TRAFFIC_SOURCE.get(args.form),
                      "peak_kind": peak_kind, "kernel": "batched_scan_kernel", "kernel_ms": round(kern_ms, 4),
                      "algorithmic_flops": int(flops), "algorithmic_bytes": int(lbytes),
                      "launches_per_search": kern_per_search})
@@ -498,30 +502,7 @@ def run_ours(args, rank, world, dist):
         scan_ms = plain["kernel_ms"] * plain["launches"]  # every scan launch of one search
         sc_plain, _ = _score(x, q, plain["D"], plain["I"], args.recall_sample, truth)
         pv = world * q.shape[0] * args.plain_steps / (plain["ms"] / 1e3)
-        if pst.get("list_major"):
-            # The list-major scan reads each list once per group of 32
-            # queries, so its bound is FP32 issue: 3 FP32 operations (sub,
-            # mul, add) per (query, row, dimension) of every 16-dimension
-            # segment sum it executed (32 rows x 16 dimensions), against
-            # 148 SMs x 128 FP32 lanes x the SM clock measured during the run.
-            ops = pst["seg_sums"] * 32 * 16 * 3
-            sm_mhz = (plain["clocks"] or {}).get("sm_mhz") or 1965.0
-            fpeak = 148 * 128 * sm_mhz * 1e6 / 1e12
-            fach = ops / (scan_ms / 1e3) / 1e12
-            proof = {"bound": "fp32", "achieved": round(fach, 2), "peak": round(fpeak, 2), "unit": "TFLOP/s",
-                     "frac": round(fach / fpeak, 4),
-                     "peak_kind": "nominal FP32 issue (148 SMs x 128 lanes x measured SM clock)",
-                     "kernel": "list_scan_kernel", "kernel_ms": round(scan_ms, 4),
-                     "launches_per_search": plain["launches"], "executed_ops": int(ops),
-                     "seg_sums_executed": round(pst["seg_sums"] / max(pst["seg_sums_max"], 1), 4),
-                     "pair_bytes": palg, "pair_bytes_rate_gbs": round(palg / (scan_ms / 1e3) / 1e9, 1),
-                     "traffic": KNOWN_TRAFFIC.get((args.workload, "plain-lm", args.nb, args.nq, args.nprobe))}
-        else:
-            pach = palg / (scan_ms / 1e3) / 1e9
-            proof = {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
-                     "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb, args.nq, args.nprobe)),
-                     "kernel": "scan_plain_kernel", "kernel_ms": round(scan_ms, 4), "algorithmic_bytes": palg}
+        proof = plain_roofline(pst, scan_ms, plain["launches"], palg, plain["clocks"], args, hbm_peak, peak_kind)
         plain_line = {"value": round(pv, 1), "unit": "queries/s", "steps": args.plain_steps,
                       "ms_per_step": round(plain["ms"] / args.plain_steps, 3),
                       "recall_at_10": round(sc_plain["recall"], 4),
@@ -631,6 +612,36 @@ def run_ours(args, rank, world, dist):
 # and the 1M x 420 precision workload at k 10 and 100.  Each is timed with
 # CUDA events on the device-pointer API (graph mode) and scored against a
 # float64 brute force over every query.
+def plain_roofline(st, scan_ms, launches, palg, clocks, args, hbm_peak, peak_kind):
+    """Roofline of the plain form's scan over one search (scan_ms: every scan
+    launch of the search).  List-major: executed FP32 operations (3 x 32 x 16
+    per executed (query, 32-row tile, 16-dimension segment) partial sum,
+    `seg_sums`) against 148 SMs x 128 FP32 lanes x the SM clock measured
+    during the run; the lists are read once per group of 32 queries, mostly
+    from L2, so the pair bytes are reported beside it, not as a fraction.
+    Query-major: pair bytes (every probed row of every query, d x 4 bytes,
+    plus queries and results) against the measured copy bandwidth."""
+    if st.get("list_major"):
+        ops = st["seg_sums"] * 32 * 16 * 3
+        sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        fpeak = 148 * 128 * sm_mhz * 1e6 / 1e12
+        fach = ops / (scan_ms / 1e3) / 1e12
+        return {"bound": "fp32", "achieved": round(fach, 2), "peak": round(fpeak, 2), "unit": "TFLOP/s",
+                "frac": round(fach / fpeak, 4),
+                "peak_kind": "nominal FP32 issue (148 SMs x 128 lanes x measured SM clock)",
+                "kernel": "list_scan_kernel", "kernel_ms": round(scan_ms, 4), "launches_per_search": launches,
+                "executed_ops": int(ops), "seg_sums_executed": round(st["seg_sums"] / max(st["seg_sums_max"], 1), 4),
+                "pair_bytes": palg, "pair_bytes_rate_gbs": round(palg / (scan_ms / 1e3) / 1e9, 1),
+                "traffic": KNOWN_TRAFFIC.get((args.workload, "plain-lm", args.nb, args.nq, args.nprobe)),
+                "traffic_source": TRAFFIC_SOURCE["plain-lm"]}
+    pach = palg / (scan_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": round(pach, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(pach / hbm_peak, 4), "peak_kind": peak_kind,
+            "traffic": KNOWN_TRAFFIC.get((args.workload, "plain", args.nb, args.nq, args.nprobe)),
+            "traffic_source": TRAFFIC_SOURCE["plain"],
+            "kernel": "scan_plain_kernel", "kernel_ms": round(scan_ms, 4), "algorithmic_bytes": palg}
+
+
 def _device_qps(idx, q, k, steps, ts, dev):
     """queries/s of `steps` device-pointer searches after two untimed ones,
     with the last answer, the stats of the last search and ms per step."""

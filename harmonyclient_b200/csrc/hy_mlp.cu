@@ -148,8 +148,8 @@ __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __res
 // Inference on the tensor cores.  The weights are packed once (mlp_pack) into
 // the tcgen05 B-operand image: W1 as 256 rows (output features) x 64 inputs,
 // one 128-byte-swizzled K-major k-block of 32 KiB; W2 as 256 rows x 256
-// inputs, four such k-blocks.  One CTA of 256 threads takes 128 queries
-// (query = TMEM lane; two threads per query split every layer's 256 columns):
+// inputs, four such k-blocks.  One CTA of 512 threads takes 128 queries
+// (query = TMEM lane; four threads per query split every layer's 256 columns):
 // features -> bf16 A tile -> MMA (M 128, N 256,
 // K 64) -> bias + GELU -> bf16 A tiles (4 k-blocks) -> MMA (K 256) -> bias +
 // GELU -> dot with W3 -> nprobe, all on chip.
@@ -181,7 +181,9 @@ __device__ inline uint4 pack8_bf16(const float* v) {
     return r;
 }
 
-__global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
+constexpr int MI_QUARTERS = 4;  // threads per query row (column quarters of every 256-wide layer)
+
+__global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
                                                            const float* __restrict__ mu, const float* __restrict__ sd,
                                                            const unsigned char* __restrict__ wimg,
                                                            const float* __restrict__ params, float margin,
@@ -195,10 +197,11 @@ __global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restri
     __shared__ uint64_t bar_w, bar_m;
     __shared__ uint32_t tbase;
     __shared__ int s_ok;
-    __shared__ float s_part[128];  // layer-3 partial sums of the upper column half
-    // Two threads per query row: warps w and w + 4 share TMEM lane quadrant
-    // w % 4 and take column halves 0 / 1 of every 256-wide layer.
-    const int warp = threadIdx.x >> 5, half = warp >> 2;
+    __shared__ float s_part[MI_QUARTERS - 1][128];  // layer-3 partial sums of column quarters 1..3
+    // Four threads per query row: warps w, w + 4, w + 8, w + 12 share TMEM
+    // lane quadrant w % 4 and take column quarters 0..3 (one 64-column
+    // k-block each) of every 256-wide layer.
+    const int warp = threadIdx.x >> 5, qt = warp >> 2;
     const int tid = threadIdx.x & 127;  // the query row within the tile
     const int row = blockIdx.x * 128 + tid;
     const bool valid = row < m;
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restri
         const float s0 = valid ? sc[0] : 0.0f;
         const float a0 = fabsf(s0) + 1e-6f;
 #pragma unroll
-        for (int c = 4 * half; c < 4 * half + 4; ++c) {
+        for (int c = 2 * qt; c < 2 * qt + 2; ++c) {
             float f[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -256,8 +259,9 @@ __global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restri
     const uint32_t lane_addr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
     if (ok) {
         // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks
-        // (this thread's column half: k-blocks 2*half, 2*half + 1).
-        for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
+        // (this thread's column quarter: k-block qt).
+        {
+            const int cb = qt;
             uint32_t u[64];
             tc::tmem_ld64(lane_addr + cb * 64, u);
 #pragma unroll
@@ -289,8 +293,9 @@ __global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restri
     tc::fence_after_sync();
     if (ok) {
         // Layer 2 epilogue and layer 3: y = bf16(GELU(Z2 + b2)) . bf16(W3) + b3,
-        // each thread over its column half.
-        for (int cb = 2 * half; cb < 2 * half + 2; ++cb) {
+        // each thread over its column quarter.
+        {
+            const int cb = qt;
             uint32_t u[64];
             tc::tmem_ld64(lane_addr + cb * 64, u);
 #pragma unroll
@@ -300,11 +305,11 @@ __global__ void __launch_bounds__(256, 1) mlp_infer_kernel(const float* __restri
                 acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
             }
         }
-        if (half == 1) s_part[tid] = acc;
+        if (qt > 0) s_part[qt - 1][tid] = acc;
     }
     __syncthreads();
-    if (ok && half == 0) {
-        const float y = (acc + s_part[tid]) + params[MLP_B3];
+    if (ok && qt == 0) {
+        const float y = (((acc + s_part[0][tid]) + s_part[1][tid]) + s_part[2][tid]) + params[MLP_B3];
         if (valid) {
             if (yout) yout[row] = y;
             if (probes) {
@@ -404,8 +409,8 @@ cudaError_t mlp_infer(const float* pscore, int m, int P, const float* mu, const 
     if (m <= 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MI_SMEM);
     if (e != cudaSuccess) return e;
-    mlp_infer_kernel<<<blocks(m, 128), 256, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin, probes, total,
-                                                         yout, err);
+    mlp_infer_kernel<<<blocks(m, 128), 128 * MI_QUARTERS, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin,
+                                                                        probes, total, yout, err);
     return cudaGetLastError();
 }
 

@@ -191,3 +191,45 @@ def test_l2_triangle_window_changes_no_answer():
     np.testing.assert_array_equal(I1, I0)
     np.testing.assert_array_equal(D1, D0)
     assert st1["tile_blocks"] < st0["tile_blocks"]
+
+
+@pytest.mark.parametrize("case", ["empty_lists", "one_query", "one_list", "k_beyond_rows", "odd_batch"])
+def test_edge_cases_equal_query_major(case):
+    rng = np.random.default_rng(41)
+    if case == "empty_lists":
+        # centroids far from every row leave most lists empty
+        x = rng.integers(0, 50, (3_000, 32)).astype(np.float32)
+        cent = np.vstack([x[:5], np.full((59, 32), 1e4, np.float32) + rng.random((59, 32)).astype(np.float32)])
+        idx = hb.Index(32, 64, 16)
+        idx.centroid_codes = cent
+        idx.add(x)
+        q, k = x[::7][:300], 10
+    elif case == "one_query":
+        x, q = datasets.gmm_uint8(20_000, 1, d=64, ncomp=64, seed=42)
+        idx = hb.Index(64, 32, 32)
+        idx.train(x)
+        idx.add(x)
+        k = 20
+    elif case == "one_list":
+        x, q = datasets.gmm_uint8(5_000, 200, d=48, ncomp=8, seed=43)
+        idx = hb.Index(48, 1, 1)
+        idx.train(x)
+        idx.add(x)
+        k = 50
+    elif case == "k_beyond_rows":
+        x, q = datasets.gmm_uint8(2_000, 100, d=16, ncomp=16, seed=44)
+        idx = hb.Index(16, 64, 2)
+        idx.train(x)
+        idx.add(x)
+        k = 256
+    else:
+        x, q = datasets.gmm_uint8(30_000, 333, d=96, ncomp=128, seed=45)
+        idx = hb.Index(96, 48, 12)
+        idx.train(x)
+        idx.add(x)
+        idx.preSearch(warmUpSearchList=10, warmUpSearchListSize=7)
+        k = 7
+    qm, lm = _both(idx, q, k)
+    _equal(qm, lm)
+    if case == "k_beyond_rows":
+        assert (lm[1][:, -1] == -1).all()
