@@ -1194,23 +1194,68 @@ __device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int
     return o2f(ub);
 }
 
-__device__ inline float dense_kth_bound(const float2* __restrict__ ce, int cnt, int k, int* hist, int lane) {
-    return kth_bound_stream([ce](int e) { return ce[e]; }, cnt, k, hist, lane);
+// k-th bound of a dense first-pass buffer in one read, held in registers:
+// lane l reads entries l, l + 32, ... and keeps the M smallest upper values
+// (score + bound) it sees; U is the k-th smallest of those 32*M values
+// (32*M >= k).  Every kept value is an entry's, so at least k entries lie at
+// or below U; values were only left out, so U is at or above the k-th
+// smallest upper value of the whole buffer.  U is that exact k-th value
+// unless one lane read more than M of the k smallest.  With cnt >= k every
+// lane keeps all its entries or M of them, so the k-th kept value is an
+// entry's, never the padding (0xffffffff).
+template <int M>
+__device__ inline float dense_kth_regs(const float2* __restrict__ ce, int cnt, int k, int lane) {
+    uint32_t a[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) a[i] = 0xffffffffu;
+#pragma unroll 4
+    for (int e = lane; e < cnt; e += 32) {
+        const float2 v = ce[e];
+        uint32_t h = f2o(v.x + v.y);
+#pragma unroll
+        for (int i = 0; i < M; ++i) {  // insertion into the ascending a[]
+            const uint32_t lo = min(a[i], h);
+            h = max(a[i], h);
+            a[i] = lo;
+        }
+    }
+    // The k-th smallest kept value, bit by bit below the bits every kept
+    // value shares: R is kept as the prefix of the answer; a bit is set when
+    // fewer than k kept values lie at or below R with that bit clear and
+    // every lower bit set.
+    const uint32_t mn = __reduce_min_sync(FULL, a[0]);
+    const uint32_t mx = __reduce_max_sync(FULL, a[M - 1]);
+    if (mn == mx) return o2f(mn);
+    const int top = 31 - __clz(mn ^ mx);
+    uint32_t R = mn & ~((2u << top) - 1u);
+#pragma unroll 1
+    for (int bit = top; bit >= 0; --bit) {
+        const uint32_t T = R | ((1u << bit) - 1u);
+        int c = 0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) c += a[i] <= T ? 1 : 0;
+        if (static_cast<int>(__reduce_add_sync(FULL, static_cast<unsigned>(c))) < k) R |= 1u << bit;
+    }
+    return o2f(R);
 }
 
 // Warp tighten of a query whose first-pass list was scanned densely: its
 // buffer holds cnt {score, error bound} pairs, entry i for row i of the list
 // (arena rows from row0).  U = an upper bound on the k-th smallest
-// score + bound with at least k entries at or below it (two 8-bit radix
-// passes below the bits all entries share; U is the upper edge of the final
-// bin that holds the k-th value); the entries with score - bound <= U are
-// rewritten in place as keys (score, arena row) at the front of the buffer.
-// Fewer than k entries: every entry is kept and the threshold is left alone.
+// score + bound with at least k entries at or below it (dense_kth_regs);
+// the entries with score - bound <= U are rewritten in place as keys
+// (score, arena row) at the front of the buffer.  Fewer than k entries:
+// every entry is kept and the threshold is left alone.
 __device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const BatchWork& w, int capq, int k,
-                                           float* __restrict__ thr, int* hist, int lane) {
+                                           float* __restrict__ thr, int lane) {
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
     const float2* ce = reinterpret_cast<const float2*>(cq);
-    const float U = cnt >= k ? dense_kth_bound(ce, cnt, k, hist, lane) : INFINITY;
+    float U = INFINITY;
+    // M about twice k/32: a lane reads more than M of the k smallest rarely.
+    if (cnt >= k)
+        U = k <= 32    ? dense_kth_regs<4>(ce, cnt, k, lane)
+            : k <= 128 ? dense_kth_regs<8>(ce, cnt, k, lane)
+                       : dense_kth_regs<16>(ce, cnt, k, lane);
     // In-place rewrite, four rounds of 32 at a time: all four rounds are
     // read (loads in flight together) before any of their writes, and writes
     // never pass the reads.
@@ -1278,13 +1323,12 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
 // Queries whose first-pass list was scanned densely, one warp each.
 __global__ void __launch_bounds__(256) tighten_dense_kernel(int nq, BatchWork w, int capq, int k,
                                                             float* __restrict__ thr, DenseFirst df) {
-    __shared__ int hist[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
     const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
     if (l0 < 0 || df.list_size[l0] > df.dense_max) return;
-    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], w, capq, k, thr, hist[warp], lane);
+    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], w, capq, k, thr, lane);
 }
 
 // Queries with 1025..2048 candidates (w.big), one warp each.

@@ -86,3 +86,17 @@ def test_bf16_device_api_matches_host_api():
     torch.cuda.synchronize()
     np.testing.assert_array_equal(dD.cpu().numpy(), Dh)
     np.testing.assert_array_equal(dI.cpu().numpy(), Ih)
+
+
+@pytest.mark.parametrize("name", ["int_small", "ip_small"])
+@pytest.mark.parametrize("k", [1, 32, 33, 100, 129, 256])
+def test_bf16_equals_plain_across_k(name, k):
+    """The first pass's k-th bound (per-lane register selection, sized by k)
+    is valid at every k: the bf16 answer equals the plain scan's."""
+    idx, x, q, c = bf16_index(name)
+    Db, Ib = idx.search(q, k)
+    assert idx.last_stats()["fallback_queries"] == 0
+    idx.set_form("plain")
+    Dp, Ip = idx.search(q, k)
+    np.testing.assert_array_equal(Db, Dp)
+    np.testing.assert_array_equal(Ib, Ip)
