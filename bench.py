@@ -368,6 +368,8 @@ def run_ours(args, rank, world, dist):
     tune = None
     if base == "fp8":
         idx.set_batch_params(oversample=args.oversample)
+    if base != "plain" and args.group_size:
+        idx.set_group_size(args.group_size)
     if base != "plain" and args.autotune:
         # Work shape picked on this batch (every shape gives the same answer).
         tune = idx.autotune(q, k, reps=2)
@@ -910,6 +912,8 @@ def main():
                     help="scan form under the learned probes")
     ap.add_argument("--oversample", type=int, default=4, help="e4m3 form: re-rank at most oversample x k")
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--group-size", type=int, default=0, choices=[0, 32, 64, 128],
+                    help="queries per group of the tensor-core passes (0: per pass by queries per list)")
     ap.add_argument("--train-queries", type=int, default=20000)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--coverage", type=float, default=0.97)

@@ -79,6 +79,7 @@ def load():
     L.hy_index_set_form.argtypes = [H, i]
     L.hy_index_set_plain_scan.argtypes = [H, i]
     L.hy_index_set_batch_params.argtypes = [H, sz, sz, sz]
+    L.hy_index_set_group_size.argtypes = [H, C.c_int]
     L.hy_index_set_coarse.argtypes = [H, i]
     L.hy_index_search.argtypes = [H, sz, vp, sz, vp, vp]
     L.hy_index_search_device.argtypes = [H, sz, vp, sz, vp, vp, vp]

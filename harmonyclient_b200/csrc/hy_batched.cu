@@ -14,10 +14,10 @@
 // form dist = |x|^2 + |q|^2 - 2 q.x (or -q.x for inner product) with a
 // rigorous bound on its distance from the plain scan's exact FP32 value.
 //
-// First pass (each query's nearest list): dense items write {dist, bound}
-// for every row; the tightening step takes each query's k-th smallest
-// dist + bound as its threshold and keeps the rows whose dist - bound reach
-// it.  Second pass (the other probed lists): rows whose dist - bound passes
+// First pass (each query's nearest list): dense items write the distance of
+// every row; the tightening step recomputes each row's bound, takes each
+// query's k-th smallest dist + bound as its threshold and keeps the rows
+// whose dist - bound reach it.  Second pass (the other probed lists): rows whose dist - bound passes
 // the threshold are emitted as candidates.  The re-rank keeps the candidates
 // whose bound can reach the top-k and gives them the exact FP32 distance (or
 // keeps the tensor-core distance when the exactness certificate shows it is
@@ -40,7 +40,8 @@ namespace {
 
 constexpr int METRIC_IP = 0, METRIC_L2 = 1;  // include/hy.h's HY_METRIC_*
 constexpr int TM = 128;      // rows per tile (MMA M)
-constexpr int NS = 4;        // A stages (one 16 KiB k-block each)
+constexpr int NS_MIN = 4;    // A stages (one 16 KiB k-block each): at least this many,
+constexpr int NS_MAX = 8;    // and as many more as shared memory holds
 constexpr int KB_BYTES = 16384;
 
 // ---------------------------------------------------------------------------
@@ -166,6 +167,18 @@ __global__ void tile_aux_kernel(const float2* __restrict__ row_aux, int64_t tile
         e = fmaxf(e, __shfl_xor_sync(FULL, e, o));
     }
     if (lane == 0) out[t] = make_float2(a, e);
+}
+
+// Per 128-row tile: the largest squared norm of its rows.
+__global__ void tile_max_kernel(const float* __restrict__ xn, int64_t tiles, float* __restrict__ out) {
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= tiles) return;
+    float m = 0.0f;
+    for (int r = lane; r < TM; r += 32) m = fmaxf(m, xn[t * TM + r]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if (lane == 0) out[t] = m;
 }
 
 // Queries in e4m3: per query scale t = max|q_j| / 448 (1 for a zero query),
@@ -471,6 +484,7 @@ struct BatchedParams {
     unsigned int* work;             // work-queue counter
     int* err;
     int nlist, nkb, rs, capq, metric;
+    int ns;                         // stages in the list k-block ring (NS_MIN..NS_MAX)
     int dense_max;                  // lists of at most this many rows: dense items (0 = none)
     float cK, cN;                   // error-bound constants (see err_coef)
 };
@@ -507,14 +521,25 @@ struct ItemSlot {
     alignas(16) float sc[QG];    // accumulator -> inner product scale (1, or list scale x query scale)
 };
 
-// Dynamic shared memory of the batched kernel for query groups of QG and nkb
-// 128-byte k-blocks per row.
+// Dynamic shared memory of the batched kernel for query groups of QG, nkb
+// 128-byte k-blocks per row and ns stages.
 template <int QG>
-constexpr size_t batched_smem(int nkb) {
+constexpr size_t batched_smem(int nkb, int ns) {
     constexpr int CW = QG / 2, CC = CW < 32 ? CW : 32;
-    return 1024 + 2 * static_cast<size_t>(nkb) * QG * 128 + static_cast<size_t>(NS) * KB_BYTES +
+    return 1024 + 2 * static_cast<size_t>(nkb) * QG * 128 + static_cast<size_t>(ns) * KB_BYTES +
            2 * sizeof(ItemSlot<QG>) + N_EPI * CW * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
            N_EPI * 32 * CC * sizeof(float);
+}
+// Dynamic shared memory per CTA: the 227 KiB opt-in limit less room for the
+// kernel's static shared variables (barriers, TMEM base, flags).
+constexpr size_t BATCHED_SMEM_CAP = 227 * 1024 - 256;
+
+// The deepest stage ring in [NS_MIN, NS_MAX] that fits (0: none fits).
+template <int QG>
+constexpr int batched_stages(int nkb) {
+    for (int ns = NS_MAX; ns >= NS_MIN; --ns)
+        if (batched_smem<QG>(nkb, ns) <= BATCHED_SMEM_CAP) return ns;
+    return 0;
 }
 
 // Accumulator column of a group's i-th query (a bijection on [0, QG)).
@@ -553,8 +578,9 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
     const int nkb = p.nkb;
     unsigned char* sB = base;                                        // 2 slots x nkb x BKB (queries)
-    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * BKB;     // NS x 16 KiB (list k-blocks)
-    Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(NS) * KB_BYTES);  // [2], 1024-aligned
+    const int ns = p.ns;                                             // stages in the ring
+    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * BKB;     // ns x 16 KiB (list k-blocks)
+    Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(ns) * KB_BYTES);  // [2], 1024-aligned
     static_assert(offsetof(Slot, xn) % 16 == 0 && offsetof(Slot, sc) % 16 == 0 && sizeof(Slot) % 16 == 0,
                   "ItemSlot alignment");
     float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][CW] per-tile test bounds
@@ -562,7 +588,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
     float* s_ip = reinterpret_cast<float*>(s_ck + N_EPI * CB);       // [N_EPI][32 lanes][CC] candidate chunks
 
-    __shared__ uint64_t full[NS], empty[NS], accf[2], acce[2], sfull[2], sfree[2];
+    __shared__ uint64_t full[NS_MAX], empty[NS_MAX], accf[2], acce[2], sfull[2], sfree[2];
     __shared__ uint32_t tbase;
     __shared__ int s_abort;
     __shared__ long long s_g[2];
@@ -572,7 +598,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     volatile int* vabort = &s_abort;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < NS; ++i) {
+        for (int i = 0; i < ns; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], 1);
         }
@@ -710,7 +736,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     } else if (warp == W_PRODUCER) {
         // ---------------- producer: list k-blocks into the stage ring
         if (lane == 0) {
-            uint32_t load_it = 0;
+            int ls = 0;        // stage of the next copy
+            uint32_t lph = 0;  // its ring round's parity
             for (uint32_t it = 0;; ++it) {
                 const int b = it & 1;
                 if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
@@ -719,9 +746,14 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const int64_t tile0 = slot[b].row0 / TM;
                 bool ok = true;
                 for (int t = 0; t < ntiles && ok; ++t) {
-                    for (int kb = 0; kb < nkb; ++kb, ++load_it) {
-                        const int s = load_it % NS;
-                        if (!wait_or_abort(&empty[s], ((load_it / NS) & 1u) ^ 1u, p.err, vabort)) {
+                    for (int kb = 0; kb < nkb; ++kb) {
+                        const int s = ls;
+                        const uint32_t ph = lph;
+                        if (++ls == ns) {
+                            ls = 0;
+                            lph ^= 1u;
+                        }
+                        if (!wait_or_abort(&empty[s], ph ^ 1u, p.err, vabort)) {
                             ok = false;
                             break;
                         }
@@ -738,7 +770,9 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         // ---------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = F8 ? tc::idesc_e4m3_f32(TM, QG) : tc::idesc_bf16_f32(TM, QG);
-            uint32_t mma_it = 0, tile_it = 0;
+            int ms = 0;        // stage of the next k-block
+            uint32_t mph = 0;  // its ring round's parity
+            uint32_t tile_it = 0;
             bool ok = true;
             for (uint32_t it = 0; ok; ++it) {
                 const int b = it & 1;
@@ -755,9 +789,14 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                     }
                     tc::fence_after_sync();
                     const uint32_t dcol = tmem + static_cast<uint32_t>(buf * QG);
-                    for (int kb = 0; kb < nkb; ++kb, ++mma_it) {
-                        const int s = mma_it % NS;
-                        if (!wait_or_abort(&full[s], (mma_it / NS) & 1u, p.err, vabort)) {
+                    for (int kb = 0; kb < nkb; ++kb) {
+                        const int s = ms;
+                        const uint32_t ph = mph;
+                        if (++ms == ns) {
+                            ms = 0;
+                            mph ^= 1u;
+                        }
+                        if (!wait_or_abort(&full[s], ph, p.err, vabort)) {
                             ok = false;
                             break;
                         }
@@ -830,11 +869,6 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 // Per-tile test bound of this warp's queries:
                 // V + max|x~| aq + max|x - x~| bq over the tile's rows.
                 const float2 ta = S.taux[t];
-                // A dense item's per-row bound terms, fetched before the wait
-                // for the accumulator so the load overlaps the MMA.
-                const int pre_row = t * TM + quad * 32 + lane;
-                const float2 xa_pre =
-                    (S.dense && pre_row < nrows) ? p.xaux[row0 + pre_row] : make_float2(0.0f, 0.0f);
                 __syncwarp();
                 for (int cc = lane; cc < CW; cc += 32) {
                     const int q = half * CW + cc;
@@ -877,23 +911,21 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 if (lane == 0) mbar_arrive_cta(&acce[buf]);
                 if (S.dense) {
                     // Dense item: every valid row of every occupied column
-                    // writes {score, error bound} at the row's offset in the
-                    // list (the warp's 32 rows are 256 contiguous bytes of
-                    // the query's buffer); the threshold is not consulted.
-                    // The bound is the tightening step's own expression.
+                    // writes its score (4 bytes) at the row's offset in the
+                    // list within the upper half of the query's buffer (the
+                    // warp's 32 rows are 128 contiguous bytes); the threshold
+                    // is not consulted, and the tightening step recomputes
+                    // each row's error bound from the row's terms.
                     const int pos = S.lrow0 + rs_row;
                     if (rvalid && pos < p.capq) {
-                        const float2 xa = xa_pre;
-                        const float rc = err_row_const(xnv, l2, p.cN);
-                        float2* cf2 = reinterpret_cast<float2*>(p.cand);
+                        float* cfs = reinterpret_cast<float*>(p.cand) + p.capq;
 #pragma unroll
                         for (int j = 0; j < CW; ++j) {
                             if (j >= nact) break;
                             const int q = half * CW + j;
                             const float ip = F8 ? __uint_as_float(u[j]) * S.sc[q] : __uint_as_float(u[j]);
                             const float score = l2 ? __fadd_rn(__fadd_rn(xnv, S.qn[q]), -2.0f * ip) : -ip;
-                            const float eb = fmaf(xa.x, S.aq[q], fmaf(xa.y, S.bq[q], rc + S.cq[q]));
-                            cf2[static_cast<int64_t>(S.qid[q]) * p.capq + pos] = make_float2(score, eb);
+                            cfs[static_cast<int64_t>(S.qid[q]) * (2 * p.capq) + pos] = score;
                         }
                     }
                     continue;
@@ -1195,22 +1227,23 @@ __device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int
 }
 
 // k-th bound of a dense first-pass buffer in one read, held in registers:
-// lane l reads entries l, l + 32, ... and keeps the M smallest upper values
-// (score + bound) it sees; U is the k-th smallest of those 32*M values
+// lane l reads entries l, l + 32, ... (entry(e) = {score, bound}) and keeps
+// the M smallest upper values (score + bound) it sees; U is the k-th
+// smallest of those 32*M values
 // (32*M >= k).  Every kept value is an entry's, so at least k entries lie at
 // or below U; values were only left out, so U is at or above the k-th
 // smallest upper value of the whole buffer.  U is that exact k-th value
 // unless one lane read more than M of the k smallest.  With cnt >= k every
 // lane keeps all its entries or M of them, so the k-th kept value is an
 // entry's, never the padding (0xffffffff).
-template <int M>
-__device__ inline float dense_kth_regs(const float2* __restrict__ ce, int cnt, int k, int lane) {
+template <int M, typename Entry>
+__device__ inline float dense_kth_regs(Entry entry, int cnt, int k, int lane) {
     uint32_t a[M];
 #pragma unroll
     for (int i = 0; i < M; ++i) a[i] = 0xffffffffu;
 #pragma unroll 4
     for (int e = lane; e < cnt; e += 32) {
-        const float2 v = ce[e];
+        const float2 v = entry(e);
         uint32_t h = f2o(v.x + v.y);
 #pragma unroll
         for (int i = 0; i < M; ++i) {  // insertion into the ascending a[]
@@ -1239,43 +1272,87 @@ __device__ inline float dense_kth_regs(const float2* __restrict__ ce, int cnt, i
     return o2f(R);
 }
 
-// Warp tighten of a query whose first-pass list was scanned densely: its
-// buffer holds cnt {score, error bound} pairs, entry i for row i of the list
-// (arena rows from row0).  U = an upper bound on the k-th smallest
-// score + bound with at least k entries at or below it (dense_kth_regs);
-// the entries with score - bound <= U are rewritten in place as keys
-// (score, arena row) at the front of the buffer.  Fewer than k entries:
-// every entry is kept and the threshold is left alone.
-__device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const BatchWork& w, int capq, int k,
+// Warp tighten of a query whose first-pass list was scanned densely: the
+// upper half of its buffer holds cnt scores, entry i for row i of the list
+// (arena rows from row0); each entry's error bound is recomputed from the
+// row's {|x~|, |x - x~|} and squared norm and the query's coefficients,
+// the same expression as the batched kernel's candidate test.  U = an upper
+// bound on the k-th smallest score + bound with at least k entries at or
+// below it (dense_kth_regs); the entries with score - bound <= U are
+// rewritten as keys (score, arena row) at the front of the buffer (key m
+// overwrites bytes [8m, 8m + 8), below every entry not yet read, which sit
+// at 4 capq + 4e with e >= m).  Fewer than k entries: every entry is kept
+// and the threshold is left alone.
+__device__ inline void tighten_dense_query(int qi, int cnt, int64_t row0, const float* __restrict__ xn,
+                                           const float2* __restrict__ xaux, const float4* __restrict__ qaux,
+                                           const float2* __restrict__ tile_aux, const float* __restrict__ tile_xn,
+                                           bool l2, float cK, float cN, const BatchWork& w, int capq, int k,
                                            float* __restrict__ thr, int lane) {
     uint64_t* cq = w.cand + static_cast<int64_t>(qi) * capq;
-    const float2* ce = reinterpret_cast<const float2*>(cq);
+    const float* cs = reinterpret_cast<const float*>(cq) + capq;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    // B = the bound expression at the list's tile maxima of |x~|, |x - x~|
+    // and |x|^2: every row's bound is at most B (each rounded operation is
+    // monotone in its non-negative operands).
+    float mx = 0.0f, my = 0.0f, mn = 0.0f;
+    for (int64_t t = row0 / TM + lane; t < (row0 + cnt + TM - 1) / TM; t += 32) {
+        const float2 a = tile_aux[t];
+        mx = fmaxf(mx, a.x);
+        my = fmaxf(my, a.y);
+        mn = fmaxf(mn, tile_xn[t]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+        my = fmaxf(my, __shfl_xor_sync(FULL, my, o));
+        mn = fmaxf(mn, __shfl_xor_sync(FULL, mn, o));
+    }
+    const float B = fmaf(mx, ec.aq, fmaf(my, ec.bq, err_row_const(mn, l2, cN) + ec.cq));
+    // U = (k-th smallest score) + B: at least k entries have score + bound
+    // at or below it.
     float U = INFINITY;
+    auto score = [&](int e) { return make_float2(cs[e], 0.0f); };
     // M about twice k/32: a lane reads more than M of the k smallest rarely.
     if (cnt >= k)
-        U = k <= 32    ? dense_kth_regs<4>(ce, cnt, k, lane)
-            : k <= 128 ? dense_kth_regs<8>(ce, cnt, k, lane)
-                       : dense_kth_regs<16>(ce, cnt, k, lane);
+        U = (k <= 32    ? dense_kth_regs<4>(score, cnt, k, lane)
+             : k <= 128 ? dense_kth_regs<8>(score, cnt, k, lane)
+                        : dense_kth_regs<16>(score, cnt, k, lane)) +
+            B;
+    // An entry is kept when score - bound <= U: at once when score <= U,
+    // never when score - B > U, else with the row's own bound.
+    const float2* xa = xaux + row0;
+    const float* xr = xn + row0;
+    auto keep_entry = [&](float sc, int e) {
+        if (sc <= U) return true;
+        if (sc - B > U) return false;
+        const float2 a = xa[e];
+        return sc - fmaf(a.x, ec.aq, fmaf(a.y, ec.bq, err_row_const(xr[e], l2, cN) + ec.cq)) <= U;
+    };
     // In-place rewrite, four rounds of 32 at a time: all four rounds are
     // read (loads in flight together) before any of their writes, and writes
     // never pass the reads.
     int m = 0;
     for (int base = 0; base < cnt; base += 128) {
-        float2 v[4];
+        float v[4];
+        bool kp[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int e = base + 32 * i + lane;
-            v[i] = e < cnt ? ce[e] : make_float2(0.0f, 0.0f);
+            v[i] = e < cnt ? cs[e] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = base + 32 * i + lane;
+            kp[i] = e < cnt && keep_entry(v[i], e);
         }
         __syncwarp();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int e = base + 32 * i + lane;
-            const bool keep = e < cnt && v[i].x - v[i].y <= U;
-            const unsigned b = __ballot_sync(FULL, keep);
-            if (keep)
+            const unsigned b = __ballot_sync(FULL, kp[i]);
+            if (kp[i])
                 cq[m + __popc(b & ((1u << lane) - 1u))] =
-                    (static_cast<uint64_t>(f2o(v[i].x)) << 32) | static_cast<uint32_t>(row0 + e);
+                    (static_cast<uint64_t>(f2o(v[i])) << 32) | static_cast<uint32_t>(row0 + e);
             m += __popc(b);
         }
     }
@@ -1321,14 +1398,18 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
 }
 
 // Queries whose first-pass list was scanned densely, one warp each.
-__global__ void __launch_bounds__(256) tighten_dense_kernel(int nq, BatchWork w, int capq, int k,
+__global__ void __launch_bounds__(256) tighten_dense_kernel(const float* __restrict__ xn,
+                                                            const float2* __restrict__ xaux,
+                                                            const float4* __restrict__ qaux, int nq, BatchWork w,
+                                                            int capq, int k, int metric, float cK, float cN,
                                                             float* __restrict__ thr, DenseFirst df) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
     const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
     if (l0 < 0 || df.list_size[l0] > df.dense_max) return;
-    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], w, capq, k, thr, lane);
+    tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], xn, xaux, qaux, df.tile_aux, df.tile_xn, metric == 1, cK,
+                        cN, w, capq, k, thr, lane);
 }
 
 // Queries with 1025..2048 candidates (w.big), one warp each.
@@ -1417,8 +1498,10 @@ __global__ void coarse_items_kernel(int nq, int nlist, int64_t rows, int ngroups
 __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4 : d + 1; }
 
 // Exact coarse selection from the tensor-core scores.  Per query (one warp):
-// cand holds nlist {score, error bound} pairs (held in registers, PER per
-// lane); U = an upper bound on the m-th smallest score + bound
+// the upper half of cand holds nlist scores; with each centroid's error
+// bound recomputed from its {|c~|, |c - c~|} and squared norm and the
+// query's coefficients, the {score, bound} pairs are held in registers (PER
+// per lane); U = an upper bound on the m-th smallest score + bound
 // (warp_select_bound); every centroid whose score - bound <= U (a set that
 // holds the exact m best, ties included) gets its exact FP32 coarse score
 // with the same sequential arithmetic as coarse_scores_kernel (dimension
@@ -1551,8 +1634,11 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
 template <int METRIC, int PER>
 __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
                                                             const float* __restrict__ q,
-                                                            const float* __restrict__ cent, int d, int m,
-                                                            int64_t* __restrict__ out_idx,
+                                                            const float* __restrict__ cent,
+                                                            const float* __restrict__ cxn,
+                                                            const float2* __restrict__ caux,
+                                                            const float4* __restrict__ qaux, float cK, float cN,
+                                                            int d, int m, int64_t* __restrict__ out_idx,
                                                             float* __restrict__ out_score) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1567,10 +1653,13 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
     const float* qrow = q + static_cast<size_t>(qi) * d;
     for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
     // Every centroid's upper bound (ordered bits) and lower bound in
-    // registers: entry r * 32 + lane.  The query's pairs are then free and
-    // their space holds its candidate keys.
+    // registers: entry r * 32 + lane.  The query's buffer is then free and
+    // holds its candidate keys.
     float2* ce = cand + static_cast<int64_t>(qi) * nlist;
+    const float* cs = reinterpret_cast<const float*>(ce) + nlist;
     uint64_t* keys = reinterpret_cast<uint64_t*>(ce);
+    const bool l2 = METRIC == METRIC_L2;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
     uint32_t hi[PER];
     float lo[PER];
 #pragma unroll
@@ -1579,9 +1668,11 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
         hi[r] = 0xffffffffu;
         lo[r] = INFINITY;
         if (e < nlist) {
-            const float2 v = ce[e];
-            hi[r] = f2o(v.x + v.y);
-            lo[r] = v.x - v.y;
+            const float sc = cs[e];
+            const float2 a = caux[e];
+            const float eb = fmaf(a.x, ec.aq, fmaf(a.y, ec.bq, err_row_const(cxn[e], l2, cN) + ec.cq));
+            hi[r] = f2o(sc + eb);
+            lo[r] = sc - eb;
         }
     }
     const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
@@ -1608,20 +1699,28 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
 // keys whose lower bound reaches it, and coarse_refine_keys_kernel selects
 // and re-scores them exactly.
 __global__ void __launch_bounds__(256) coarse_thr_kernel(const float2* __restrict__ cand, int nq, int S, int m,
-                                                         float* __restrict__ thr) {
+                                                         const float* __restrict__ cxn,
+                                                         const float2* __restrict__ caux,
+                                                         const float4* __restrict__ qaux, int metric, float cK,
+                                                         float cN, float* __restrict__ thr) {
     __shared__ int hist[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
-    const float2* ce = cand + static_cast<int64_t>(qi) * S;
+    // The dense launch's scores (upper half of the query's buffer) and each
+    // centroid's recomputed error bound.
+    const float* cs = reinterpret_cast<const float*>(cand + static_cast<int64_t>(qi) * S) + S;
+    const bool l2 = metric == METRIC_L2;
+    const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
     uint32_t hv[32];
 #pragma unroll
     for (int r = 0; r < 32; ++r) {
         const int e = r * 32 + lane;
         hv[r] = 0xffffffffu;
         if (e < S) {
-            const float2 v = ce[e];
-            hv[r] = f2o(v.x + v.y);
+            const float2 a = caux[e];
+            const float eb = fmaf(a.x, ec.aq, fmaf(a.y, ec.bq, err_row_const(cxn[e], l2, cN) + ec.cq));
+            hv[r] = f2o(cs[e] + eb);
         }
     }
     const float U = o2f(warp_select_bound<32>(hv, S, m, hist[warp], lane));
@@ -2010,7 +2109,7 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.big2, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     if (df.dense_max > 0) {
-        tighten_dense_kernel<<<(nq + 7) / 8, 256, 0, s>>>(nq, w, capq, k, thr, df);
+        tighten_dense_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
@@ -2064,8 +2163,11 @@ size_t coarse_refine_smem(int nlist, int d, int warps) {
     return static_cast<size_t>(warps) * ((per_warp + 15) & ~size_t(15));
 }
 
-cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent, int d,
-                                 int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s) {
+cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent,
+                                 const float* cxn, const float2* caux, const float4* qaux, int d, int metric, int m,
+                                 int64_t* out_idx, float* out_score, cudaStream_t s) {
+    float cK, cN;
+    err_consts(d, false, &cK, &cN);
     int warps = 4;
     while (warps > 1 && coarse_refine_smem(nlist, d, warps) > 200 * 1024) warps >>= 1;
     const size_t smem = coarse_refine_smem(nlist, d, warps);
@@ -2074,7 +2176,8 @@ cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
-        kern<<<grid, 32 * warps, smem, s>>>(cand, nq, nlist, q, cent, d, m, out_idx, out_score);
+        kern<<<grid, 32 * warps, smem, s>>>(cand, nq, nlist, q, cent, cxn, caux, qaux, cK, cN, d, m, out_idx,
+                                            out_score);
         return cudaGetLastError();
     };
     if (nlist > 2048) return cudaErrorInvalidValue;
@@ -2083,9 +2186,12 @@ cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q
     return nlist <= 1024 ? run(coarse_refine_kernel<METRIC_IP, 32>) : run(coarse_refine_kernel<METRIC_IP, 64>);
 }
 
-cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, float* thr, cudaStream_t s) {
+cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, const float* cxn, const float2* caux,
+                              const float4* qaux, int d, int metric, float* thr, cudaStream_t s) {
     if (S > 1024 || m > S) return cudaErrorInvalidValue;
-    coarse_thr_kernel<<<(nq + 7) / 8, 256, 0, s>>>(cand, nq, S, m, thr);
+    float cK, cN;
+    err_consts(d, false, &cK, &cN);
+    coarse_thr_kernel<<<(nq + 7) / 8, 256, 0, s>>>(cand, nq, S, m, cxn, caux, qaux, metric, cK, cN, thr);
     return cudaGetLastError();
 }
 
@@ -2154,6 +2260,12 @@ cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t row
     return cudaGetLastError();
 }
 
+cudaError_t launch_tile_max(const float* xn, int64_t rows, float* tile_max, cudaStream_t s) {
+    const int64_t tiles = rows / TM;
+    tile_max_kernel<<<grid_for(tiles * 32, 256), 256, 0, s>>>(xn, tiles, tile_max);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
                                  const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s) {
     const int64_t n = static_cast<int64_t>(nq) * (j1 - j0);
@@ -2184,17 +2296,17 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
 
 int batched_group_size(int d, bool f8) {
     const int nkb = f8 ? (d + 127) / 128 : (d + 63) / 64;
-    constexpr size_t cap = 227 * 1024;
-    if (batched_smem<128>(nkb) <= cap) return 128;
-    if (batched_smem<64>(nkb) <= cap) return 64;
-    if (batched_smem<32>(nkb) <= cap) return 32;
+    if (batched_stages<128>(nkb)) return 128;
+    if (batched_stages<64>(nkb)) return 64;
+    if (batched_stages<32>(nkb)) return 32;
     return 0;
 }
 
 template <int QG, bool F8>
-static cudaError_t launch_batched_t(const BatchedParams& p, int nsm, cudaStream_t s) {
-    const size_t smem = batched_smem<QG>(p.nkb);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+static cudaError_t launch_batched_t(BatchedParams p, int nsm, cudaStream_t s) {
+    p.ns = batched_stages<QG>(p.nkb);
+    if (p.ns == 0) return cudaErrorInvalidValue;
+    const size_t smem = batched_smem<QG>(p.nkb, p.ns);
     cudaError_t e = cudaFuncSetAttribute(batched_scan_kernel<QG, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;

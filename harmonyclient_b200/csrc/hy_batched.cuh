@@ -51,6 +51,9 @@ cudaError_t launch_arena_integral(const float* codes, int64_t n, const float* xn
 // Per arena row {|x~|, |x - x~|} for the error bound (tscale == nullptr: the
 // bf16 image, else the e4m3 image with those tile scales), and per 128-row
 // tile the maxima of both.
+// tile_max[t] = the largest xn over rows [128 t, 128 t + 128) (rows a
+// multiple of 128).
+cudaError_t launch_tile_max(const float* xn, int64_t rows, float* tile_max, cudaStream_t s);
 cudaError_t launch_row_aux(const ArenaLayout& L, const float* codes, int64_t rows, const float* tscale, float2* aux,
                            float2* tile_aux, cudaStream_t s);
 
@@ -77,14 +80,17 @@ struct BatchWork {
 cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int j0, int j1, int nlist,
                                  const int32_t* list_size, int rs, int qg, const BatchWork& w, cudaStream_t s);
 // The first pass's dense lists: a query whose probes[q * nprobe] list has at
-// most dense_max rows (capped at capq) holds {score, error bound} pairs, one
-// per row of that list.  dense_max 0: no dense lists.
+// most dense_max rows (capped at capq) holds one f32 score per row of that
+// list in the upper half of its buffer (bytes 4 capq + 4 i).  dense_max 0:
+// no dense lists.
 struct DenseFirst {
     const int64_t* probes = nullptr;
     int nprobe = 0;
     const int32_t* list_size = nullptr;
     const int64_t* list_off = nullptr;
     int dense_max = 0;
+    const float2* tile_aux = nullptr;  // per arena tile {max |x~|, max |x - x~|}
+    const float* tile_xn = nullptr;    // per arena tile, max |x|^2
 };
 // thr := min(thr, k-th smallest upper bound over each query's candidates),
 // and the candidates that can still reach the top-k are compacted as keys.
@@ -103,21 +109,26 @@ cudaError_t launch_centroid_image(const float* cent, int nlist, int d, void* img
 // w.pair_off [2], w.item_off [2].
 cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int64_t* list_off, int32_t* list_size,
                                 const BatchWork& w, cudaStream_t s);
-// From the dense {score, bound} pairs of the coarse launch (cand, nq x nlist):
-// the exact m best centroids per query and their exact coarse scores, as
-// launch_select gives them from coarse_scores (cand is overwritten).  Needs m <= 256 and
-// coarse_refine_smem(nlist, d, 1) <= 200 KiB.
+// From the dense scores of the coarse launch (cand, nq x nlist slots of 8
+// bytes, scores in each query's upper half) and the bounds recomputed from
+// cxn / caux (the centroid index's squared norms and {|c~|, |c - c~|}) and
+// qaux: the exact m best centroids per query and their exact coarse scores,
+// as launch_select gives them from coarse_scores (cand is overwritten).
+// Needs m <= 256 and coarse_refine_smem(nlist, d, 1) <= 200 KiB.
 size_t coarse_refine_smem(int nlist, int d, int warps);
-cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent, int d,
-                                 int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
+cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent,
+                                 const float* cxn, const float2* caux, const float4* qaux, int d, int metric, int m,
+                                 int64_t* out_idx, float* out_score, cudaStream_t s);
 
 // More than 2048 centroids: thr[q] := a bound on the m-th smallest
-// score + bound among the S <= 1024 dense pairs of query q (cand, nq x S),
-// then, from the keys a thresholded launch over all centroids emitted
-// (cand + q * stride, ccnt[q] of them), the exact m best as
-// launch_coarse_refine gives them (cand is overwritten).  cxn / caux: the
-// centroid index's squared norms and {|c~|, |c - c~|}.
-cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, float* thr, cudaStream_t s);
+// score + bound among the S <= 1024 dense scores of query q (cand, nq x S
+// slots, bounds recomputed as for launch_coarse_refine), then, from the keys
+// a thresholded launch over all centroids emitted (cand + q * stride, ccnt[q]
+// of them), the exact m best as launch_coarse_refine gives them (cand is
+// overwritten).  cxn / caux: the centroid index's squared norms and
+// {|c~|, |c - c~|}.
+cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, const float* cxn, const float2* caux,
+                              const float4* qaux, int d, int metric, float* thr, cudaStream_t s);
 cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int nq, int stride, const float* q,
                                       const float* cent, const float* cxn, const float2* caux, const float4* qaux,
                                       int d, int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
@@ -142,8 +153,8 @@ struct BatchedLaunch {
     int qg = 128;     // queries per group (batched_group_size)
     bool f8 = false;  // e4m3 operands
     // Lists of at most dense_max rows (capped at capq) are scanned densely:
-    // every row's {score, error bound} lands at the row's offset in the list
-    // within the query's candidate buffer, with no threshold test, and the
+    // every row's f32 score lands at the row's offset in the list within the
+    // upper half of the query's candidate buffer, with no threshold test, and the
     // query's count is set to the list size (each query must have one such
     // list in the launch; launch_tighten turns them into keys).  0 = every
     // list through the threshold test.

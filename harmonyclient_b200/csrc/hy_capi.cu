@@ -194,10 +194,13 @@ struct hy_index {
     size_t capq = 8192;       // candidate slots per query
     size_t oversample = 4;    // e4m3 form: exact re-rank of at most oversample * k candidates
     size_t row_slice = 2048;  // rows per work item
+    int group_size = 0;       // queries per group of the search passes (0: per pass, by queries per list)
+    double learned_mean = 0;  // the probe model's held-out mean nprobe (0: unknown)
     int nsm = 0;
     DevBuf abf;               // bf16 tensor-core image of the arena
     DevBuf xaux;              // per arena row {|x~|, |x - x~|}
     DevBuf taux;              // per 128-row tile, maxima of xaux
+    DevBuf txn;               // per 128-row tile, the largest squared norm
     bool abf_valid = false;
     DevBuf b_cert;            // the bf16 image's exactness certificate {integral, max row norm}
     float arena_maxxn = -1.0f;  // its largest row squared norm when integral (<= 256), else -1
@@ -776,6 +779,8 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
                                        h->lscale.as<float>(), h->tscale.as<float>(), h->a8.p, s));
         HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, h->tscale.as<float>(),
                                    h->x8aux.as<float2>(), h->t8aux.as<float2>(), s));
+        HY_RET(h->txn.ensure(tiles * sizeof(float)));
+        HY_CUDA(hy::launch_tile_max(h->norms.as<float>(), (int64_t)rows, h->txn.as<float>(), s));
         h->a8_valid = true;
         return HY_OK;
     }
@@ -787,6 +792,8 @@ int ensure_bf16_image(hy_index* h, cudaStream_t s) {
     HY_CUDA(hy::launch_to_bf16_arena(h->L, h->codes.as<float>(), (int64_t)rows, h->abf.p, s));
     HY_CUDA(hy::launch_row_aux(h->L, h->codes.as<float>(), (int64_t)rows, nullptr, h->xaux.as<float2>(), h->taux.as<float2>(),
                                s));
+    HY_RET(h->txn.ensure(rows / hy::BATCH_ROW_ALIGN * sizeof(float)));
+    HY_CUDA(hy::launch_tile_max(h->norms.as<float>(), (int64_t)rows, h->txn.as<float>(), s));
     // Exactness certificate of the image (see launch_prep_queries).
     HY_RET(h->b_cert.ensure(2 * sizeof(int32_t)));
     const int32_t init[2] = {1, 0};
@@ -881,7 +888,7 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     b.qg = qg;
     b.f8 = false;
     if (nlist <= 2048) {
-        // Every (query, centroid) {score, bound} pair, then the exact best.
+        // Every (query, centroid) score, then the exact best.
         w.item_cap = (int64_t)ngroups * ns_full;
         HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, ns_full, h->c_off.as<int64_t>(),
                                         h->c_size.as<int32_t>(), w, s));
@@ -890,7 +897,8 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
         b.dense_max = nlist;
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
         HY_CUDA(hy::launch_coarse_refine(reinterpret_cast<float2*>(h->c_cand.p), (int)m, nlist, qq,
-                                         h->cent.as<float>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+                                         h->cent.as<float>(), h->c_norm.as<float>(), h->c_aux.as<float2>(),
+                                         h->b_qn.as<float4>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
         h->launches += 3;
         return HY_OK;
     }
@@ -908,7 +916,8 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     b.dense_max = S;
     HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
     HY_CUDA(hy::launch_coarse_thr(reinterpret_cast<const float2*>(h->c_cand.p), (int)m, S, (int)nprobe,
-                                  h->b_thr.as<float>(), s));
+                                  h->c_norm.as<float>(), h->c_aux.as<float2>(), h->b_qn.as<float4>(), (int)h->d,
+                                  h->metric, h->b_thr.as<float>(), s));
     w.item_cap = (int64_t)ngroups * ns_full;
     HY_CUDA(hy::launch_coarse_items((int)m, nlist, ngroups, ns_full, h->c_off.as<int64_t>(), h->c_size.as<int32_t>(),
                                     w, s));
@@ -988,7 +997,25 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     size_t max_slices = 1;
     for (size_t l = 0; l < nlist; ++l)
         max_slices = std::max(max_slices, ((size_t)h->h_list_size[l] + h->row_slice - 1) / h->row_slice);
-    const size_t item_cap = std::min<size_t>((qc * nprobe / 128 + nlist) * max_slices, size_t(4) << 20);
+    // Queries per group of each pass (hy_index_set_group_size): by default
+    // the smallest of 64 / 128 holding four times the pass's expected
+    // queries per list (measured on 1M x 128 at about 10 queries per list:
+    // 64 ahead of 128 and 32).  The first pass has one list per query; the
+    // second the rest of the fixed nprobe, or of the probe model's held-out
+    // mean.
+    auto pass_group = [&](double pairs) {
+        if (h->group_size) return std::min(h->group_size, qg);
+        const double per_list = pairs / (double)nlist;
+        int g = 64;
+        while (g < qg && g < 4.0 * per_list) g *= 2;
+        return std::min(g, qg);
+    };
+    const double np_rest =
+        (learned_on(h) && h->learned_mean > 0) ? std::max(0.0, h->learned_mean - 1.0) : (double)(nprobe - 1);
+    const int qg1 = pass_group((double)qc);
+    const int qg2 = pass_group((double)qc * np_rest);
+    const size_t item_cap =
+        std::min<size_t>((qc / qg1 + qc * nprobe / qg2 + 2 * nlist) * max_slices, size_t(4) << 20);
     HY_RET(h->b_items.ensure(item_cap * sizeof(int4)));
     hy::BatchWork w;
     w.items = h->b_items.as<int4>();
@@ -1052,7 +1079,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         b.lscale = f8 ? h->lscale.as<float>() : nullptr;
         b.qscale = f8 ? h->b_qs.as<float>() : nullptr;
         b.f8 = f8;
-        b.qg = qg;
+        b.qg = qg1;
         b.qb = h->b_qb.p;
         b.qaux = h->b_qn.as<float4>();
         b.thr = h->b_thr.as<float>();
@@ -1068,7 +1095,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         // bound; pass 2: the remaining probed lists under the tight threshold.
         const bool last = timed && q0 + qc >= n;
         HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 0, 1, (int)nlist,
-                                         h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
+                                         h->list_size.as<int32_t>(), (int)h->row_slice, qg1, w, s));
         if (last) HY_CUDA(ev_record(h->ev[6], s));
         b.dense_max = dense_max;
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
@@ -1081,12 +1108,15 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
         df.list_size = h->list_size.as<int32_t>();
         df.list_off = h->list_off.as<int64_t>();
         df.dense_max = dense_max;
+        df.tile_aux = f8 ? h->t8aux.as<float2>() : h->taux.as<float2>();
+        df.tile_xn = h->txn.as<float>();
         HY_CUDA(hy::launch_tighten(h->norms.as<float>(), f8 ? h->x8aux.as<float2>() : h->xaux.as<float2>(),
                                    h->b_qn.as<float4>(), (int)m, w, (int)capq, (int)k, h->metric, (int)h->d, f8,
                                    h->nsm, h->b_thr.as<float>(), s, df));
         if (nprobe > 1) {
             HY_CUDA(hy::launch_invert_probes(h->w_probes.as<int64_t>(), (int)m, (int)nprobe, 1, (int)nprobe,
-                                             (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, qg, w, s));
+                                             (int)nlist, h->list_size.as<int32_t>(), (int)h->row_slice, qg2, w, s));
+            b.qg = qg2;
             if (last) HY_CUDA(ev_record(h->ev[8], s));
             HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
             if (last) HY_CUDA(ev_record(h->ev[9], s));
@@ -1439,6 +1469,14 @@ int hy_index_set_plain_scan(hy_index* h, int mode) {
     std::lock_guard<std::mutex> g(h->mu);
     h->epoch++;  // a captured search graph no longer matches
     h->plain_scan = mode;
+    return HY_OK;
+}
+
+int hy_index_set_group_size(hy_index* h, int qg) {
+    HY_CHECK(h, HY_ERR_ARG, "set_group_size: NULL handle");
+    HY_CHECK(qg == 0 || qg == 32 || qg == 64 || qg == 128, HY_ERR_ARG, "set_group_size: qg must be 0, 32, 64 or 128");
+    h->epoch++;  // a captured search graph no longer matches
+    h->group_size = qg;
     return HY_OK;
 }
 
@@ -1929,6 +1967,7 @@ int hy_index_train_probe_model(hy_index* h, size_t n, const float* q, size_t max
     h->margin = margin;
     h->model_P = (int)P;
     h->model_ready = true;
+    h->learned_mean = mean_np / (double)nv;
     if (report) {
         report[0] = (float)last_loss;
         report[1] = (float)(covered / (double)nv);
@@ -1977,6 +2016,7 @@ int hy_index_set_probe_model(hy_index* h, const float* in) {
     HY_CUDA(cudaMemcpy(h->m_sd.p, in + hy::MLP_NPARAM + hy::MLP_IN, hy::MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
     h->margin = in[hy::MLP_NPARAM + 2 * hy::MLP_IN];
     h->model_P = (int)in[hy::MLP_NPARAM + 2 * hy::MLP_IN + 1];
+    h->learned_mean = 0;
     HY_RET(h->m_wimg.ensure(hy::mlp_wimg_bytes()));
     HY_CUDA(hy::mlp_pack(h->m_params.as<float>(), h->m_wimg.as<unsigned char>(), nullptr));
     HY_CUDA(cudaDeviceSynchronize());

@@ -156,6 +156,11 @@ class Index:
     def set_batch_params(self, capq=0, oversample=0, row_slice=0):
         check(self._L.hy_index_set_batch_params(self._h, int(capq), int(oversample), int(row_slice)))
 
+    def set_group_size(self, qg=0):
+        """Queries per group of the tensor-core forms' search passes (32, 64
+        or 128; 0 picks per pass by the expected queries per list)."""
+        check(self._L.hy_index_set_group_size(self._h, int(qg)))
+
     def search(self, queries, k):
         q = _f32(queries, self.d)
         n = q.shape[0]

@@ -192,6 +192,14 @@ HY_API int hy_index_set_plain_scan(hy_index* h, int mode);
  * whose nearest list is not scanned densely or has fewer than k rows. */
 HY_API int hy_index_set_batch_params(hy_index* h, size_t capq, size_t oversample, size_t row_slice);
 
+/* Queries per group of the tensor-core forms' two search passes: 32, 64 or
+ * 128 (capped at what d allows), or 0 (default) to pick per pass 64 or 128,
+ * the smaller when it holds four times the pass's expected queries per list
+ * (fewer accumulator columns and a deeper copy ring for sparse passes; a list
+ * probed by more queries than a group holds is read once per group).  The
+ * results do not depend on it. */
+HY_API int hy_index_set_group_size(hy_index* h, int qg);
+
 /* Coarse quantiser of the bf16 form (no counterpart in the reference, which
  * scores every centroid exactly, src/Index.cpp:985-990).  HY_COARSE_EXACT:
  * exact FP32 scores of every centroid, then the nprobe best.

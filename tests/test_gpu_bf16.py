@@ -100,3 +100,17 @@ def test_bf16_equals_plain_across_k(name, k):
     Dp, Ip = idx.search(q, k)
     np.testing.assert_array_equal(Db, Dp)
     np.testing.assert_array_equal(Ib, Ip)
+
+
+@pytest.mark.parametrize("qg", [32, 64, 128])
+def test_bf16_group_sizes_equal_plain(qg):
+    """Every query-group size (and with it the copy-ring depth) returns the
+    plain scan's answer; groups smaller than a list's query count split it."""
+    idx, x, q, c = bf16_index("int_small")
+    idx.set_group_size(qg)
+    Db, Ib = idx.search(q, c["k"])
+    assert idx.last_stats()["fallback_queries"] == 0
+    idx.set_form("plain")
+    Dp, Ip = idx.search(q, c["k"])
+    np.testing.assert_array_equal(Db, Dp)
+    np.testing.assert_array_equal(Ib, Ip)
