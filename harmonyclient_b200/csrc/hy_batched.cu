@@ -1511,15 +1511,41 @@ __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4
 // pairs in cand.  Shared memory per warp: 256 histogram bins, the query and
 // a 32-row staging block of centroids.
 // The exact m best of a query's c candidate centroids (ids in keys[0, c),
-// overwritten): exact FP32 coarse scores with coarse_scores_kernel's
-// arithmetic, 32 at a time (rows staged in shared memory by asynchronous
-// copies, all in flight at once; lane i sums row i in dimension order; with d
-// a multiple of 4 the copies and reads are 16 bytes wide, row pitch d + 4, so
-// a 512-byte warp read takes the minimum four wavefronts), then ordered by
-// (score, centroid) and written as select_warp_kernel writes them.
+// and in sids[0, c) when sids is given and c <= 256): exact FP32 coarse
+// scores with coarse_scores_kernel's arithmetic (dimension order, separately
+// rounded operations), 32 candidates per round (lane i sums row i), then
+// ordered by (score, centroid) and written as select_warp_kernel writes them.
+// With d a multiple of 4 the rows are staged in shared memory by 16-byte
+// asynchronous copies (row pitch d + 4, so a warp's 512-byte read takes the
+// minimum four wavefronts) in two dimension halves: while the lanes sum one
+// half of this round's rows, the copies of the other half of the next
+// round's rows are in flight.  Up to 128 candidates the scored keys stay in
+// registers (lane i, round r: candidate 32 r + i); more are written back to
+// keys and merged through shared-memory-free warp sorts.
 template <int METRIC>
-__device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs, float* stage, int pitch,
-                                         const float* __restrict__ cent, int d, int m, int qi,
+__device__ inline float coarse_dot(const float* qs, const float* row, int j0, int j1, float acc) {
+#pragma unroll 4
+    for (int jj = j0; jj < j1; jj += 4) {
+        const float4 a = *reinterpret_cast<const float4*>(qs + jj);
+        const float4 b = *reinterpret_cast<const float4*>(row + jj);
+        if (METRIC == METRIC_L2) {
+            acc = sq_add(acc, a.x, b.x);
+            acc = sq_add(acc, a.y, b.y);
+            acc = sq_add(acc, a.z, b.z);
+            acc = sq_add(acc, a.w, b.w);
+        } else {
+            acc = ip_add(acc, a.x, b.x);
+            acc = ip_add(acc, a.y, b.y);
+            acc = ip_add(acc, a.z, b.z);
+            acc = ip_add(acc, a.w, b.w);
+        }
+    }
+    return acc;
+}
+
+template <int METRIC>
+__device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c, const float* qs, float* stage,
+                                         int pitch, const float* __restrict__ cent, int d, int m, int qi,
                                          int64_t* __restrict__ out_idx, float* __restrict__ out_score, int lane) {
     // Fewer candidates than m (not reached when the bound holds m of them):
     // the missing probes are -1.
@@ -1528,58 +1554,102 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
         if (out_score) out_score[static_cast<int64_t>(qi) * m + e] = FLT_MAX;
     }
     const bool v4 = (d & 3) == 0;
-    for (int c0 = 0; c0 < c; c0 += 32) {
-        const int nr = min(32, c - c0);
-        const int cidr = lane < nr ? static_cast<int>(keys[c0 + lane]) : 0;
-        for (int r = 0; r < nr; ++r) {
-            const float* src = cent + static_cast<size_t>(__shfl_sync(FULL, cidr, r)) * d;
-            float* dst = stage + r * pitch;
-            if (v4)
-                for (int j = 4 * lane; j < d; j += 128) cp_async16(dst + j, src + j);
-            else
-                for (int j = lane; j < d; j += 32) cp_async4(dst + j, src + j);
+    const bool in_regs = c <= 128;
+    const bool ids_smem = sids != nullptr && c <= 256;
+    auto cid_of = [&](int e) { return ids_smem ? sids[e] : static_cast<int>(keys[e]); };
+    uint64_t kr[4] = {KEY_MAX, KEY_MAX, KEY_MAX, KEY_MAX};
+    if (v4) {
+        const int dh = ((d >> 1) + 3) & ~3;  // first half [0, dh), second [dh, d)
+        // Copies of dims [j0, j1) of nr rows (lane i holds row i's centroid
+        // in cid_), 16 bytes each, spread over the warp; every lane takes
+        // part in the shuffles.
+        auto copy_rows = [&](int cid_, int nr, int j0, int j1) {
+            const int ch = (j1 - j0) >> 2;
+            if (ch == 0) return;
+            const int n = nr * ch;
+            for (int t0 = 0; t0 < n; t0 += 32) {
+                const int t = t0 + lane;
+                const int r = min(t / ch, 31);
+                const int id = __shfl_sync(FULL, cid_, r);
+                const int j = j0 + 4 * (t - r * ch);
+                if (t < n) cp_async16(stage + r * pitch + j, cent + static_cast<size_t>(id) * d + j);
+            }
+        };
+        int cid = lane < min(32, c) ? cid_of(lane) : 0;
+        copy_rows(cid, min(32, c), 0, dh);
+        cp_async_commit();
+        copy_rows(cid, min(32, c), dh, d);
+        cp_async_commit();
+        for (int c0 = 0, r = 0; c0 < c; c0 += 32, ++r) {
+            const int nr = min(32, c - c0);
+            const int nn = max(0, min(32, c - c0 - 32));  // next round's rows
+            const int cidn = lane < nn ? cid_of(c0 + 32 + lane) : 0;
+            float acc = 0.0f;
+            cp_async_wait_group<1>();  // this round's first half
+            __syncwarp();
+            if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, 0, dh, acc);
+            __syncwarp();
+            copy_rows(cidn, nn, 0, dh);
+            cp_async_commit();
+            cp_async_wait_group<1>();  // this round's second half
+            __syncwarp();
+            if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, dh, d, acc);
+            __syncwarp();
+            copy_rows(cidn, nn, dh, d);
+            cp_async_commit();
+            if (lane < nr) {
+                const float score = METRIC == METRIC_L2 ? acc : -acc;
+                const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cid);
+                if (in_regs) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (i == r) kr[i] = key;
+                } else {
+                    keys[c0 + lane] = key;
+                }
+            }
+            cid = cidn;
         }
         cp_async_wait_all();
         __syncwarp();
-        if (lane < nr) {
-            const float* row = stage + lane * pitch;
-            float acc = 0.0f;
-            if (v4) {
-#pragma unroll 4
-                for (int jj = 0; jj < d; jj += 4) {
-                    const float4 a = *reinterpret_cast<const float4*>(qs + jj);
-                    const float4 b = *reinterpret_cast<const float4*>(row + jj);
-                    if (METRIC == METRIC_L2) {
-                        acc = sq_add(acc, a.x, b.x);
-                        acc = sq_add(acc, a.y, b.y);
-                        acc = sq_add(acc, a.z, b.z);
-                        acc = sq_add(acc, a.w, b.w);
-                    } else {
-                        acc = ip_add(acc, a.x, b.x);
-                        acc = ip_add(acc, a.y, b.y);
-                        acc = ip_add(acc, a.z, b.z);
-                        acc = ip_add(acc, a.w, b.w);
-                    }
-                }
-            } else {
+    } else {
+        for (int c0 = 0, r = 0; c0 < c; c0 += 32, ++r) {
+            const int nr = min(32, c - c0);
+            const int cidr = lane < nr ? cid_of(c0 + lane) : 0;
+            for (int rr = 0; rr < nr; ++rr) {
+                const float* src = cent + static_cast<size_t>(__shfl_sync(FULL, cidr, rr)) * d;
+                float* dst = stage + rr * pitch;
+                for (int j = lane; j < d; j += 32) cp_async4(dst + j, src + j);
+            }
+            cp_async_wait_all();
+            __syncwarp();
+            if (lane < nr) {
+                const float* row = stage + lane * pitch;
+                float acc = 0.0f;
                 for (int jj = 0; jj < d; ++jj)
                     acc = METRIC == METRIC_L2 ? sq_add(acc, qs[jj], row[jj]) : ip_add(acc, qs[jj], row[jj]);
+                const float score = METRIC == METRIC_L2 ? acc : -acc;
+                const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cidr);
+                if (in_regs) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (i == r) kr[i] = key;
+                } else {
+                    keys[c0 + lane] = key;
+                }
             }
-            const float score = METRIC == METRIC_L2 ? acc : -acc;
-            keys[c0 + lane] = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cidr);
+            __syncwarp();
         }
-        __syncwarp();
     }
     // The m smallest keys, ascending.  Up to 128 candidates: each key's rank
     // is the number of smaller keys (keys are distinct: the centroid is in
     // the low bits), and it goes to that position.
-    if (c <= 128) {
+    if (in_regs) {
         uint64_t kk[4];
         int rank[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const int e = r * 32 + lane;
-            kk[r] = e < c ? keys[e] : KEY_MAX;
+            kk[r] = r * 32 + lane < c ? kr[r] : KEY_MAX;
             rank[r] = 0;
         }
         // Every key, broadcast from the lane that holds it.
@@ -1603,6 +1673,7 @@ __device__ inline void coarse_exact_best(uint64_t* keys, int c, const float* qs,
         }
         return;
     }
+    __syncwarp();
     // More: sorted blocks of 256 merged into the running best 256.
     uint64_t t[8];
 #pragma unroll
@@ -1676,19 +1747,24 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
         }
     }
     const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
-    __syncwarp();  // every pair has been read before the first key is written
-    // Centroids that can be among the m best.
+    __syncwarp();  // every pair has been read, and the histogram too
+    // Centroids that can be among the m best: ids in keys, and the first
+    // 256 also in the histogram's space.
     int c = 0;
 #pragma unroll
     for (int r = 0; r < PER; ++r) {
         const int e = r * 32 + lane;
         const bool keep = e < nlist && lo[r] <= U;
         const unsigned bal = __ballot_sync(FULL, keep);
-        if (keep) keys[c + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint64_t>(e);
+        if (keep) {
+            const int at = c + __popc(bal & ((1u << lane) - 1u));
+            keys[at] = static_cast<uint64_t>(e);
+            if (at < 256) hist[at] = e;
+        }
         c += __popc(bal);
     }
     __syncwarp();
-    coarse_exact_best<METRIC>(keys, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
+    coarse_exact_best<METRIC>(keys, hist, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
 }
 
 // The coarse step for more than 2048 lists, in two tensor-core launches.
@@ -1784,7 +1860,7 @@ __global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __res
         c += __popc(bal);
     }
     __syncwarp();
-    coarse_exact_best<METRIC>(keys, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
+    coarse_exact_best<METRIC>(keys, nullptr, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
 }
 
 // ---------------------------------------------------------------------------

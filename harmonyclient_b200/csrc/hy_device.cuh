@@ -72,6 +72,12 @@ __device__ inline void cp_async4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Closes the group of this thread's asynchronous copies issued since the
+// last commit (an empty group when there were none).
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's committed groups are still pending.
+template <int N>
+__device__ inline void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Plain arrival (count 1) on a CTA-local mbarrier.
 __device__ inline void mbar_arrive_cta(uint64_t* bar) {
