@@ -1227,49 +1227,68 @@ __device__ inline float kth_bound_stream(Get get, int cnt, int k, int* hist, int
 }
 
 // k-th bound of a dense first-pass buffer in one read, held in registers:
-// lane l reads entries l, l + 32, ... (entry(e) = {score, bound}) and keeps
-// the M smallest upper values (score + bound) it sees; U is the k-th
-// smallest of those 32*M values
-// (32*M >= k).  Every kept value is an entry's, so at least k entries lie at
-// or below U; values were only left out, so U is at or above the k-th
-// smallest upper value of the whole buffer.  U is that exact k-th value
-// unless one lane read more than M of the k smallest.  With cnt >= k every
-// lane keeps all its entries or M of them, so the k-th kept value is an
-// entry's, never the padding (0xffffffff).
+// lane l reads entries l, l + 32, ... (entry(e) = {score, bound}), four at a
+// time, and keeps the M smallest upper values (score + bound) it sees: the
+// four are sorted and merged into the kept M (the elementwise minimum of
+// the kept values and the four reversed is a bitonic sequence holding the M
+// smallest, which a bitonic merge sorts).  U is then an upper bound on the
+// k-th smallest of the 32*M kept values (32*M >= k): the kept values'
+// k-th, searched bit by bit over 16 bits below the bits they all share, and
+// the upper edge of the final bin.  Every kept value is an entry's, so at
+// least k entries lie at or below U; values were only left out, so U is at
+// or above the k-th smallest upper value of the whole buffer.  With
+// cnt >= k every lane keeps all its entries or M of them, so the k-th kept
+// value is an entry's, never the padding (0xffffffff).
 template <int M, typename Entry>
 __device__ inline float dense_kth_regs(Entry entry, int cnt, int k, int lane) {
+    static_assert(M >= 4 && (M & (M - 1)) == 0, "M: a power of two, at least 4");
+    auto cx = [](uint32_t& x, uint32_t& y) {
+        const uint32_t lo = min(x, y);
+        y = max(x, y);
+        x = lo;
+    };
     uint32_t a[M];
 #pragma unroll
     for (int i = 0; i < M; ++i) a[i] = 0xffffffffu;
-#pragma unroll 4
-    for (int e = lane; e < cnt; e += 32) {
-        const float2 v = entry(e);
-        uint32_t h = f2o(v.x + v.y);
+    for (int e0 = lane; e0 < cnt; e0 += 128) {
+        uint32_t b[4];
 #pragma unroll
-        for (int i = 0; i < M; ++i) {  // insertion into the ascending a[]
-            const uint32_t lo = min(a[i], h);
-            h = max(a[i], h);
-            a[i] = lo;
+        for (int i = 0; i < 4; ++i) {
+            const int e = e0 + 32 * i;
+            b[i] = 0xffffffffu;
+            if (e < cnt) {
+                const float2 v = entry(e);
+                b[i] = f2o(v.x + v.y);
+            }
         }
+        cx(b[0], b[1]);
+        cx(b[2], b[3]);
+        cx(b[0], b[2]);
+        cx(b[1], b[3]);
+        cx(b[1], b[2]);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[M - 4 + i] = min(a[M - 4 + i], b[3 - i]);
+#pragma unroll
+        for (int st = M / 2; st > 0; st >>= 1)
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+                if ((i & st) == 0) cx(a[i], a[i + st]);
     }
-    // The k-th smallest kept value, bit by bit below the bits every kept
-    // value shares: R is kept as the prefix of the answer; a bit is set when
-    // fewer than k kept values lie at or below R with that bit clear and
-    // every lower bit set.
     const uint32_t mn = __reduce_min_sync(FULL, a[0]);
     const uint32_t mx = __reduce_max_sync(FULL, a[M - 1]);
     if (mn == mx) return o2f(mn);
     const int top = 31 - __clz(mn ^ mx);
+    const int low = top > 15 ? top - 15 : 0;
     uint32_t R = mn & ~((2u << top) - 1u);
 #pragma unroll 1
-    for (int bit = top; bit >= 0; --bit) {
+    for (int bit = top; bit >= low; --bit) {
         const uint32_t T = R | ((1u << bit) - 1u);
         int c = 0;
 #pragma unroll
         for (int i = 0; i < M; ++i) c += a[i] <= T ? 1 : 0;
         if (static_cast<int>(__reduce_add_sync(FULL, static_cast<unsigned>(c))) < k) R |= 1u << bit;
     }
-    return o2f(R);
+    return o2f(R | ((1u << low) - 1u));
 }
 
 // Warp tighten of a query whose first-pass list was scanned densely: the
