@@ -460,6 +460,150 @@ __global__ void item_fill_kernel(const int64_t* __restrict__ item_off, const int
     }
 }
 
+// The inversion in two launches (nlist <= INVERT_SMEM_LISTS).  The first
+// counts pairs per list in shared memory (each CTA a contiguous range of
+// `per` pairs, loads in flight eight at a time) and adds the counts to
+// w.pair_cnt; the last CTA to finish (a ticket on w.done after a fence)
+// turns the counts into pair offsets and item offsets, zeroes the fill
+// counters and resets the ticket.  The second places the pairs (as
+// probe_fill_smem_kernel) and writes the item descriptors.
+__device__ inline int64_t probe_list(const int64_t* __restrict__ probes, int64_t i, int wd, int nprobe, int j0) {
+    return probes[(i / wd) * nprobe + j0 + i % wd];
+}
+
+__global__ void __launch_bounds__(512) invert_count_kernel(const int64_t* __restrict__ probes, int nq, int nprobe,
+                                                           int j0, int j1, int nlist, int64_t per,
+                                                           const int32_t* __restrict__ list_size, int rs, int qg,
+                                                           BatchWork w) {
+    extern __shared__ int h[];  // [nlist]
+    __shared__ int s_last;
+    __shared__ long long part[512];
+    const int t = threadIdx.x;
+    const int wd = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * wd;
+    const int64_t a = blockIdx.x * per, b = min(n, a + per);
+    for (int l = t; l < nlist; l += blockDim.x) h[l] = 0;
+    __syncthreads();
+    for (int64_t i0 = a; i0 < b; i0 += 8 * 512) {
+        int64_t l[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int64_t i = i0 + u * 512 + t;
+            l[u] = i < b ? probe_list(probes, i, wd, nprobe, j0) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (l[u] >= 0) atomicAdd(&h[l[u]], 1);
+    }
+    __syncthreads();
+    for (int l = t; l < nlist; l += blockDim.x)
+        if (h[l]) atomicAdd(&w.pair_cnt[l], h[l]);
+    __threadfence();
+    __syncthreads();
+    if (t == 0) s_last = atomicAdd(w.done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // Last CTA: pair offsets and item offsets (thread t: a contiguous run
+    // of lists), fill counters zeroed, ticket reset.
+    const int run = (nlist + 511) / 512;
+    const int la = min(nlist, t * run), lb = min(nlist, la + run);
+    long long sp = 0, si = 0;
+    for (int l = la; l < lb; ++l) {
+        const int c = __ldcg(&w.pair_cnt[l]), sz = list_size[l];
+        sp += c;
+        si += (c > 0 && sz > 0) ? static_cast<long long>((c + qg - 1) / qg) * ((sz + rs - 1) / rs) : 0;
+        w.pair_fill[l] = 0;
+    }
+    // Two exclusive scans over the 512 runs (pairs, then items).
+    for (int pass = 0; pass < 2; ++pass) {
+        const long long mine = pass == 0 ? sp : si;
+        part[t] = mine;
+        __syncthreads();
+        for (int o = 1; o < 512; o <<= 1) {
+            const long long v = t >= o ? part[t - o] : 0;
+            __syncthreads();
+            part[t] += v;
+            __syncthreads();
+        }
+        long long acc = part[t] - mine;
+        for (int l = la; l < lb; ++l) {
+            const int c = __ldcg(&w.pair_cnt[l]), sz = list_size[l];
+            if (pass == 0) {
+                w.pair_off[l] = acc;
+                acc += c;
+            } else {
+                w.item_off[l] = acc;
+                acc += (c > 0 && sz > 0) ? static_cast<long long>((c + qg - 1) / qg) * ((sz + rs - 1) / rs) : 0;
+            }
+        }
+        if (t == 511) {
+            if (pass == 0)
+                w.pair_off[nlist] = part[511];
+            else
+                w.item_off[nlist] = part[511];
+        }
+        __syncthreads();
+    }
+    if (t == 0) *w.done = 0u;
+}
+
+__global__ void __launch_bounds__(512) invert_fill_kernel(const int64_t* __restrict__ probes, int nq, int nprobe,
+                                                          int j0, int j1, int nlist, int64_t per,
+                                                          const int32_t* __restrict__ list_size, int rs,
+                                                          BatchWork w) {
+    extern __shared__ int h[];  // [nlist] counts, then ranks; [nlist] bases
+    int* base = h + nlist;
+    const int t = threadIdx.x;
+    const int wd = j1 - j0;
+    const int64_t n = static_cast<int64_t>(nq) * wd;
+    const int64_t a = blockIdx.x * per, b = min(n, a + per);
+    for (int l = t; l < nlist; l += blockDim.x) h[l] = 0;
+    __syncthreads();
+    for (int64_t i0 = a; i0 < b; i0 += 8 * 512) {
+        int64_t l[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int64_t i = i0 + u * 512 + t;
+            l[u] = i < b ? probe_list(probes, i, wd, nprobe, j0) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (l[u] >= 0) atomicAdd(&h[l[u]], 1);
+    }
+    __syncthreads();
+    for (int l = t; l < nlist; l += blockDim.x) {
+        base[l] = h[l] ? atomicAdd(&w.pair_fill[l], h[l]) : 0;
+        h[l] = 0;
+    }
+    __syncthreads();
+    for (int64_t i0 = a; i0 < b; i0 += 8 * 512) {
+        int64_t l[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int64_t i = i0 + u * 512 + t;
+            l[u] = i < b ? probe_list(probes, i, wd, nprobe, j0) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (l[u] >= 0) {
+                const int64_t i = i0 + u * 512 + t;
+                w.pairs[w.pair_off[l[u]] + base[l[u]] + atomicAdd(&h[l[u]], 1)] = static_cast<int32_t>(i / wd);
+            }
+    }
+    // Item descriptors {list, query group, row slice} below item_cap, one
+    // warp per list.
+    const int lane = t & 31;
+    for (int64_t l = blockIdx.x * 16 + (t >> 5); l < nlist; l += gridDim.x * 16) {
+        const int64_t ia = w.item_off[l], ib = w.item_off[l + 1];
+        const int nrs = max(1, (list_size[l] + rs - 1) / rs);
+        for (int64_t g = ia + lane; g < ib && g < w.item_cap; g += 32) {
+            const int k = static_cast<int>(g - ia);
+            w.items[g] = make_int4(static_cast<int>(l), k / nrs, k % nrs, 0);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 struct BatchedParams {
     const unsigned char* abf;       // tensor-core image of the arena (bf16 or e4m3)
@@ -2366,6 +2510,20 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
     const int64_t n = static_cast<int64_t>(nq) * (j1 - j0);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.pair_cnt, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
+    if (nlist <= INVERT_SMEM_LISTS && w.done) {
+        // About 160 CTAs of 512 threads (at least 4096 pairs each).
+        const int64_t per = std::max<int64_t>(4096, (n + 159) / 160);
+        const int nblk = static_cast<int>(std::max<int64_t>(1, (n + per - 1) / per));
+        invert_count_kernel<<<nblk, 512, static_cast<size_t>(nlist) * 4, s>>>(probes, nq, nprobe, j0, j1, nlist, per,
+                                                                              list_size, rs, qg, w);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const int fblk = std::max(nblk, (nlist + 15) / 16 < 148 ? (nlist + 15) / 16 : 148);
+        const int64_t fper = (n + fblk - 1) / fblk;
+        invert_fill_kernel<<<fblk, 512, static_cast<size_t>(nlist) * 8, s>>>(probes, nq, nprobe, j0, j1, nlist,
+                                                                             std::max<int64_t>(fper, 1), list_size, rs,
+                                                                             w);
+        return cudaGetLastError();
+    }
     if ((e = cudaMemsetAsync(w.pair_fill, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
     if (nlist <= INVERT_SMEM_LISTS) {
         // About 160 CTAs of 512 threads (at least 512 pairs each).

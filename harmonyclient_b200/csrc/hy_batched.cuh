@@ -73,6 +73,7 @@ struct BatchWork {
     int32_t* overflow;   // [1 + nq]: count, then query ids
     int32_t* big;        // [1 + nq]: queries re-ranked by the CTA kernel (count, then ids)
     int32_t* big2;       // [1 + nq]: queries tightened by the CTA kernel (count, then ids)
+    unsigned int* done = nullptr;  // [1], zero between launches: the inversion's ticket
 };
 
 // Inverts probe columns [j0, j1) of every query into per-list query groups

@@ -82,6 +82,14 @@ struct DevBuf {
         bytes = want;
         return HY_OK;
     }
+    // ensure(n), and zero the bytes when they were just allocated.
+    int ensure_zeroed(size_t n) {
+        const bool fresh = n > bytes;
+        int rc = ensure(n);
+        if (rc == HY_OK && fresh && cudaMemset(p, 0, bytes) != cudaSuccess)
+            return fail(HY_ERR_CUDA, "cudaMemset of a new buffer failed");
+        return rc;
+    }
     template <class T>
     T* as() const {
         return static_cast<T*>(p);
@@ -211,6 +219,7 @@ struct hy_index {
     DevBuf b_qs;              // e4m3 per-query scales
     DevBuf b_big;             // queries re-ranked by the CTA kernel
     DevBuf b_qb, b_qn, b_thr, b_pcnt, b_pfill, b_poff, b_pairs, b_icnt, b_ioff, b_work, b_cand, b_ccnt, b_ovf, b_items;
+    DevBuf b_done;            // the probe inversion's ticket (zero between launches)
     DevBuf b_fq, b_fpr, b_fD, b_fI, b_fcnt, b_fbtot;  // device-side exact fallback
     // coarse quantiser on the tensor cores (bf16 form): the centroids as a
     // one-list index (image, row aux, tile aux, norms, list offsets/sizes)
@@ -557,6 +566,7 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
     HY_RET(h->b_icnt.ensure(nlist * sizeof(int32_t)));
     HY_RET(h->b_ioff.ensure((nlist + 1) * sizeof(int64_t)));
     HY_RET(h->b_work.ensure(sizeof(unsigned int)));
+    HY_RET(h->b_done.ensure_zeroed(sizeof(unsigned int)));
     HY_RET(h->b_cand.ensure(m * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(m * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((m + 1) * sizeof(int32_t)));
@@ -581,6 +591,7 @@ int scan_lists(hy_index* h, size_t m, const float* qq, size_t k, size_t nprobe, 
     w.item_cnt = h->b_icnt.as<int32_t>();
     w.item_off = h->b_ioff.as<int64_t>();
     w.work = h->b_work.as<unsigned int>();
+    w.done = h->b_done.as<unsigned int>();
     int32_t* ovf = h->b_ovf.as<int32_t>();
     HY_CUDA(cudaMemsetAsync(h->b_ccnt.p, 0, m * sizeof(int32_t), s));
     HY_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
@@ -968,6 +979,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_icnt.ensure(nlist * sizeof(int32_t)));
     HY_RET(h->b_ioff.ensure((nlist + 1) * sizeof(int64_t)));
     HY_RET(h->b_work.ensure(sizeof(unsigned int)));
+    HY_RET(h->b_done.ensure_zeroed(sizeof(unsigned int)));
     HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
@@ -1027,6 +1039,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     w.item_cnt = h->b_icnt.as<int32_t>();
     w.item_off = h->b_ioff.as<int64_t>();
     w.work = h->b_work.as<unsigned int>();
+    w.done = h->b_done.as<unsigned int>();
     w.cand = h->b_cand.as<uint64_t>();
     w.cand_cnt = h->b_ccnt.as<int32_t>();
     w.big = h->b_big.as<int32_t>();
