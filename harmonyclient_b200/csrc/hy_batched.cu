@@ -2050,6 +2050,33 @@ __device__ void rerank_warp_query(const ArenaLayout& L, const float* __restrict_
                                   int rmax, bool l2, float cN, bool exact, const float* qs, uint64_t* sl,
                                   float* __restrict__ Dq, int64_t* __restrict__ Iq, int lane) {
     uint64_t key[KR], srt[KR];
+    if (exact && rmax == 0) {
+        // Certified exact tensor-core distances: the k smallest keys
+        // (distance, arena row) are the answer, the same ones the bounded
+        // selection below would keep.
+#pragma unroll
+        for (int r = 0; r < KR; ++r) {
+            const int e = r * 32 + lane;
+            srt[r] = e < n ? cq[e] : KEY_MAX;
+        }
+        warp_sort<KR>(srt, lane);
+#pragma unroll
+        for (int r = 0; r < KR; ++r) {
+            const int e = r * 32 + lane;
+            if (e < k) {
+                const uint64_t kk = srt[r];
+                if (kk == KEY_MAX) {
+                    Dq[e] = l2 ? FLT_MAX : -FLT_MAX;
+                    Iq[e] = -1;
+                } else {
+                    const float sc = o2f(static_cast<uint32_t>(kk >> 32));
+                    Dq[e] = l2 ? sc : -sc;
+                    Iq[e] = ids[kk & 0xffffffffu];
+                }
+            }
+        }
+        return;
+    }
     float lo[KR];
 #pragma unroll
     for (int r = 0; r < KR; ++r) {
