@@ -44,7 +44,7 @@ METRIC = "QPS at recall@10>=0.95, 1 B200: learned+BF16 vs plain FP32 scan; scan 
 KNOWN_TRAFFIC = {
     ("c2", "plain", 1_000_000, 10_000, 64): 216_530_000_000,
     ("c2", "plain-lm", 1_000_000, 10_000, 64): 492_300_000,
-    ("c2", "learned", 1_000_000, 10_000, 64): 295_400_000,
+    ("c2", "learned", 1_000_000, 10_000, 64): 261_650_000,
     ("c2", "bf16", 1_000_000, 10_000, 64): 325_000_000,
 }
 TRAFFIC_SOURCE = {

@@ -2237,12 +2237,17 @@ __global__ void __launch_bounds__(256) rerank_kernel(ArenaLayout L, const float*
         s_over = cnt > capq ? 1 : 0;
     }
     stage_query(L, q + static_cast<size_t>(qi) * L.d, qs);
+    // Certified exact tensor-core distances need no bounds (e = 0).
+    const bool no_bounds = qexact != nullptr && qexact[qi] != 0 && rmax == 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t key = cq[i];
         const int64_t row = static_cast<int64_t>(key & 0xffffffffu);
         const float sc = o2f(static_cast<uint32_t>(key >> 32));
-        const float2 xa = xaux[row];
-        const float e = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+        float e = 0.0f;
+        if (!no_bounds) {
+            const float2 xa = xaux[row];
+            e = fmaf(xa.x, ec.aq, fmaf(xa.y, ec.bq, err_row_const(xn[row], l2, cN) + ec.cq));
+        }
         hi[i] = f2o(sc + e);
         lo[i] = sc - e;
     }
