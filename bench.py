@@ -45,7 +45,7 @@ KNOWN_TRAFFIC = {
     ("c2", "plain", 1_000_000, 10_000, 64): 216_530_000_000,
     ("c2", "plain-lm", 1_000_000, 10_000, 64): 492_300_000,
     ("c2", "learned", 1_000_000, 10_000, 64): 261_650_000,
-    ("c2", "bf16", 1_000_000, 10_000, 64): 325_000_000,
+    ("c2", "bf16", 1_000_000, 10_000, 64): 292_800_000,
 }
 TRAFFIC_SOURCE = {
     "plain": "query-major scan_plain_kernel, 1,000-query ncu capture scaled x10 "
