@@ -628,6 +628,7 @@ struct BatchedParams {
     unsigned int* work;             // work-queue counter
     int* err;
     int nlist, nkb, rs, capq, metric;
+    int ksplit;                     // 1: A k-blocks 2j, 2j+1 (hi, lo) both take query k-block j
     int ns;                         // stages in the list k-block ring (NS_MIN..NS_MAX)
     int dense_max;                  // lists of at most this many rows: dense items (0 = none)
     float cK, cN;                   // error-bound constants (see err_coef)
@@ -720,10 +721,11 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     using Slot = ItemSlot<QG>;
     extern __shared__ unsigned char sm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
-    const int nkb = p.nkb;
+    const int nkb = p.nkb;                  // list (A) k-blocks per row
+    const int nkbq = nkb >> p.ksplit;       // query (B) k-blocks per row
     unsigned char* sB = base;                                        // 2 slots x nkb x BKB (queries)
     const int ns = p.ns;                                             // stages in the ring
-    unsigned char* sA = sB + 2 * static_cast<size_t>(nkb) * BKB;     // ns x 16 KiB (list k-blocks)
+    unsigned char* sA = sB + 2 * static_cast<size_t>(nkbq) * BKB;    // ns x 16 KiB (list k-blocks)
     Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(ns) * KB_BYTES);  // [2], 1024-aligned
     static_assert(offsetof(Slot, xn) % 16 == 0 && offsetof(Slot, sc) % 16 == 0 && sizeof(Slot) % 16 == 0,
                   "ItemSlot alignment");
@@ -855,19 +857,19 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             // of the accumulator): every 16-byte chunk is its own
             // asynchronous copy, all in flight at once; empty query slots are
             // zero-filled.
-            unsigned char* dst = sB + static_cast<size_t>(b) * nkb * BKB;
-            const size_t qstride = static_cast<size_t>(nkb) * 128;
+            unsigned char* dst = sB + static_cast<size_t>(b) * nkbq * BKB;
+            const size_t qstride = static_cast<size_t>(nkbq) * 128;
             for (int i = gt; i < QG; i += 32 * N_GATHER) {
                 const int col = group_col<QG>(i);
                 if (i < nqv) {
                     const unsigned char* src = p.qb + static_cast<size_t>(grp[i]) * qstride;
-                    for (int kb = 0; kb < nkb; ++kb)
+                    for (int kb = 0; kb < nkbq; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
                             cp_async16(dst + kb * BKB + col * 128 + (((c ^ (col & 7)) & 7) << 4),
                                        src + kb * 128 + c * 16);
                 } else {
-                    for (int kb = 0; kb < nkb; ++kb)
+                    for (int kb = 0; kb < nkbq; ++kb)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
                             *reinterpret_cast<uint4*>(dst + kb * BKB + col * 128 + (c << 4)) = make_uint4(0, 0, 0, 0);
@@ -924,7 +926,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
                 const int ntiles = slot[b].ntiles;
                 if (ntiles < 0) break;
                 tc::fence_after_sync();
-                const uint32_t b0 = smem_u32(sB + static_cast<size_t>(b) * nkb * BKB);
+                const uint32_t b0 = smem_u32(sB + static_cast<size_t>(b) * nkbq * BKB);
                 for (int t = 0; t < ntiles && ok; ++t, ++tile_it) {
                     const int buf = tile_it & 1;
                     if (!wait_or_abort(&acce[buf], ((tile_it >> 1) & 1u) ^ 1u, p.err, vabort)) {
@@ -949,7 +951,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk) {
                             const uint64_t ad = tc::sdesc_sw128(a0 + kk * 32);
-                            const uint64_t bd = tc::sdesc_sw128(b0 + kb * BKB + kk * 32);
+                            const uint64_t bd = tc::sdesc_sw128(b0 + (kb >> p.ksplit) * BKB + kk * 32);
                             if constexpr (F8)
                                 tc::mma_e4m3(dcol, ad, bd, idesc, (kb | kk) != 0 ? 1u : 0u);
                             else
@@ -1594,8 +1596,14 @@ __global__ void __launch_bounds__(256) tighten_warp2_kernel(const float* __restr
 // ---------------------------------------------------------------------------
 // The coarse quantiser on the tensor cores.  The centroids form a one-list
 // index of their own (rows padded to whole 128-row tiles with zeros): its
-// bf16 image, per-row {|c~|, |c - c~|}, squared norms (the sequential f32
-// sum the arena's rows get) and per-tile maxima.
+// split bf16 image, per-row bound terms, squared norms (the sequential f32
+// sum the arena's rows get) and per-tile maxima.  Split image: each value c
+// as hi = bf16(c) and lo = bf16(c - hi); a tile holds, per 64 dimensions,
+// the hi k-block then the lo k-block, and the batched kernel multiplies
+// both by the same query k-block, so the accumulator sums q~.(hi + lo)
+// (|c - hi - lo| <= 2^-16 |c|, against 2^-8 |c| for one bf16).  Bound terms
+// {|(|hi| + |lo|)|, |c - hi - lo|}: the first covers |hi + lo| and the
+// magnitudes the accumulation adds.
 __global__ void rowmajor_image_kernel(const float* __restrict__ x, int64_t n, int d, int nkb, int64_t rows,
                                       unsigned char* __restrict__ out) {
     const int w = nkb * 64;
@@ -1604,9 +1612,12 @@ __global__ void rowmajor_image_kernel(const float* __restrict__ x, int64_t n, in
     const int64_t r = i / w;
     const int j = static_cast<int>(i % w);
     const float v = (r < n && j < d) ? x[r * d + j] : 0.0f;
-    unsigned char* dst =
-        out + ((r >> 7) * nkb + (j >> 6)) * KB_BYTES + tc::kblock_offset(static_cast<uint32_t>(r & 127), j & 63);
-    *reinterpret_cast<__nv_bfloat16*>(dst) = __float2bfloat16_rn(v);
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+    const uint32_t off = tc::kblock_offset(static_cast<uint32_t>(r & 127), j & 63);
+    unsigned char* tile = out + (r >> 7) * (2 * nkb) * KB_BYTES;
+    *reinterpret_cast<__nv_bfloat16*>(tile + (2 * (j >> 6)) * KB_BYTES + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(tile + (2 * (j >> 6) + 1) * KB_BYTES + off) = lo;
 }
 
 __global__ void rowmajor_aux_kernel(const float* __restrict__ x, int64_t n, int d, int64_t rows,
@@ -1618,9 +1629,12 @@ __global__ void rowmajor_aux_kernel(const float* __restrict__ x, int64_t n, int 
     if (r < n)
         for (int j = lane; j < d; j += 32) {
             const float v = x[r * d + j];
-            const float vb = __bfloat162float(__float2bfloat16_rn(v));
-            nn = fmaf(vb, vb, nn);
-            ee = fmaf(v - vb, v - vb, ee);
+            const float hi = __bfloat162float(__float2bfloat16_rn(v));
+            const float lo = __bfloat162float(__float2bfloat16_rn(v - hi));
+            const float m = fabsf(hi) + fabsf(lo);
+            const float e = (v - hi) - lo;  // exact: both differences are of nearby values
+            nn = fmaf(m, m, nn);
+            ee = fmaf(e, e, ee);
         }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -2363,8 +2377,10 @@ cudaError_t launch_to_bf16_arena(const ArenaLayout& L, const float* codes, int64
 }
 
 // Error-bound constants for dimension d (see err_coef).
-static void err_consts(int d, bool f8, float* cK, float* cN) {
-    const int K = f8 ? (d + 127) / 128 * 128 : (d + 63) / 64 * 64;
+// ksplit: every dimension accumulates two products (the split centroid
+// image's hi and lo parts).
+static void err_consts(int d, bool f8, float* cK, float* cN, bool ksplit = false) {
+    const int K = (f8 ? (d + 127) / 128 * 128 : (d + 63) / 64 * 64) * (ksplit ? 2 : 1);
     const double u = 1.0 / 16777216.0, inflate = 1.0 + 1.0 / 128.0;
     *cK = static_cast<float>((K + 8) * u * inflate);
     *cN = static_cast<float>((3.0 * d + 16) * u * inflate);
@@ -2410,7 +2426,7 @@ cudaError_t launch_fb_scatter(const int32_t* ovf, const float* fD, const int64_t
 cudaError_t launch_centroid_image(const float* cent, int nlist, int d, void* img, float2* aux, float2* tile_aux,
                                   float* xn, cudaStream_t s) {
     const int64_t rows = (static_cast<int64_t>(nlist) + TM - 1) / TM * TM;
-    const int nkb = (d + 63) / 64;
+    const int nkb = (d + 63) / 64;  // 64-dimension blocks (two k-blocks each in the image)
     rowmajor_image_kernel<<<grid_for(rows * nkb * 64, 256), 256, 0, s>>>(cent, nlist, d, nkb, rows,
                                                                          static_cast<unsigned char*>(img));
     rowmajor_aux_kernel<<<grid_for(rows * 32, 256), 256, 0, s>>>(cent, nlist, d, rows, aux, xn);
@@ -2438,7 +2454,7 @@ cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q
                                  const float* cxn, const float2* caux, const float4* qaux, int d, int metric, int m,
                                  int64_t* out_idx, float* out_score, cudaStream_t s) {
     float cK, cN;
-    err_consts(d, false, &cK, &cN);
+    err_consts(d, false, &cK, &cN, true);  // the split centroid image
     int warps = 4;
     while (warps > 1 && coarse_refine_smem(nlist, d, warps) > 200 * 1024) warps >>= 1;
     const size_t smem = coarse_refine_smem(nlist, d, warps);
@@ -2461,7 +2477,7 @@ cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, const fl
                               const float4* qaux, int d, int metric, float* thr, cudaStream_t s) {
     if (S > 1024 || m > S) return cudaErrorInvalidValue;
     float cK, cN;
-    err_consts(d, false, &cK, &cN);
+    err_consts(d, false, &cK, &cN, true);  // the split centroid image
     coarse_thr_kernel<<<(nq + 7) / 8, 256, 0, s>>>(cand, nq, S, m, cxn, caux, qaux, metric, cK, cN, thr);
     return cudaGetLastError();
 }
@@ -2474,7 +2490,7 @@ cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int n
     const size_t smem = coarse_refine_smem(0, d, warps);
     if (smem > 200 * 1024 || m > 256) return cudaErrorInvalidValue;
     float cK, cN;
-    err_consts(d, false, &cK, &cN);
+    err_consts(d, false, &cK, &cN, true);  // the split centroid image
     const dim3 grid((nq + warps - 1) / warps);
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -2589,9 +2605,9 @@ int batched_group_size(int d, bool f8) {
 
 template <int QG, bool F8>
 static cudaError_t launch_batched_t(BatchedParams p, int nsm, cudaStream_t s) {
-    p.ns = batched_stages<QG>(p.nkb);
+    p.ns = batched_stages<QG>(p.nkb >> p.ksplit);
     if (p.ns == 0) return cudaErrorInvalidValue;
-    const size_t smem = batched_smem<QG>(p.nkb, p.ns);
+    const size_t smem = batched_smem<QG>(p.nkb >> p.ksplit, p.ns);
     cudaError_t e = cudaFuncSetAttribute(batched_scan_kernel<QG, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -2622,13 +2638,14 @@ cudaError_t launch_batched_scan(const BatchedLaunch& b, const BatchWork& w, int*
     p.work = w.work;
     p.err = err;
     p.nlist = b.nlist;
-    p.nkb = b.f8 ? (b.d + 127) / 128 : (b.d + 63) / 64;
+    p.ksplit = b.ksplit ? 1 : 0;
+    p.nkb = (b.f8 ? (b.d + 127) / 128 : (b.d + 63) / 64) << p.ksplit;
     p.rs = b.rs;
     p.capq = b.capq;
     p.metric = b.metric;
     p.dense_max = std::min(b.dense_max, b.capq);
     p.xaux = b.xaux;
-    err_consts(b.d, b.f8, &p.cK, &p.cN);
+    err_consts(b.d, b.f8, &p.cK, &p.cN, b.ksplit);
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.work, 0, sizeof(unsigned int), s)) != cudaSuccess) return e;
     switch (b.qg * 2 + (b.f8 ? 1 : 0)) {

@@ -16,6 +16,8 @@ inline size_t bf16_image_bytes(int64_t rows, int d) {
     const int nkb = (d + 63) / 64;
     return static_cast<size_t>(rows / BATCH_ROW_ALIGN) * nkb * BATCH_KB_BYTES;
 }
+// The split (hi, lo) bf16 image of launch_centroid_image.
+inline size_t bf16_split_image_bytes(int64_t rows, int d) { return 2 * bf16_image_bytes(rows, d); }
 
 // Bytes of the e4m3 image (128-byte k-blocks of 128 dimensions).
 inline size_t f8_image_bytes(int64_t rows, int d) {
@@ -100,9 +102,11 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
                            DenseFirst df);
 
 // The coarse quantiser on the tensor cores (bf16 form).  The centroids
-// (row-major, nlist x d) as a one-list index: bf16 image, per-row
-// {|c~|, |c - c~|}, per-tile maxima and squared norms, rows padded to whole
-// 128-row tiles (img: bf16_image_bytes(rows), aux/xn: rows, tile_aux: rows/128).
+// (row-major, nlist x d) as a one-list index: split bf16 image (per 64
+// dimensions a hi k-block, bf16(c), then a lo k-block, bf16(c - hi); launched
+// with BatchedLaunch::ksplit), per-row {|(|hi| + |lo|)|, |c - hi - lo|},
+// per-tile maxima and squared norms, rows padded to whole 128-row tiles
+// (img: bf16_split_image_bytes(rows), aux/xn: rows, tile_aux: rows/128).
 cudaError_t launch_centroid_image(const float* cent, int nlist, int d, void* img, float2* aux, float2* tile_aux,
                                   float* xn, cudaStream_t s);
 // Work of one coarse launch over nq queries: list_off[2], list_size[1] of the
@@ -153,6 +157,7 @@ struct BatchedLaunch {
     int nlist, d, rs, capq, metric, nsm;
     int qg = 128;     // queries per group (batched_group_size)
     bool f8 = false;  // e4m3 operands
+    bool ksplit = false;  // abf is a split image (launch_centroid_image): two k-blocks per query k-block
     // Lists of at most dense_max rows (capped at capq) are scanned densely:
     // every row's f32 score lands at the row's offset in the list within the
     // upper half of the query's candidate buffer, with no threshold test, and the

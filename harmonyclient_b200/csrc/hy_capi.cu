@@ -832,7 +832,7 @@ bool coarse_on_tensor(const hy_index* h, size_t nprobe) {
 int ensure_centroid_image(hy_index* h, cudaStream_t s) {
     if (h->cimg_valid) return HY_OK;
     const size_t rows = (h->nlist + hy::BATCH_ROW_ALIGN - 1) / hy::BATCH_ROW_ALIGN * hy::BATCH_ROW_ALIGN;
-    HY_RET(h->c_img.ensure(hy::bf16_image_bytes((int64_t)rows, (int)h->d)));
+    HY_RET(h->c_img.ensure(hy::bf16_split_image_bytes((int64_t)rows, (int)h->d)));
     HY_RET(h->c_aux.ensure(rows * sizeof(float2)));
     HY_RET(h->c_taux.ensure(rows / hy::BATCH_ROW_ALIGN * sizeof(float2)));
     HY_RET(h->c_norm.ensure(rows * sizeof(float)));
@@ -898,6 +898,7 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     b.nsm = h->nsm;
     b.qg = qg;
     b.f8 = false;
+    b.ksplit = true;
     if (nlist <= 2048) {
         // Every (query, centroid) score, then the exact best.
         w.item_cap = (int64_t)ngroups * ns_full;
