@@ -239,17 +239,26 @@ __global__ void prep_queries_f8_kernel(const float* __restrict__ q, int nq, int 
 }
 
 // Queries: bf16 rows padded to nkb*64, and per query {|q|^2 (sequential f32,
-// the exact arithmetic's value), |q|, |q~|, |q - q~|}.
-__global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, int nkb,
-                                    __nv_bfloat16* __restrict__ qb, float4* __restrict__ qaux, float amax,
-                                    int32_t* __restrict__ qexact) {
-    const int i = blockIdx.x;
-    if (i >= nq) return;
+// the exact arithmetic's value), |q|, |q~|, |q - q~|}.  One warp per query
+// (PREP_WARPS per CTA): the lanes convert and reduce, and lane 0 takes the
+// sequential sum from the row staged in shared memory.
+constexpr int PREP_WARPS = 8;
+constexpr int PREP_DMAX = 768;  // the bf16 forms' largest d
+__global__ void __launch_bounds__(32 * PREP_WARPS) prep_queries_kernel(const float* __restrict__ q, int nq, int d,
+                                                                       int nkb, __nv_bfloat16* __restrict__ qb,
+                                                                       float4* __restrict__ qaux, float amax,
+                                                                       int32_t* __restrict__ qexact) {
+    __shared__ float rowbuf[PREP_WARPS][PREP_DMAX];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * PREP_WARPS + warp;
+    if (i >= nq) return;  // whole warp
     const float* src = q + static_cast<size_t>(i) * d;
+    float* row = rowbuf[warp];
     float nn = 0.0f, ee = 0.0f;
     bool integral = true;
-    for (int j = threadIdx.x; j < nkb * 64; j += blockDim.x) {
+    for (int j = lane; j < nkb * 64; j += 32) {
         const float v = j < d ? src[j] : 0.0f;
+        if (j < d) row[j] = v;
         integral = integral && v == rintf(v) && fabsf(v) <= 256.0f;
         const __nv_bfloat16 b = __float2bfloat16_rn(v);
         qb[static_cast<size_t>(i) * nkb * 64 + j] = b;
@@ -257,26 +266,18 @@ __global__ void prep_queries_kernel(const float* __restrict__ q, int nq, int d, 
         nn = fmaf(vb, vb, nn);
         ee = fmaf(v - vb, v - vb, ee);
     }
-    __shared__ float red[2][4];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         nn += __shfl_xor_sync(FULL, nn, o);
         ee += __shfl_xor_sync(FULL, ee, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        red[0][threadIdx.x >> 5] = nn;
-        red[1][threadIdx.x >> 5] = ee;
-    }
-    const int all_integral = __syncthreads_and(integral ? 1 : 0);
-    if (threadIdx.x == 0) {
+    const bool all_integral = __all_sync(FULL, integral);
+    __syncwarp();
+    if (lane == 0) {
         float s = 0.0f;
-        for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(src[j], src[j]));
-        float tn = 0.0f, te = 0.0f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            tn += red[0][w];
-            te += red[1][w];
-        }
-        qaux[i] = make_float4(s, sqrtf(s), sqrtf(tn), sqrtf(te));
+#pragma unroll 8
+        for (int j = 0; j < d; ++j) s = __fadd_rn(s, __fmul_rn(row[j], row[j]));
+        qaux[i] = make_float4(s, sqrtf(s), sqrtf(nn), sqrtf(ee));
         if (qexact) qexact[i] = (amax >= 0.0f && all_integral && s + amax < 8388608.0f) ? 1 : 0;
     }
 }
@@ -1540,26 +1541,29 @@ __global__ void __launch_bounds__(256) tighten_warp_kernel(const float* __restri
                                                            float* __restrict__ thr, DenseFirst df) {
     __shared__ int hist[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int qi = blockIdx.x * 8 + warp;
-    if (qi >= nq) return;  // whole warp
-    const int cnt = w.cand_cnt[qi];
-    if (df.dense_max > 0) {
-        const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
-        if (l0 >= 0 && df.list_size[l0] <= df.dense_max) return;  // tighten_dense_kernel's
-    }
-    if (cnt < k) return;
-    if (cnt > capq) return;  // overflowed: left for the re-rank to report
-    if (cnt > TIGHTEN_WARP_MAX) {
-        if (lane == 0) {
-            if (cnt > 2 * TIGHTEN_WARP_MAX)
-                w.big2[1 + atomicAdd(&w.big2[0], 1)] = qi;
-            else
-                w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
+    auto one = [&](int qi) {
+        const int cnt = w.cand_cnt[qi];
+        if (cnt < k) return;
+        if (cnt > capq) return;  // overflowed: left for the re-rank to report
+        if (cnt > TIGHTEN_WARP_MAX) {
+            if (lane == 0) {
+                if (cnt > 2 * TIGHTEN_WARP_MAX)
+                    w.big2[1 + atomicAdd(&w.big2[0], 1)] = qi;
+                else
+                    w.big[1 + atomicAdd(&w.big[0], 1)] = qi;
+            }
+            return;
         }
+        tighten_warp_query<TIGHTEN_WARP_MAX / 32>(qi, cnt, xn, xaux, qaux, w, capq, k, metric == 1, cK, cN, thr,
+                                                  hist[warp], lane);
+    };
+    if (df.dense_max > 0) {
+        // The queries tighten_dense_kernel listed (first-pass list not dense).
+        const int n = w.rest[0];
+        for (int li = blockIdx.x * 8 + warp; li < n; li += gridDim.x * 8) one(w.rest[1 + li]);
         return;
     }
-    tighten_warp_query<TIGHTEN_WARP_MAX / 32>(qi, cnt, xn, xaux, qaux, w, capq, k, metric == 1, cK, cN, thr,
-                                              hist[warp], lane);
+    for (int qi = blockIdx.x * 8 + warp; qi < nq; qi += gridDim.x * 8) one(qi);
 }
 
 // Queries whose first-pass list was scanned densely, one warp each.
@@ -1572,7 +1576,11 @@ __global__ void __launch_bounds__(256) tighten_dense_kernel(const float* __restr
     const int qi = blockIdx.x * 8 + warp;
     if (qi >= nq) return;  // whole warp
     const int64_t l0 = df.probes[static_cast<int64_t>(qi) * df.nprobe];
-    if (l0 < 0 || df.list_size[l0] > df.dense_max) return;
+    if (l0 < 0 || df.list_size[l0] > df.dense_max) {
+        // Thresholded first-pass list: tighten_warp_kernel's.
+        if (lane == 0) w.rest[1 + atomicAdd(&w.rest[0], 1)] = qi;
+        return;
+    }
     tighten_dense_query(qi, w.cand_cnt[qi], df.list_off[l0], xn, xaux, qaux, df.tile_aux, df.tile_xn, metric == 1, cK,
                         cN, w, capq, k, thr, lane);
 }
@@ -2396,10 +2404,12 @@ cudaError_t launch_tighten(const float* xn, const float2* xaux, const float4* qa
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.big2, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
     if (df.dense_max > 0) {
+        if ((e = cudaMemsetAsync(w.rest, 0, sizeof(int32_t), s)) != cudaSuccess) return e;
         tighten_dense_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    tighten_warp_kernel<<<(nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k, metric, cK, cN, thr, df);
+    tighten_warp_kernel<<<df.dense_max > 0 ? 2 * nsm : (nq + 7) / 8, 256, 0, s>>>(xn, xaux, qaux, nq, w, capq, k,
+                                                                                  metric, cK, cN, thr, df);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     tighten_warp2_kernel<<<2 * nsm, 256, 0, s>>>(xn, xaux, qaux, w, capq, k, metric, cK, cN, thr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2513,8 +2523,9 @@ cudaError_t launch_prep_queries(const float* q, int nq, int d, void* qb, float4*
         prep_queries_f8_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 127) / 128, static_cast<unsigned char*>(qb), qaux,
                                                   qscale);
     } else {
-        prep_queries_kernel<<<nq, 128, 0, s>>>(q, nq, d, (d + 63) / 64, static_cast<__nv_bfloat16*>(qb), qaux, amax,
-                                               qexact);
+        if (d > PREP_DMAX) return cudaErrorInvalidValue;
+        prep_queries_kernel<<<(nq + PREP_WARPS - 1) / PREP_WARPS, 32 * PREP_WARPS, 0, s>>>(
+            q, nq, d, (d + 63) / 64, static_cast<__nv_bfloat16*>(qb), qaux, amax, qexact);
     }
     return cudaGetLastError();
 }

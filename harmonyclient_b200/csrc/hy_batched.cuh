@@ -75,6 +75,7 @@ struct BatchWork {
     int32_t* overflow;   // [1 + nq]: count, then query ids
     int32_t* big;        // [1 + nq]: queries re-ranked by the CTA kernel (count, then ids)
     int32_t* big2;       // [1 + nq]: queries tightened by the CTA kernel (count, then ids)
+    int32_t* rest = nullptr;  // [1 + nq]: queries whose first-pass list was not dense (count, then ids)
     unsigned int* done = nullptr;  // [1], zero between launches: the inversion's ticket
 };
 

@@ -984,7 +984,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     HY_RET(h->b_cand.ensure(qc * capq * sizeof(uint64_t)));
     HY_RET(h->b_ccnt.ensure(qc * sizeof(int32_t)));
     HY_RET(h->b_ovf.ensure((qc + 1) * sizeof(int32_t)));
-    HY_RET(h->b_big.ensure(2 * (qc + 1) * sizeof(int32_t)));
+    HY_RET(h->b_big.ensure(3 * (qc + 1) * sizeof(int32_t)));
     // Exact fallback on the device: every overflowed query of a chunk is
     // searched again by the plain scan over the same probe lists.
     const size_t fbcap = qc;
@@ -1045,6 +1045,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     w.cand_cnt = h->b_ccnt.as<int32_t>();
     w.big = h->b_big.as<int32_t>();
     w.big2 = w.big + (qc + 1);
+    w.rest = w.big2 + (qc + 1);
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
