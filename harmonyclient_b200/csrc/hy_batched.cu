@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(512) invert_count_kernel(const int64_t* __rest
                                                            BatchWork w) {
     extern __shared__ int h[];  // [nlist]
     __shared__ int s_last;
-    __shared__ long long part[512];
+    __shared__ long long wpart[16];
     const int t = threadIdx.x;
     const int wd = j1 - j0;
     const int64_t n = static_cast<int64_t>(nq) * wd;
@@ -516,18 +516,30 @@ __global__ void __launch_bounds__(512) invert_count_kernel(const int64_t* __rest
         si += (c > 0 && sz > 0) ? static_cast<long long>((c + qg - 1) / qg) * ((sz + rs - 1) / rs) : 0;
         w.pair_fill[l] = 0;
     }
-    // Two exclusive scans over the 512 runs (pairs, then items).
+    // Two exclusive scans over the 512 runs (pairs, then items): within each
+    // warp by shuffles, then over the 16 warp totals.
+    const int lane = t & 31, warp = t >> 5;
     for (int pass = 0; pass < 2; ++pass) {
         const long long mine = pass == 0 ? sp : si;
-        part[t] = mine;
-        __syncthreads();
-        for (int o = 1; o < 512; o <<= 1) {
-            const long long v = t >= o ? part[t - o] : 0;
-            __syncthreads();
-            part[t] += v;
-            __syncthreads();
+        long long incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += u;
         }
-        long long acc = part[t] - mine;
+        if (lane == 31) wpart[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            long long x = lane < 16 ? wpart[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+                const long long u = __shfl_up_sync(FULL, x, o);
+                if (lane >= o) x += u;
+            }
+            if (lane < 16) wpart[lane] = x;  // inclusive over warps
+        }
+        __syncthreads();
+        long long acc = incl - mine + (warp > 0 ? wpart[warp - 1] : 0);
         for (int l = la; l < lb; ++l) {
             const int c = __ldcg(&w.pair_cnt[l]), sz = list_size[l];
             if (pass == 0) {
@@ -540,9 +552,9 @@ __global__ void __launch_bounds__(512) invert_count_kernel(const int64_t* __rest
         }
         if (t == 511) {
             if (pass == 0)
-                w.pair_off[nlist] = part[511];
+                w.pair_off[nlist] = wpart[15];
             else
-                w.item_off[nlist] = part[511];
+                w.item_off[nlist] = wpart[15];
         }
         __syncthreads();
     }
@@ -2570,8 +2582,8 @@ cudaError_t launch_invert_probes(const int64_t* probes, int nq, int nprobe, int 
     cudaError_t e;
     if ((e = cudaMemsetAsync(w.pair_cnt, 0, nlist * sizeof(int32_t), s)) != cudaSuccess) return e;
     if (nlist <= INVERT_SMEM_LISTS && w.done) {
-        // About 160 CTAs of 512 threads (at least 4096 pairs each).
-        const int64_t per = std::max<int64_t>(4096, (n + 159) / 160);
+        // Up to about one CTA of 512 threads per SM (at least 1024 pairs each).
+        const int64_t per = std::max<int64_t>(1024, (n + 147) / 148);
         const int nblk = static_cast<int>(std::max<int64_t>(1, (n + per - 1) / per));
         invert_count_kernel<<<nblk, 512, static_cast<size_t>(nlist) * 4, s>>>(probes, nq, nprobe, j0, j1, nlist, per,
                                                                               list_size, rs, qg, w);

@@ -261,16 +261,23 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
         // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks
         // (this thread's column quarter: k-block qt).
         {
+            // 16 columns per TMEM load in a loop that is not unrolled: the
+            // GELU code stays small enough for the instruction cache.
             const int cb = qt;
-            uint32_t u[64];
-            tc::tmem_ld64(lane_addr + cb * 64, u);
+#pragma unroll 1
+            for (int c2 = 0; c2 < 4; ++c2) {
+                uint32_t u[16];
+                tc::tmem_ld16(lane_addr + cb * 64 + 16 * c2, u);
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                float h[8];
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int c = 2 * c2 + hh;
+                    float h[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    h[j] = gelu(__uint_as_float(u[8 * c + j]) + __ldg(params + MLP_B1 + cb * 64 + 8 * c + j));
-                *reinterpret_cast<uint4*>(sA + cb * 16384 + tid * 128 + (((c ^ (tid & 7)) & 7) << 4)) = pack8_bf16(h);
+                    for (int j = 0; j < 8; ++j)
+                        h[j] = gelu(__uint_as_float(u[8 * hh + j]) + __ldg(params + MLP_B1 + cb * 64 + 8 * c + j));
+                    *reinterpret_cast<uint4*>(sA + cb * 16384 + tid * 128 + (((c ^ (tid & 7)) & 7) << 4)) =
+                        pack8_bf16(h);
+                }
             }
         }
     }
@@ -296,13 +303,16 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
         // each thread over its column quarter.
         {
             const int cb = qt;
-            uint32_t u[64];
-            tc::tmem_ld64(lane_addr + cb * 64, u);
+#pragma unroll 1
+            for (int c2 = 0; c2 < 4; ++c2) {
+                uint32_t u[16];
+                tc::tmem_ld16(lane_addr + cb * 64 + 16 * c2, u);
 #pragma unroll
-            for (int j = 0; j < 64; ++j) {
-                const int n = cb * 64 + j;
-                const float a = gelu(__uint_as_float(u[j]) + __ldg(params + MLP_B2 + n));
-                acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
+                for (int j = 0; j < 16; ++j) {
+                    const int n = cb * 64 + 16 * c2 + j;
+                    const float a = gelu(__uint_as_float(u[j]) + __ldg(params + MLP_B2 + n));
+                    acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
+                }
             }
         }
         if (qt > 0) s_part[qt - 1][tid] = acc;
