@@ -448,13 +448,26 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                     // live rows can stay under its threshold (the partial,
                     // which only grows, already exceeds it) is dropped from
                     // the tile without the block's other 16 dimensions.
+                    auto dead_here = [&](int qi, float a) -> bool {
+                        const float lb = first ? a : __fadd_rn(spw[qi * 32], a);
+                        return !((alive >> qi) & 1u) || lb > s_thr[qi];
+                    };
                     auto half_dead = [&](int qi, float a) -> bool {
                         if (!prune) return false;
-                        const float lb = first ? a : __fadd_rn(spw[qi * 32], a);
-                        const bool dead = !((alive >> qi) & 1u) || lb > s_thr[qi];
-                        if (!__all_sync(FULL, dead)) return false;
+                        if (!__all_sync(FULL, dead_here(qi, a))) return false;
                         alive &= ~(1u << qi);
                         return true;
+                    };
+                    // Both queries of a pair in one warp reduction.
+                    auto half_dead2 = [&](int qa, float a0, int qb, float a1, bool& da, bool& db) {
+                        da = db = false;
+                        if (!prune) return;
+                        const unsigned m = (dead_here(qa, a0) ? 1u : 0u) | (dead_here(qb, a1) ? 2u : 0u);
+                        const unsigned all = __reduce_and_sync(FULL, m);
+                        da = (all & 1u) != 0u;
+                        db = (all & 2u) != 0u;
+                        if (da) alive &= ~(1u << qa);
+                        if (db) alive &= ~(1u << qb);
                     };
                     uint32_t todo = live;
                     while (todo) {
@@ -467,7 +480,8 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                             const float* yb = qbase + qb * L.row_pitch;
                             float a0 = 0.0f, a1 = 0.0f;
                             chain2<L2, 0, 4>(ya, yb, xr, a0, a1);
-                            const bool da = half_dead(qa, a0), db = half_dead(qb, a1);
+                            bool da, db;
+                            half_dead2(qa, a0, qb, a1, da, db);
                             computed += 4 - (da ? 1 : 0) - (db ? 1 : 0);
                             if (!da && !db) {
                                 chain2<L2, 4, 8>(ya, yb, xr, a0, a1);
