@@ -215,6 +215,11 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     __shared__ int s_qid[QG];
     __shared__ int s_next, s_ntiles, s_nrows, s_nqv, s_done, s_list;
     __shared__ long long s_row0;
+    // The next item, claimed and described by warp 0 while the CTA scans the
+    // current one (scalars only: two CTAs of the pitch-32 scan fill an SM's
+    // shared memory to within a few hundred bytes).
+    __shared__ int n_ntiles, n_nrows, n_nqv, n_done, n_list;
+    __shared__ long long n_row0, n_pq, s_pq;
     // Per-warp ring tags: tile index within the item and block of each slot.
     __shared__ int s_tag_tile[LM_WARPS][R];
     __shared__ int s_tag_b[LM_WARPS][R];
@@ -232,40 +237,55 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
     unsigned long long loaded = 0, computed = 0, possible = 0, possible_sums = 0;
     const int64_t nitems = p.item_off[p.nlist];
 
+    // Lane 0 of warp 0: claim the next item and load its descriptor into
+    // n_* (n_pq: the offset of its query ids in p.pairs).
+    auto prefetch = [&]() {
+        if (lane != 0) return;
+        // No further items once a wait anywhere has given up.
+        const unsigned int g = *reinterpret_cast<volatile int*>(p.err) ? 0xffffffffu : atomicAdd(p.work, 1u);
+        if (g == 0xffffffffu || static_cast<int64_t>(g) >= nitems) {
+            n_done = 1;
+            return;
+        }
+        const int4 it = decode_item(p, g);
+        const int l = it.x;
+        const int lrow0 = it.z * p.rs;
+        n_nqv = min(QG, p.pair_cnt[l] - it.y * QG);
+        n_nrows = min(p.rs, p.list_size[l] - lrow0);
+        n_ntiles = (n_nrows + 31) >> 5;
+        n_row0 = p.list_off[l] + lrow0;
+        n_list = l;
+        n_pq = p.pair_off[l] + static_cast<int64_t>(it.y) * QG;
+        n_done = 0;
+    };
+    if (warp == 0) prefetch();
+
     for (;;) {
-        __syncthreads();  // previous item done (and, first time, barriers initialised)
+        __syncthreads();  // previous item done, the next one prefetched (and, first time, barriers initialised)
         if (threadIdx.x == 0) {
-            // No further items once a wait anywhere has given up.
-            const unsigned int g = *reinterpret_cast<volatile int*>(p.err) ? 0xffffffffu : atomicAdd(p.work, 1u);
-            s_done = 1;
-            if (g != 0xffffffffu && static_cast<int64_t>(g) < nitems) {
-                const int4 it = decode_item(p, g);
-                const int l = it.x;
-                const int nq_l = p.pair_cnt[l];
-                const int lrow0 = it.z * p.rs;
-                s_nqv = min(QG, nq_l - it.y * QG);
-                s_nrows = min(p.rs, p.list_size[l] - lrow0);
-                s_ntiles = (s_nrows + 31) >> 5;
-                s_row0 = p.list_off[l] + lrow0;
-                s_list = l;
-                s_next = 0;
-                s_done = 0;
-                // query ids of the group
-                const int32_t* pq = p.pairs + p.pair_off[l] + static_cast<int64_t>(it.y) * QG;
-                for (int j = 0; j < QG; ++j) s_qid[j] = j < s_nqv ? pq[j] : -1;
-            }
+            s_done = n_done;
+            s_nqv = n_nqv;
+            s_nrows = n_nrows;
+            s_ntiles = n_ntiles;
+            s_row0 = n_row0;
+            s_list = n_list;
+            s_pq = n_pq;
+            s_next = 0;
         }
         __syncthreads();
         if (s_done) break;
         const int nqv = s_nqv;
-        // Thresholds (score units; +inf when the query has none).
+        const int32_t* pq = p.pairs + s_pq;
+        // Query ids and thresholds (score units; +inf when the query has none).
         if (threadIdx.x < QG) {
             const int j = threadIdx.x;
+            const int qid = j < nqv ? pq[j] : -1;
             float t = -INFINITY;
             if (j < nqv) {
-                const uint32_t key = p.thr ? p.thr[s_qid[j]] : 0xffffffffu;
+                const uint32_t key = p.thr ? p.thr[qid] : 0xffffffffu;
                 t = key == 0xffffffffu ? INFINITY : o2f(key);
             }
+            s_qid[j] = qid;
             s_thr[j] = t;
         }
         // The group's queries in the arena's block-padded layout.
@@ -277,11 +297,13 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
                 while (b + 1 < L.nb && e >= L.boff[b + 1]) ++b;
                 const int w = L.bstart[b + 1] - L.bstart[b];
                 const int jj = e - L.boff[b];
-                if (jj < w) v = p.q[static_cast<size_t>(s_qid[j]) * L.d + L.bstart[b] + jj];
+                // The query id from the pair list (s_qid is being written).
+                if (jj < w) v = p.q[static_cast<size_t>(pq[j]) * L.d + L.bstart[b] + jj];
             }
             qs[i] = v;
         }
         if (p.triangle) {
+            __syncthreads();  // s_qid and s_thr are read below
             const float* cl = p.cent + static_cast<size_t>(s_list) * L.d;
             for (int j = warp; j < QG; j += LM_WARPS) {
                 float c = 0.0f;
@@ -325,6 +347,7 @@ __global__ void __launch_bounds__(LM_WARPS * 32, MULTI ? 1 : 2)
             }
         }
         __syncthreads();
+        if (warp == 0) prefetch();  // the next item, while the other warps start on this one
         const int ntiles = s_ntiles, nrows = s_nrows;
         const int64_t row0 = s_row0;
         const uint32_t qmask = nqv >= 32 ? 0xffffffffu : ((1u << nqv) - 1u);
