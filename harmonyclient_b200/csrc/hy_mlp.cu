@@ -148,8 +148,8 @@ __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __res
 // Inference on the tensor cores.  The weights are packed once (mlp_pack) into
 // the tcgen05 B-operand image: W1 as 256 rows (output features) x 64 inputs,
 // one 128-byte-swizzled K-major k-block of 32 KiB; W2 as 256 rows x 256
-// inputs, four such k-blocks.  One CTA of 512 threads takes 128 queries
-// (query = TMEM lane; four threads per query split every layer's 256 columns):
+// inputs, four such k-blocks.  One CTA of 1024 threads takes 128 queries
+// (query = TMEM lane; eight threads per query split every layer's 256 columns):
 // features -> bf16 A tile -> MMA (M 128, N 256,
 // K 64) -> bias + GELU -> bf16 A tiles (4 k-blocks) -> MMA (K 256) -> bias +
 // GELU -> dot with W3 -> nprobe, all on chip.
@@ -181,9 +181,10 @@ __device__ inline uint4 pack8_bf16(const float* v) {
     return r;
 }
 
-constexpr int MI_QUARTERS = 4;  // threads per query row (column quarters of every 256-wide layer)
+constexpr int MI_PARTS = 8;                 // threads per query row (column parts of every 256-wide layer)
+constexpr int MI_COLS = MLP_H / MI_PARTS;   // columns of a layer per thread
 
-__global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
+__global__ void __launch_bounds__(128 * MI_PARTS, 1) mlp_infer_kernel(const float* __restrict__ pscore, int m, int P,
                                                            const float* __restrict__ mu, const float* __restrict__ sd,
                                                            const unsigned char* __restrict__ wimg,
                                                            const float* __restrict__ params, float margin,
@@ -197,10 +198,9 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
     __shared__ uint64_t bar_w, bar_m;
     __shared__ uint32_t tbase;
     __shared__ int s_ok;
-    __shared__ float s_part[MI_QUARTERS - 1][128];  // layer-3 partial sums of column quarters 1..3
-    // Four threads per query row: warps w, w + 4, w + 8, w + 12 share TMEM
-    // lane quadrant w % 4 and take column quarters 0..3 (one 64-column
-    // k-block each) of every 256-wide layer.
+    // MI_PARTS threads per query row: warps w, w + 4, w + 8, ... share TMEM
+    // lane quadrant w % 4 and take column parts 0, 1, ... (MI_COLS columns
+    // each) of every 256-wide layer.
     const int warp = threadIdx.x >> 5, qt = warp >> 2;
     const int tid = threadIdx.x & 127;  // the query row within the tile
     const int row = blockIdx.x * 128 + tid;
@@ -223,8 +223,9 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
         const float* sc = pscore + static_cast<size_t>(valid ? row : 0) * P;
         const float s0 = valid ? sc[0] : 0.0f;
         const float a0 = fabsf(s0) + 1e-6f;
+        constexpr int FC = 8 / MI_PARTS > 0 ? 8 / MI_PARTS : 1;  // 8-feature chunks per thread
 #pragma unroll
-        for (int c = 2 * qt; c < 2 * qt + 2; ++c) {
+        for (int c = FC * qt; c < FC * qt + FC; ++c) {
             float f[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -259,22 +260,23 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
     const uint32_t lane_addr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
     if (ok) {
         // Layer 1 epilogue: H1 = bf16(GELU(Z1 + b1)) into the 4 A k-blocks
-        // (this thread's column quarter: k-block qt).
+        // (this thread's MI_COLS columns).
         {
             // 16 columns per TMEM load in a loop that is not unrolled: the
             // GELU code stays small enough for the instruction cache.
-            const int cb = qt;
 #pragma unroll 1
-            for (int c2 = 0; c2 < 4; ++c2) {
+            for (int c2 = 0; c2 < MI_COLS / 16; ++c2) {
+                const int col0 = MI_COLS * qt + 16 * c2;  // first of the 16 columns
+                const int cb = col0 >> 6;                 // its A k-block
                 uint32_t u[16];
-                tc::tmem_ld16(lane_addr + cb * 64 + 16 * c2, u);
+                tc::tmem_ld16(lane_addr + col0, u);
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) {
-                    const int c = 2 * c2 + hh;
+                    const int c = ((col0 & 63) >> 3) + hh;  // 8-column chunk within the k-block
                     float h[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
-                        h[j] = gelu(__uint_as_float(u[8 * hh + j]) + __ldg(params + MLP_B1 + cb * 64 + 8 * c + j));
+                        h[j] = gelu(__uint_as_float(u[8 * hh + j]) + __ldg(params + MLP_B1 + col0 + 8 * hh + j));
                     *reinterpret_cast<uint4*>(sA + cb * 16384 + tid * 128 + (((c ^ (tid & 7)) & 7) << 4)) =
                         pack8_bf16(h);
                 }
@@ -300,26 +302,31 @@ __global__ void __launch_bounds__(128 * MI_QUARTERS, 1) mlp_infer_kernel(const f
     tc::fence_after_sync();
     if (ok) {
         // Layer 2 epilogue and layer 3: y = bf16(GELU(Z2 + b2)) . bf16(W3) + b3,
-        // each thread over its column quarter.
+        // each thread over its MI_COLS columns.
         {
-            const int cb = qt;
 #pragma unroll 1
-            for (int c2 = 0; c2 < 4; ++c2) {
+            for (int c2 = 0; c2 < MI_COLS / 16; ++c2) {
+                const int col0 = MI_COLS * qt + 16 * c2;
                 uint32_t u[16];
-                tc::tmem_ld16(lane_addr + cb * 64 + 16 * c2, u);
+                tc::tmem_ld16(lane_addr + col0, u);
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int n = cb * 64 + 16 * c2 + j;
+                    const int n = col0 + j;
                     const float a = gelu(__uint_as_float(u[j]) + __ldg(params + MLP_B2 + n));
                     acc = fmaf(bf16r(a), bf16r(__ldg(params + MLP_W3 + n)), acc);
                 }
             }
         }
-        if (qt > 0) s_part[qt - 1][tid] = acc;
+        // Layer-3 partial sums of column parts 1.. in the A tiles' space: the
+        // second MMA, which read them, has completed (bar_m).
+        if (qt > 0) reinterpret_cast<float*>(sA)[(qt - 1) * 128 + tid] = acc;
     }
     __syncthreads();
     if (ok && qt == 0) {
-        const float y = (((acc + s_part[0][tid]) + s_part[1][tid]) + s_part[2][tid]) + params[MLP_B3];
+        float y = acc;
+#pragma unroll
+        for (int j = 0; j < MI_PARTS - 1; ++j) y += reinterpret_cast<const float*>(sA)[j * 128 + tid];
+        y += params[MLP_B3];
         if (valid) {
             if (yout) yout[row] = y;
             if (probes) {
@@ -419,7 +426,7 @@ cudaError_t mlp_infer(const float* pscore, int m, int P, const float* mu, const 
     if (m <= 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MI_SMEM);
     if (e != cudaSuccess) return e;
-    mlp_infer_kernel<<<blocks(m, 128), 128 * MI_QUARTERS, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin,
+    mlp_infer_kernel<<<blocks(m, 128), 128 * MI_PARTS, MI_SMEM, s>>>(pscore, m, P, mu, sd, wimg, params, margin,
                                                                         probes, total, yout, err);
     return cudaGetLastError();
 }
