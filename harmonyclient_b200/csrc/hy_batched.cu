@@ -643,6 +643,7 @@ struct BatchedParams {
     int nlist, nkb, rs, capq, metric;
     int ksplit;                     // 1: A k-blocks 2j, 2j+1 (hi, lo) both take query k-block j
     int ns;                         // stages in the list k-block ring (NS_MIN..NS_MAX)
+    int nslot;                      // item slots (2 or SLOT_MAX)
     int dense_max;                  // lists of at most this many rows: dense items (0 = none)
     float cK, cN;                   // error-bound constants (see err_coef)
 };
@@ -657,8 +658,11 @@ constexpr int N_EPI = 8;
 constexpr int BATCH_THREADS = 32 * (W_EPI0 + N_EPI);
 constexpr int CB = 256;         // per-epilogue-warp candidate staging
 
-// Item metadata of one query slot (two slots: the item being scanned and the
-// next one being gathered).
+// Item metadata of one query slot.  Two slots hold the item being scanned and
+// the next one being gathered; a third lets the gather run a further item
+// ahead, since a slot only frees when the epilogue has finished its item.
+constexpr int SLOT_MAX = 3;
+constexpr int NS_SLOT3 = 5;   // three slots only when they leave this many stages
 constexpr int RS_MAX = 2048;  // largest row slice (rows staged per slot)
 template <int QG>
 struct ItemSlot {
@@ -680,12 +684,12 @@ struct ItemSlot {
 };
 
 // Dynamic shared memory of the batched kernel for query groups of QG, nkb
-// 128-byte k-blocks per row and ns stages.
+// 128-byte k-blocks per row, ns stages and nslot item slots.
 template <int QG>
-constexpr size_t batched_smem(int nkb, int ns) {
+constexpr size_t batched_smem(int nkb, int ns, int nslot) {
     constexpr int CW = QG / 2, CC = CW < 32 ? CW : 32;
-    return 1024 + 2 * static_cast<size_t>(nkb) * QG * 128 + static_cast<size_t>(ns) * KB_BYTES +
-           2 * sizeof(ItemSlot<QG>) + N_EPI * CW * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
+    return 1024 + nslot * static_cast<size_t>(nkb) * QG * 128 + static_cast<size_t>(ns) * KB_BYTES +
+           nslot * sizeof(ItemSlot<QG>) + N_EPI * CW * sizeof(float) + N_EPI * CB * (sizeof(int) + sizeof(uint64_t)) +
            N_EPI * 32 * CC * sizeof(float);
 }
 // Dynamic shared memory per CTA: the 227 KiB opt-in limit less room for the
@@ -694,9 +698,9 @@ constexpr size_t BATCHED_SMEM_CAP = 227 * 1024 - 256;
 
 // The deepest stage ring in [NS_MIN, NS_MAX] that fits (0: none fits).
 template <int QG>
-constexpr int batched_stages(int nkb) {
+constexpr int batched_stages(int nkb, int nslot = 2) {
     for (int ns = NS_MAX; ns >= NS_MIN; --ns)
-        if (batched_smem<QG>(nkb, ns) <= BATCHED_SMEM_CAP) return ns;
+        if (batched_smem<QG>(nkb, ns, nslot) <= BATCHED_SMEM_CAP) return ns;
     return 0;
 }
 
@@ -736,21 +740,22 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
     const int nkb = p.nkb;                  // list (A) k-blocks per row
     const int nkbq = nkb >> p.ksplit;       // query (B) k-blocks per row
-    unsigned char* sB = base;                                        // 2 slots x nkb x BKB (queries)
+    const int nsl = p.nslot;                                         // item slots
+    unsigned char* sB = base;                                        // nsl slots x nkb x BKB (queries)
     const int ns = p.ns;                                             // stages in the ring
-    unsigned char* sA = sB + 2 * static_cast<size_t>(nkbq) * BKB;    // ns x 16 KiB (list k-blocks)
-    Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(ns) * KB_BYTES);  // [2], 1024-aligned
+    unsigned char* sA = sB + static_cast<size_t>(nsl) * nkbq * BKB;  // ns x 16 KiB (list k-blocks)
+    Slot* slot = reinterpret_cast<Slot*>(sA + static_cast<size_t>(ns) * KB_BYTES);  // [nsl], 1024-aligned
     static_assert(offsetof(Slot, xn) % 16 == 0 && offsetof(Slot, sc) % 16 == 0 && sizeof(Slot) % 16 == 0,
                   "ItemSlot alignment");
-    float* sR = reinterpret_cast<float*>(slot + 2);                  // [N_EPI][CW] per-tile test bounds
+    float* sR = reinterpret_cast<float*>(slot + nsl);                // [N_EPI][CW] per-tile test bounds
     int* s_cq = reinterpret_cast<int*>(sR + N_EPI * CW);             // [N_EPI][CB]
     uint64_t* s_ck = reinterpret_cast<uint64_t*>(s_cq + N_EPI * CB);  // [N_EPI][CB]
     float* s_ip = reinterpret_cast<float*>(s_ck + N_EPI * CB);       // [N_EPI][32 lanes][CC] candidate chunks
 
-    __shared__ uint64_t full[NS_MAX], empty[NS_MAX], accf[2], acce[2], sfull[2], sfree[2];
+    __shared__ uint64_t full[NS_MAX], empty[NS_MAX], accf[2], acce[2], sfull[SLOT_MAX], sfree[SLOT_MAX];
     __shared__ uint32_t tbase;
     __shared__ int s_abort;
-    __shared__ long long s_g[2];
+    __shared__ long long s_g[SLOT_MAX];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool l2 = p.metric == 1;
@@ -764,6 +769,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         for (int i = 0; i < 2; ++i) {
             mbar_init(&accf[i], 1);
             mbar_init(&acce[i], N_EPI);
+        }
+        for (int i = 0; i < nsl; ++i) {
             mbar_init(&sfull[i], 32 * N_GATHER);
             mbar_init(&sfree[i], 1 + N_EPI);  // MMA commit + every epilogue warp
         }
@@ -781,8 +788,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         // ---------------- gather: fetch an item, decode it, stage its queries
         const int gt = threadIdx.x - 32 * W_GATHER0;  // 0..63
         for (uint32_t it = 0;; ++it) {
-            const int b = it & 1;
-            if (!wait_or_abort(&sfree[b], ((it >> 1) & 1u) ^ 1u, p.err, vabort)) break;
+            const int b = static_cast<int>(it % nsl);
+            if (!wait_or_abort(&sfree[b], ((it / nsl) & 1u) ^ 1u, p.err, vabort)) break;
             Slot& S = slot[b];
             // One index per slot: a gather thread may still be reading this
             // item's index while thread 0 already fetches the next one.
@@ -898,8 +905,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             int ls = 0;        // stage of the next copy
             uint32_t lph = 0;  // its ring round's parity
             for (uint32_t it = 0;; ++it) {
-                const int b = it & 1;
-                if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+                const int b = static_cast<int>(it % nsl);
+                if (!wait_or_abort(&sfull[b], (it / nsl) & 1u, p.err, vabort)) break;
                 const int ntiles = slot[b].ntiles;
                 if (ntiles < 0) break;
                 const int64_t tile0 = slot[b].row0 / TM;
@@ -934,8 +941,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
             uint32_t tile_it = 0;
             bool ok = true;
             for (uint32_t it = 0; ok; ++it) {
-                const int b = it & 1;
-                if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+                const int b = static_cast<int>(it % nsl);
+                if (!wait_or_abort(&sfull[b], (it / nsl) & 1u, p.err, vabort)) break;
                 const int ntiles = slot[b].ntiles;
                 if (ntiles < 0) break;
                 tc::fence_after_sync();
@@ -1012,8 +1019,8 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1) batched_scan_kernel(const __
         const float cf = l2 ? -2.0f : -1.0f;
         uint32_t tile_it = 0;
         for (uint32_t it = 0;; ++it) {
-            const int b = it & 1;
-            if (!wait_or_abort(&sfull[b], (it >> 1) & 1u, p.err, vabort)) break;
+            const int b = static_cast<int>(it % nsl);
+            if (!wait_or_abort(&sfull[b], (it / nsl) & 1u, p.err, vabort)) break;
             const Slot& S = slot[b];
             const int ntiles = S.ntiles;
             if (ntiles < 0) break;
@@ -2628,9 +2635,14 @@ int batched_group_size(int d, bool f8) {
 
 template <int QG, bool F8>
 static cudaError_t launch_batched_t(BatchedParams p, int nsm, cudaStream_t s) {
-    p.ns = batched_stages<QG>(p.nkb >> p.ksplit);
+    p.nslot = SLOT_MAX;
+    p.ns = batched_stages<QG>(p.nkb >> p.ksplit, SLOT_MAX);
+    if (p.ns < NS_SLOT3) {
+        p.nslot = 2;
+        p.ns = batched_stages<QG>(p.nkb >> p.ksplit, 2);
+    }
     if (p.ns == 0) return cudaErrorInvalidValue;
-    const size_t smem = batched_smem<QG>(p.nkb >> p.ksplit, p.ns);
+    const size_t smem = batched_smem<QG>(p.nkb >> p.ksplit, p.ns, p.nslot);
     cudaError_t e = cudaFuncSetAttribute(batched_scan_kernel<QG, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
