@@ -1700,6 +1700,12 @@ __global__ void coarse_items_kernel(int nq, int nlist, int64_t rows, int ngroups
 // Staging row pitch of coarse_refine_kernel (floats): d + 4 when d is a
 // multiple of 4 (16-byte rows), else d + 1 (conflict-free column reads).
 __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4 : d + 1; }
+// Shared memory per warp of the refine kernels: two copy barriers (16
+// bytes), 256 histogram bins, the query and a 32-row staging block.
+__host__ __device__ inline size_t refine_warp_bytes(int d) {
+    const size_t pitch = refine_pitch(d);
+    return (16 + 1024 + pitch * 4 + 32 * pitch * 4 + 15) & ~size_t(15);
+}
 
 // Exact coarse selection from the tensor-core scores.  Per query (one warp):
 // the upper half of cand holds nlist scores; with each centroid's error
@@ -1712,18 +1718,18 @@ __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4
 // order, separately rounded operations), and the m best (score, centroid)
 // keys, ascending with ties to the lower centroid, are written as
 // select_warp_kernel writes them.  The candidate keys overwrite the query's
-// pairs in cand.  Shared memory per warp: 256 histogram bins, the query and
-// a 32-row staging block of centroids.
+// pairs in cand.  Shared memory per warp: two copy barriers, 256 histogram
+// bins, the query and a 32-row staging block of centroids.
 // The exact m best of a query's c candidate centroids (ids in keys[0, c),
 // and in sids[0, c) when sids is given and c <= 256): exact FP32 coarse
 // scores with coarse_scores_kernel's arithmetic (dimension order, separately
 // rounded operations), 32 candidates per round (lane i sums row i), then
 // ordered by (score, centroid) and written as select_warp_kernel writes them.
-// With d a multiple of 4 the rows are staged in shared memory by 16-byte
-// asynchronous copies (row pitch d + 4, so a warp's 512-byte read takes the
-// minimum four wavefronts) in two dimension halves: while the lanes sum one
-// half of this round's rows, the copies of the other half of the next
-// round's rows are in flight.  Up to 128 candidates the scored keys stay in
+// With d a multiple of 4 the rows are staged in shared memory (row pitch
+// d + 4, so a warp's 512-byte read takes the minimum four wavefronts) in two
+// dimension halves, each lane's half-row by one bulk copy completing on the
+// half's barrier: while the lanes sum one half of this round's rows, the
+// copies of the other half of the next round's rows are in flight.  Up to 128 candidates the scored keys stay in
 // registers (lane i, round r: candidate 32 r + i); more are written back to
 // keys and merged through shared-memory-free warp sorts.
 template <int METRIC>
@@ -1747,10 +1753,40 @@ __device__ inline float coarse_dot(const float* qs, const float* row, int j0, in
     return acc;
 }
 
+// Ranks of a warp's c <= 32 R keys (lane i, round r: key 32 r + i in kr[r],
+// all c of them also in kbuf) among one another, and each of the m smallest
+// written at its rank.
+template <int R>
+__device__ inline void rank_write(const uint64_t (&kr)[4], const uint64_t* kbuf, int c, int m, int qi,
+                                  int64_t* __restrict__ out_idx, float* __restrict__ out_score, int lane) {
+    int rank[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) rank[i] = 0;
+    int e = 0;
+    for (; e + 1 < c; e += 2) {
+        const ulonglong2 two = *reinterpret_cast<const ulonglong2*>(kbuf + e);
+#pragma unroll
+        for (int i = 0; i < R; ++i) rank[i] += (two.x < kr[i] ? 1 : 0) + (two.y < kr[i] ? 1 : 0);
+    }
+    if (e < c) {
+        const uint64_t one = kbuf[e];
+#pragma unroll
+        for (int i = 0; i < R; ++i) rank[i] += one < kr[i] ? 1 : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        if (i * 32 + lane < c && rank[i] < m) {
+            out_idx[static_cast<int64_t>(qi) * m + rank[i]] = static_cast<int64_t>(kr[i] & 0xffffffffu);
+            if (out_score) out_score[static_cast<int64_t>(qi) * m + rank[i]] = o2f(static_cast<uint32_t>(kr[i] >> 32));
+        }
+    }
+}
+
 template <int METRIC>
-__device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c, const float* qs, float* stage,
-                                         int pitch, const float* __restrict__ cent, int d, int m, int qi,
-                                         int64_t* __restrict__ out_idx, float* __restrict__ out_score, int lane) {
+__device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, uint64_t* kbuf, uint64_t* bars, int c,
+                                         const float* qs, float* stage, int pitch, const float* __restrict__ cent,
+                                         int d, int m, int qi, int64_t* __restrict__ out_idx,
+                                         float* __restrict__ out_score, int* err, int lane) {
     // Fewer candidates than m (not reached when the bound holds m of them):
     // the missing probes are -1.
     for (int e = c + lane; e < m; e += 32) {
@@ -1764,43 +1800,60 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c,
     uint64_t kr[4] = {KEY_MAX, KEY_MAX, KEY_MAX, KEY_MAX};
     if (v4) {
         const int dh = ((d >> 1) + 3) & ~3;  // first half [0, dh), second [dh, d)
-        // Copies of dims [j0, j1) of nr rows (lane i holds row i's centroid
-        // in cid_), 16 bytes each, spread over the warp; every lane takes
-        // part in the shuffles.
-        auto copy_rows = [&](int cid_, int nr, int j0, int j1) {
-            const int ch = (j1 - j0) >> 2;
-            if (ch == 0) return;
-            const int n = nr * ch;
-            for (int t0 = 0; t0 < n; t0 += 32) {
-                const int t = t0 + lane;
-                const int r = min(t / ch, 31);
-                const int id = __shfl_sync(FULL, cid_, r);
-                const int j = j0 + 4 * (t - r * ch);
-                if (t < n) cp_async16(stage + r * pitch + j, cent + static_cast<size_t>(id) * d + j);
+        const uint32_t hb0 = static_cast<uint32_t>(dh) * 4u, hb1 = static_cast<uint32_t>(d - dh) * 4u;
+        if (lane == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+        // Phases of each half's barrier issued and consumed.
+        uint32_t iss0 = 0, iss1 = 0, use0 = 0, use1 = 0;
+        // Dims [j0, j0 + bytes / 4) of nr rows: lane i's row (centroid cid_)
+        // by one bulk copy completing on bar.
+        auto copy_half = [&](uint64_t* bar, int j0, uint32_t bytes, int cid_, int nr) {
+            fence_proxy_async();  // the half's earlier reads before the copies' writes
+            if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(nr) * bytes);
+            __syncwarp();
+            if (lane < nr) bulk_g2s(stage + lane * pitch + j0, cent + static_cast<size_t>(cid_) * d + j0, bytes, bar);
+        };
+        auto copy_round = [&](int cid_, int nr) {
+            if (nr == 0) return;
+            copy_half(&bars[0], 0, hb0, cid_, nr);
+            ++iss0;
+            if (hb1) {
+                copy_half(&bars[1], dh, hb1, cid_, nr);
+                ++iss1;
             }
         };
         int cid = lane < min(32, c) ? cid_of(lane) : 0;
-        copy_rows(cid, min(32, c), 0, dh);
-        cp_async_commit();
-        copy_rows(cid, min(32, c), dh, d);
-        cp_async_commit();
+        copy_round(cid, min(32, c));
+        bool ok = true;
         for (int c0 = 0, r = 0; c0 < c; c0 += 32, ++r) {
             const int nr = min(32, c - c0);
             const int nn = max(0, min(32, c - c0 - 32));  // next round's rows
             const int cidn = lane < nn ? cid_of(c0 + 32 + lane) : 0;
             float acc = 0.0f;
-            cp_async_wait_group<1>();  // this round's first half
-            __syncwarp();
+            ok = mbar_wait_bounded(&bars[0], use0 & 1u, err);  // this round's first half
+            if (!ok) break;
+            ++use0;
             if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, 0, dh, acc);
             __syncwarp();
-            copy_rows(cidn, nn, 0, dh);
-            cp_async_commit();
-            cp_async_wait_group<1>();  // this round's second half
-            __syncwarp();
-            if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, dh, d, acc);
-            __syncwarp();
-            copy_rows(cidn, nn, dh, d);
-            cp_async_commit();
+            if (nn) {
+                copy_half(&bars[0], 0, hb0, cidn, nn);
+                ++iss0;
+            }
+            if (hb1) {
+                ok = mbar_wait_bounded(&bars[1], use1 & 1u, err);  // this round's second half
+                if (!ok) break;
+                ++use1;
+                if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, dh, d, acc);
+                __syncwarp();
+                if (nn) {
+                    copy_half(&bars[1], dh, hb1, cidn, nn);
+                    ++iss1;
+                }
+            }
             if (lane < nr) {
                 const float score = METRIC == METRIC_L2 ? acc : -acc;
                 const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cid);
@@ -1814,7 +1867,14 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c,
             }
             cid = cidn;
         }
-        cp_async_wait_all();
+        if (!ok) {
+            // A copy that did not complete in time: the status word is
+            // raised; wait (bounded) for whatever is still in flight, and
+            // write nothing.
+            while (use0 < iss0 && mbar_wait_bounded(&bars[0], use0 & 1u, nullptr)) ++use0;
+            while (use1 < iss1 && mbar_wait_bounded(&bars[1], use1 & 1u, nullptr)) ++use1;
+            return;
+        }
         __syncwarp();
     } else {
         for (int c0 = 0, r = 0; c0 < c; c0 += 32, ++r) {
@@ -1847,33 +1907,20 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c,
     }
     // The m smallest keys, ascending.  Up to 128 candidates: each key's rank
     // is the number of smaller keys (keys are distinct: the centroid is in
-    // the low bits), and it goes to that position.
+    // the low bits), and it goes to that position.  The keys are read back
+    // as shared-memory broadcasts, two per load.
     if (in_regs) {
-        uint64_t kk[4];
-        int rank[4];
+        __syncwarp();  // the candidate ids (which kbuf may overlay) are read
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            kk[r] = r * 32 + lane < c ? kr[r] : KEY_MAX;
-            rank[r] = 0;
-        }
-        // Every key, broadcast from the lane that holds it.
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            if (r * 32 >= c) break;  // warp-uniform
-            const int lim = min(32, c - r * 32);
-            for (int src = 0; src < lim; ++src) {
-                const uint64_t kj = __shfl_sync(FULL, kk[r], src);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) rank[i] += kj < kk[i] ? 1 : 0;
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            if (r * 32 + lane < c && rank[r] < m) {
-                out_idx[static_cast<int64_t>(qi) * m + rank[r]] = static_cast<int64_t>(kk[r] & 0xffffffffu);
-                if (out_score)
-                    out_score[static_cast<int64_t>(qi) * m + rank[r]] = o2f(static_cast<uint32_t>(kk[r] >> 32));
-            }
+        for (int r = 0; r < 4; ++r)
+            if (r * 32 + lane < c) kbuf[r * 32 + lane] = kr[r];
+        __syncwarp();
+        switch ((c + 31) >> 5) {
+            case 1: rank_write<1>(kr, kbuf, c, m, qi, out_idx, out_score, lane); break;
+            case 2: rank_write<2>(kr, kbuf, c, m, qi, out_idx, out_score, lane); break;
+            case 3: rank_write<3>(kr, kbuf, c, m, qi, out_idx, out_score, lane); break;
+            case 4: rank_write<4>(kr, kbuf, c, m, qi, out_idx, out_score, lane); break;
+            default: break;
         }
         return;
     }
@@ -1907,20 +1954,20 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, int c,
 }
 
 template <int METRIC, int PER>
-__global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
+__global__ void __launch_bounds__(128, 1) coarse_refine_kernel(float2* __restrict__ cand, int nq, int nlist,
                                                             const float* __restrict__ q,
                                                             const float* __restrict__ cent,
                                                             const float* __restrict__ cxn,
                                                             const float2* __restrict__ caux,
                                                             const float4* __restrict__ qaux, float cK, float cN,
                                                             int d, int m, int64_t* __restrict__ out_idx,
-                                                            float* __restrict__ out_score) {
+                                                            float* __restrict__ out_score, int* err) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pitch = refine_pitch(d);
-    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
-    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
-    int* hist = reinterpret_cast<int*>(base);
+    unsigned char* base = sm + warp * refine_warp_bytes(d);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+    int* hist = reinterpret_cast<int*>(base + 16);
     float* qs = reinterpret_cast<float*>(hist + 256);
     float* stage = qs + pitch;
     const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -1968,7 +2015,8 @@ __global__ void __launch_bounds__(128) coarse_refine_kernel(float2* __restrict__
         c += __popc(bal);
     }
     __syncwarp();
-    coarse_exact_best<METRIC>(keys, hist, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
+    coarse_exact_best<METRIC>(keys, hist, reinterpret_cast<uint64_t*>(hist), bars, c, qs, stage, pitch, cent, d, m,
+                              qi, out_idx, out_score, err, lane);
 }
 
 // The coarse step for more than 2048 lists, in two tensor-core launches.
@@ -2013,7 +2061,7 @@ __global__ void __launch_bounds__(256) coarse_thr_kernel(const float2* __restric
 // score + bound; the centroids with score - bound <= U go to
 // coarse_exact_best.
 template <int METRIC>
-__global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __restrict__ cand,
+__global__ void __launch_bounds__(128, 1) coarse_refine_keys_kernel(uint64_t* __restrict__ cand,
                                                                  const int32_t* __restrict__ ccnt, int nq, int stride,
                                                                  const float* __restrict__ q,
                                                                  const float* __restrict__ cent,
@@ -2021,13 +2069,13 @@ __global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __res
                                                                  const float2* __restrict__ caux,
                                                                  const float4* __restrict__ qaux, int d, int m,
                                                                  float cK, float cN, int64_t* __restrict__ out_idx,
-                                                                 float* __restrict__ out_score) {
+                                                                 float* __restrict__ out_score, int* err) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pitch = refine_pitch(d);
-    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
-    unsigned char* base = sm + warp * ((per_warp + 15) & ~size_t(15));
-    int* hist = reinterpret_cast<int*>(base);
+    unsigned char* base = sm + warp * refine_warp_bytes(d);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+    int* hist = reinterpret_cast<int*>(base + 16);
     float* qs = reinterpret_cast<float*>(hist + 256);
     float* stage = qs + pitch;
     const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -2064,7 +2112,8 @@ __global__ void __launch_bounds__(128) coarse_refine_keys_kernel(uint64_t* __res
         c += __popc(bal);
     }
     __syncwarp();
-    coarse_exact_best<METRIC>(keys, nullptr, c, qs, stage, pitch, cent, d, m, qi, out_idx, out_score, lane);
+    coarse_exact_best<METRIC>(keys, nullptr, reinterpret_cast<uint64_t*>(hist), bars, c, qs, stage, pitch, cent, d,
+                              m, qi, out_idx, out_score, err, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -2473,15 +2522,13 @@ cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int
 }
 
 size_t coarse_refine_smem(int nlist, int d, int warps) {
-    const int pitch = refine_pitch(d);
     (void)nlist;
-    const size_t per_warp = 1024 + static_cast<size_t>(pitch) * 4 + static_cast<size_t>(32) * pitch * 4;
-    return static_cast<size_t>(warps) * ((per_warp + 15) & ~size_t(15));
+    return static_cast<size_t>(warps) * refine_warp_bytes(d);
 }
 
 cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent,
                                  const float* cxn, const float2* caux, const float4* qaux, int d, int metric, int m,
-                                 int64_t* out_idx, float* out_score, cudaStream_t s) {
+                                 int64_t* out_idx, float* out_score, int* err, cudaStream_t s) {
     float cK, cN;
     err_consts(d, false, &cK, &cN, true);  // the split centroid image
     int warps = 4;
@@ -2493,7 +2540,7 @@ cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         kern<<<grid, 32 * warps, smem, s>>>(cand, nq, nlist, q, cent, cxn, caux, qaux, cK, cN, d, m, out_idx,
-                                            out_score);
+                                            out_score, err);
         return cudaGetLastError();
     };
     if (nlist > 2048) return cudaErrorInvalidValue;
@@ -2513,7 +2560,8 @@ cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, const fl
 
 cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int nq, int stride, const float* q,
                                       const float* cent, const float* cxn, const float2* caux, const float4* qaux,
-                                      int d, int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s) {
+                                      int d, int metric, int m, int64_t* out_idx, float* out_score, int* err,
+                                      cudaStream_t s) {
     int warps = 4;
     while (warps > 1 && coarse_refine_smem(0, d, warps) > 200 * 1024) warps >>= 1;
     const size_t smem = coarse_refine_smem(0, d, warps);
@@ -2525,7 +2573,7 @@ cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int n
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         kern<<<grid, 32 * warps, smem, s>>>(cand, ccnt, nq, stride, q, cent, cxn, caux, qaux, d, m, cK, cN, out_idx,
-                                            out_score);
+                                            out_score, err);
         return cudaGetLastError();
     };
     return metric == METRIC_L2 ? run(coarse_refine_keys_kernel<METRIC_L2>) : run(coarse_refine_keys_kernel<METRIC_IP>);

@@ -120,11 +120,12 @@ cudaError_t launch_coarse_items(int nq, int nlist, int ngroups, int nslices, int
 // cxn / caux (the centroid index's squared norms and {|c~|, |c - c~|}) and
 // qaux: the exact m best centroids per query and their exact coarse scores,
 // as launch_select gives them from coarse_scores (cand is overwritten).
-// Needs m <= 256 and coarse_refine_smem(nlist, d, 1) <= 200 KiB.
+// Needs m <= 256 and coarse_refine_smem(nlist, d, 1) <= 200 KiB.  A staging
+// copy that does not complete within the wait limit raises *err.
 size_t coarse_refine_smem(int nlist, int d, int warps);
 cudaError_t launch_coarse_refine(float2* cand, int nq, int nlist, const float* q, const float* cent,
                                  const float* cxn, const float2* caux, const float4* qaux, int d, int metric, int m,
-                                 int64_t* out_idx, float* out_score, cudaStream_t s);
+                                 int64_t* out_idx, float* out_score, int* err, cudaStream_t s);
 
 // More than 2048 centroids: thr[q] := a bound on the m-th smallest
 // score + bound among the S <= 1024 dense scores of query q (cand, nq x S
@@ -137,7 +138,8 @@ cudaError_t launch_coarse_thr(const float2* cand, int nq, int S, int m, const fl
                               const float4* qaux, int d, int metric, float* thr, cudaStream_t s);
 cudaError_t launch_coarse_refine_keys(uint64_t* cand, const int32_t* ccnt, int nq, int stride, const float* q,
                                       const float* cent, const float* cxn, const float2* caux, const float4* qaux,
-                                      int d, int metric, int m, int64_t* out_idx, float* out_score, cudaStream_t s);
+                                      int d, int metric, int m, int64_t* out_idx, float* out_score, int* err,
+                                      cudaStream_t s);
 
 // Largest list the batched search's first pass scans densely (the candidate
 // buffer's size caps it further).

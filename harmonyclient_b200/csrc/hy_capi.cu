@@ -910,7 +910,8 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
         HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
         HY_CUDA(hy::launch_coarse_refine(reinterpret_cast<float2*>(h->c_cand.p), (int)m, nlist, qq,
                                          h->cent.as<float>(), h->c_norm.as<float>(), h->c_aux.as<float2>(),
-                                         h->b_qn.as<float4>(), (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+                                         h->b_qn.as<float4>(), (int)h->d, h->metric, (int)nprobe, probes, pscore,
+                                         h->w_err.as<int>(), s));
         h->launches += 3;
         return HY_OK;
     }
@@ -940,7 +941,7 @@ int coarse_tensor(hy_index* h, size_t m, const float* qq, size_t nprobe, int64_t
     HY_CUDA(hy::launch_batched_scan(b, w, h->w_err.as<int>(), s));
     HY_CUDA(hy::launch_coarse_refine_keys(h->c_cand.as<uint64_t>(), w.cand_cnt, (int)m, nlist, qq, h->cent.as<float>(),
                                           h->c_norm.as<float>(), h->c_aux.as<float2>(), h->b_qn.as<float4>(),
-                                          (int)h->d, h->metric, (int)nprobe, probes, pscore, s));
+                                          (int)h->d, h->metric, (int)nprobe, probes, pscore, h->w_err.as<int>(), s));
     h->launches += 6;
     return HY_OK;
 }

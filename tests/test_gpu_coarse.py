@@ -43,6 +43,27 @@ def test_tensor_probes_equal_exact(name):
     np.testing.assert_array_equal(_probes(idx, q, "tensor"), plain)
 
 
+@pytest.mark.parametrize("d", [4, 8, 12, 20, 36])
+def test_tensor_probes_equal_exact_small_dims(d):
+    """The exact re-scoring stages centroid rows in two dimension halves (at
+    d = 4 the second half is empty); 70 probes of 300 lists take three
+    rounds of 32 rows."""
+    x, q = datasets.gmm_float(20_000, 400, d=d, ncomp=300, seed=50 + d)
+    idx = hb.Index(d, 300, 70)
+    idx.train(x)
+    idx.add(x)
+    plain = idx.probes(q)
+    np.testing.assert_array_equal(_probes(idx, q, "tensor"), plain)
+    idx.set_form("bf16")
+    try:
+        Dt, It = idx.search(q, 10)
+    finally:
+        idx.set_form("plain")
+    Dp, Ip = idx.search(q, 10)
+    np.testing.assert_array_equal(It, Ip)
+    np.testing.assert_array_equal(Dt, Dp)
+
+
 @pytest.fixture(scope="module")
 def wide():
     # 1,000 lists (not a multiple of 128), 3,000 queries, integer data.
