@@ -1810,9 +1810,11 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, uint64
         // Phases of each half's barrier issued and consumed.
         uint32_t iss0 = 0, iss1 = 0, use0 = 0, use1 = 0;
         // Dims [j0, j0 + bytes / 4) of nr rows: lane i's row (centroid cid_)
-        // by one bulk copy completing on bar.
+        // by one bulk copy completing on bar.  The half's earlier reads have
+        // all returned (every lane's sum used them before the __syncwarp
+        // that precedes a reuse), as in a copy pipeline whose consumers
+        // release a stage by arriving on a barrier.
         auto copy_half = [&](uint64_t* bar, int j0, uint32_t bytes, int cid_, int nr) {
-            fence_proxy_async();  // the half's earlier reads before the copies' writes
             if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(nr) * bytes);
             __syncwarp();
             if (lane < nr) bulk_g2s(stage + lane * pitch + j0, cent + static_cast<size_t>(cid_) * d + j0, bytes, bar);
@@ -1975,45 +1977,68 @@ __global__ void __launch_bounds__(128, 1) coarse_refine_kernel(float2* __restric
     const float* qrow = q + static_cast<size_t>(qi) * d;
     for (int j = lane; j < d; j += 32) qs[j] = qrow[j];
     // Every centroid's upper bound (ordered bits) and lower bound in
-    // registers: entry r * 32 + lane.  The query's buffer is then free and
-    // holds its candidate keys.
+    // registers: entry r * 32 + lane, or, with exactly 32 PER centroids,
+    // entry 4 (32 (r / 4) + lane) + r % 4 (16-byte loads of four centroids'
+    // terms).  The query's buffer is then free and holds its candidate keys.
     float2* ce = cand + static_cast<int64_t>(qi) * nlist;
     const float* cs = reinterpret_cast<const float*>(ce) + nlist;
     uint64_t* keys = reinterpret_cast<uint64_t*>(ce);
     const bool l2 = METRIC == METRIC_L2;
     const ErrCoef ec = err_coef(qaux[qi], l2, cK, cN);
+    const bool vec = nlist == PER * 32;
+    auto entry = [&](int r) { return vec ? 4 * ((r >> 2) * 32 + lane) + (r & 3) : r * 32 + lane; };
     uint32_t hi[PER];
     float lo[PER];
+    auto bound = [&](int r, float sc, float ax, float ay, float xn) {
+        const float eb = fmaf(ax, ec.aq, fmaf(ay, ec.bq, err_row_const(xn, l2, cN) + ec.cq));
+        hi[r] = f2o(sc + eb);
+        lo[r] = sc - eb;
+    };
+    if (vec) {
 #pragma unroll
-    for (int r = 0; r < PER; ++r) {
-        const int e = r * 32 + lane;
-        hi[r] = 0xffffffffu;
-        lo[r] = INFINITY;
-        if (e < nlist) {
-            const float sc = cs[e];
-            const float2 a = caux[e];
-            const float eb = fmaf(a.x, ec.aq, fmaf(a.y, ec.bq, err_row_const(cxn[e], l2, cN) + ec.cq));
-            hi[r] = f2o(sc + eb);
-            lo[r] = sc - eb;
+        for (int g = 0; g < PER / 4; ++g) {
+            const int e0 = 4 * (g * 32 + lane);
+            const float4 sc = *reinterpret_cast<const float4*>(cs + e0);
+            const float4 a01 = *reinterpret_cast<const float4*>(caux + e0);
+            const float4 a23 = *reinterpret_cast<const float4*>(caux + e0 + 2);
+            const float4 xn = *reinterpret_cast<const float4*>(cxn + e0);
+            bound(4 * g, sc.x, a01.x, a01.y, xn.x);
+            bound(4 * g + 1, sc.y, a01.z, a01.w, xn.y);
+            bound(4 * g + 2, sc.z, a23.x, a23.y, xn.z);
+            bound(4 * g + 3, sc.w, a23.z, a23.w, xn.w);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int e = r * 32 + lane;
+            hi[r] = 0xffffffffu;
+            lo[r] = INFINITY;
+            if (e < nlist) bound(r, cs[e], caux[e].x, caux[e].y, cxn[e]);
         }
     }
     const float U = o2f(warp_select_bound<PER>(hi, nlist, m, hist, lane));
     __syncwarp();  // every pair has been read, and the histogram too
-    // Centroids that can be among the m best: ids in keys, and the first
-    // 256 also in the histogram's space.
+    // Centroids that can be among the m best: the first 256 ids in the
+    // histogram's space, the rest in keys (and there all of them when there
+    // are more than 256).
     int c = 0;
 #pragma unroll
     for (int r = 0; r < PER; ++r) {
-        const int e = r * 32 + lane;
+        const int e = entry(r);
         const bool keep = e < nlist && lo[r] <= U;
         const unsigned bal = __ballot_sync(FULL, keep);
         if (keep) {
             const int at = c + __popc(bal & ((1u << lane) - 1u));
-            keys[at] = static_cast<uint64_t>(e);
-            if (at < 256) hist[at] = e;
+            if (at < 256)
+                hist[at] = e;
+            else
+                keys[at] = static_cast<uint64_t>(e);
         }
         c += __popc(bal);
     }
+    __syncwarp();
+    if (c > 256)
+        for (int e = lane; e < 256; e += 32) keys[e] = static_cast<uint64_t>(hist[e]);
     __syncwarp();
     coarse_exact_best<METRIC>(keys, hist, reinterpret_cast<uint64_t*>(hist), bars, c, qs, stage, pitch, cent, d, m,
                               qi, out_idx, out_score, err, lane);
