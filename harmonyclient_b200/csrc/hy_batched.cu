@@ -1700,8 +1700,8 @@ __global__ void coarse_items_kernel(int nq, int nlist, int64_t rows, int ngroups
 // Staging row pitch of coarse_refine_kernel (floats): d + 4 when d is a
 // multiple of 4 (16-byte rows), else d + 1 (conflict-free column reads).
 __host__ __device__ inline int refine_pitch(int d) { return (d & 3) == 0 ? d + 4 : d + 1; }
-// Shared memory per warp of the refine kernels: two copy barriers (16
-// bytes), 256 histogram bins, the query and a 32-row staging block.
+// Shared memory per warp of the refine kernels: the copy barrier (16 bytes
+// with padding), 256 histogram bins, the query and a 32-row staging block.
 __host__ __device__ inline size_t refine_warp_bytes(int d) {
     const size_t pitch = refine_pitch(d);
     return (16 + 1024 + pitch * 4 + 32 * pitch * 4 + 15) & ~size_t(15);
@@ -1718,7 +1718,7 @@ __host__ __device__ inline size_t refine_warp_bytes(int d) {
 // order, separately rounded operations), and the m best (score, centroid)
 // keys, ascending with ties to the lower centroid, are written as
 // select_warp_kernel writes them.  The candidate keys overwrite the query's
-// pairs in cand.  Shared memory per warp: two copy barriers, 256 histogram
+// pairs in cand.  Shared memory per warp: the copy barrier, 256 histogram
 // bins, the query and a 32-row staging block of centroids.
 // The exact m best of a query's c candidate centroids (ids in keys[0, c),
 // and in sids[0, c) when sids is given and c <= 256): exact FP32 coarse
@@ -1726,10 +1726,10 @@ __host__ __device__ inline size_t refine_warp_bytes(int d) {
 // rounded operations), 32 candidates per round (lane i sums row i), then
 // ordered by (score, centroid) and written as select_warp_kernel writes them.
 // With d a multiple of 4 the rows are staged in shared memory (row pitch
-// d + 4, so a warp's 512-byte read takes the minimum four wavefronts) in two
-// dimension halves, each lane's half-row by one bulk copy completing on the
-// half's barrier: while the lanes sum one half of this round's rows, the
-// copies of the other half of the next round's rows are in flight.  Up to 128 candidates the scored keys stay in
+// d + 4, so a warp's 512-byte read takes the minimum four wavefronts), each
+// lane's row by one bulk copy completing on a barrier (the cost of a bulk
+// copy is per copy, not per byte: whole rows measured faster than
+// dimension halves pipelined against the sums).  Up to 128 candidates the scored keys stay in
 // registers (lane i, round r: candidate 32 r + i); more are written back to
 // keys and merged through shared-memory-free warp sorts.
 template <int METRIC>
@@ -1799,63 +1799,39 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, uint64
     auto cid_of = [&](int e) { return ids_smem ? sids[e] : static_cast<int>(keys[e]); };
     uint64_t kr[4] = {KEY_MAX, KEY_MAX, KEY_MAX, KEY_MAX};
     if (v4) {
-        const int dh = ((d >> 1) + 3) & ~3;  // first half [0, dh), second [dh, d)
-        const uint32_t hb0 = static_cast<uint32_t>(dh) * 4u, hb1 = static_cast<uint32_t>(d - dh) * 4u;
+        const uint32_t rb = static_cast<uint32_t>(d) * 4u;  // bytes of one row
+        uint64_t* bar = &bars[0];
         if (lane == 0) {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
+            mbar_init(bar, 1);
             fence_mbar_init();
         }
         __syncwarp();
-        // Phases of each half's barrier issued and consumed.
-        uint32_t iss0 = 0, iss1 = 0, use0 = 0, use1 = 0;
-        // Dims [j0, j0 + bytes / 4) of nr rows: lane i's row (centroid cid_)
-        // by one bulk copy completing on bar.  The half's earlier reads have
-        // all returned (every lane's sum used them before the __syncwarp
-        // that precedes a reuse), as in a copy pipeline whose consumers
-        // release a stage by arriving on a barrier.
-        auto copy_half = [&](uint64_t* bar, int j0, uint32_t bytes, int cid_, int nr) {
-            if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(nr) * bytes);
+        uint32_t issued = 0, used = 0;  // phases of the barrier issued and consumed
+        // nr rows: lane i's row (centroid cid_) by one bulk copy completing
+        // on the barrier.  A round's reads of the staging block have all
+        // returned (every lane's sum used them before the __syncwarp that
+        // precedes the next round's copies), as in a copy pipeline whose
+        // consumers release a stage by arriving on a barrier.
+        auto copy_rows = [&](int cid_, int nr) {
+            if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(nr) * rb);
             __syncwarp();
-            if (lane < nr) bulk_g2s(stage + lane * pitch + j0, cent + static_cast<size_t>(cid_) * d + j0, bytes, bar);
-        };
-        auto copy_round = [&](int cid_, int nr) {
-            if (nr == 0) return;
-            copy_half(&bars[0], 0, hb0, cid_, nr);
-            ++iss0;
-            if (hb1) {
-                copy_half(&bars[1], dh, hb1, cid_, nr);
-                ++iss1;
-            }
+            if (lane < nr) bulk_g2s(stage + lane * pitch, cent + static_cast<size_t>(cid_) * d, rb, bar);
+            ++issued;
         };
         int cid = lane < min(32, c) ? cid_of(lane) : 0;
-        copy_round(cid, min(32, c));
+        if (c > 0) copy_rows(cid, min(32, c));
         bool ok = true;
         for (int c0 = 0, r = 0; c0 < c; c0 += 32, ++r) {
             const int nr = min(32, c - c0);
             const int nn = max(0, min(32, c - c0 - 32));  // next round's rows
             const int cidn = lane < nn ? cid_of(c0 + 32 + lane) : 0;
             float acc = 0.0f;
-            ok = mbar_wait_bounded(&bars[0], use0 & 1u, err);  // this round's first half
+            ok = mbar_wait_bounded(bar, used & 1u, err);
             if (!ok) break;
-            ++use0;
-            if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, 0, dh, acc);
+            ++used;
+            if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, 0, d, acc);
             __syncwarp();
-            if (nn) {
-                copy_half(&bars[0], 0, hb0, cidn, nn);
-                ++iss0;
-            }
-            if (hb1) {
-                ok = mbar_wait_bounded(&bars[1], use1 & 1u, err);  // this round's second half
-                if (!ok) break;
-                ++use1;
-                if (lane < nr) acc = coarse_dot<METRIC>(qs, stage + lane * pitch, dh, d, acc);
-                __syncwarp();
-                if (nn) {
-                    copy_half(&bars[1], dh, hb1, cidn, nn);
-                    ++iss1;
-                }
-            }
+            if (nn) copy_rows(cidn, nn);
             if (lane < nr) {
                 const float score = METRIC == METRIC_L2 ? acc : -acc;
                 const uint64_t key = (static_cast<uint64_t>(f2o(score)) << 32) | static_cast<uint32_t>(cid);
@@ -1873,8 +1849,7 @@ __device__ inline void coarse_exact_best(uint64_t* keys, const int* sids, uint64
             // A copy that did not complete in time: the status word is
             // raised; wait (bounded) for whatever is still in flight, and
             // write nothing.
-            while (use0 < iss0 && mbar_wait_bounded(&bars[0], use0 & 1u, nullptr)) ++use0;
-            while (use1 < iss1 && mbar_wait_bounded(&bars[1], use1 & 1u, nullptr)) ++use1;
+            while (used < issued && mbar_wait_bounded(bar, used & 1u, nullptr)) ++used;
             return;
         }
         __syncwarp();
