@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import harmonyclient_b200 as hb
+from harmonyclient_b200 import datasets
 from oracle import port
 from tests.golden import cases
 from tests.topk_check import assert_topk_equal, probe_tied_rows
@@ -98,6 +99,39 @@ def test_bf16_equals_plain_across_k(name, k):
     assert idx.last_stats()["fallback_queries"] == 0
     idx.set_form("plain")
     Dp, Ip = idx.search(q, k)
+    np.testing.assert_array_equal(Db, Dp)
+    np.testing.assert_array_equal(Ib, Ip)
+
+
+def test_bf16_equals_plain_duplicated_rows():
+    """1,500 copies of one row in a first-pass list, queries next to it:
+    the dense tightening's k-th bound falls on a run of equal scores, and the
+    answer, ties to the lower id, is still the plain scan's."""
+    x, q = datasets.gmm_uint8(20_000, 60, d=32, ncomp=40, seed=3)
+    x[:1500] = x[0]
+    q[:20] = np.clip(x[0] + np.arange(20)[:, None] % 3, 0, 255)
+    idx = hb.Index(32, 8, 1)
+    idx.train(x)
+    idx.add(x)
+    idx.set_form("bf16")
+    Db, Ib = idx.search(q, 100)
+    idx.set_form("plain")
+    Dp, Ip = idx.search(q, 100)
+    np.testing.assert_array_equal(Db, Dp)
+    np.testing.assert_array_equal(Ib, Ip)
+
+
+def test_bf16_equals_plain_long_dense_lists():
+    """First-pass lists of about 5,000 rows (dense tightening over many
+    rounds of 128 scores per warp): the answer is still the plain scan's."""
+    x, q = datasets.gmm_uint8(60_000, 300, d=32, ncomp=40, seed=7)
+    idx = hb.Index(32, 12, 2)
+    idx.train(x)
+    idx.add(x)
+    idx.set_form("bf16")
+    Db, Ib = idx.search(q, 100)
+    idx.set_form("plain")
+    Dp, Ip = idx.search(q, 100)
     np.testing.assert_array_equal(Db, Dp)
     np.testing.assert_array_equal(Ib, Ip)
 
