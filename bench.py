@@ -616,7 +616,8 @@ def run_ours(args, rank, world, dist):
 # float64 brute force over every query.
 def plain_roofline(st, scan_ms, launches, palg, clocks, args, hbm_peak, peak_kind):
     """Roofline of the plain form's scan over one search (scan_ms: every scan
-    launch of the search).  List-major: executed FP32 operations (3 x 32 x 16
+    launch of the search's last query chunk, the launches the library's
+    kernel events time).  List-major: executed FP32 operations (3 x 32 x 16
     per executed (query, 32-row tile, 16-dimension segment) partial sum,
     `seg_sums`) against 148 SMs x 128 FP32 lanes x the SM clock measured
     during the run; the lists are read once per group of 32 queries, mostly
@@ -624,7 +625,11 @@ def plain_roofline(st, scan_ms, launches, palg, clocks, args, hbm_peak, peak_kin
     Query-major: pair bytes (every probed row of every query, d x 4 bytes,
     plus queries and results) against the measured copy bandwidth."""
     if st.get("list_major"):
+        # The counters and kernel_ms cover the search's last query chunk; its
+        # pair bytes are the unpruned segment sums' rows (32 rows x 16
+        # dimensions x 4 bytes each, tiles padded to 32 rows).
         ops = st["seg_sums"] * 32 * 16 * 3
+        palg = st["seg_sums_max"] * 32 * 16 * 4
         sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
         fpeak = 148 * 128 * sm_mhz * 1e6 / 1e12
         fach = ops / (scan_ms / 1e3) / 1e12

@@ -739,6 +739,11 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
         const size_t m = std::min(qc, n - q0);
         const float* qq = dq + q0 * h->d;
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
+        // The list-major scan's counters restart at the last query chunk, the
+        // one whose scan launches the kernel events time, so that the
+        // executed partial sums and kernel_ms describe the same launches.
+        if (lm && q0 > 0 && q0 + m >= n)
+            HY_CUDA(cudaMemsetAsync(h->w_counters.p, 0, 4 * sizeof(unsigned long long), s));
         HY_CUDA(hy::launch_coarse_scores(qq, (int)m, h->cent.as<float>(), (int)h->nlist, (int)h->d, h->metric,
                                          h->w_scores.as<float>(), s));
         HY_CUDA(hy::launch_select(h->w_scores.as<float>(), (int)m, (int)h->nlist, (int)nprobe,

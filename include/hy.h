@@ -109,7 +109,8 @@ typedef struct {
     uint64_t kernel_launches; /* launches kernel_ms covers */
     uint64_t graph_replayed;  /* device-pointer search in graph mode: 1 when the call replayed a graph */
     uint64_t seg_sums;        /* list-major plain scan: (query, 32-row tile, 16-dimension segment) partial
-                                 sums computed: 32 x 16 x 3 FP32 operations each */
+                                 sums computed: 32 x 16 x 3 FP32 operations each; like kernel_ms, and
+                                 with the tile counts, they cover the last query chunk */
     uint64_t seg_sums_max;    /* list-major plain scan: the segment sums a scan without pruning computes */
     uint64_t list_major;      /* plain form: 1 when the search ran the list-major scan */
 } hy_search_stats_t;
