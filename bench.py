@@ -389,6 +389,7 @@ def run_ours(args, rank, world, dist):
     I_main = dI.cpu().numpy()
     D_main = dD.cpu().numpy()
     kern_ms, kern_per_search = _kernel_ms(idx, dq, dD, dI, k, 3, stream, npq)
+    kern_chunk = int(idx.last_stats()["chunk_queries"]) or q.shape[0]  # queries the timed launches cover
 
     # End to end through the public host API: pinned host queries in, results
     # back to pinned host memory, every step (with the learned form this
@@ -467,10 +468,13 @@ def run_ours(args, rank, world, dist):
         # (query, probed row) pair of its pass and reads each list that some
         # query probes in that pass once, as bf16 rows (d x 2 bytes).  The
         # bound is whichever of the two takes longer at the measured peaks.
-        flops = rows_main * 2 * d / kern_per_search
+        # kern_ms covers the launches of the search's last query chunk, so
+        # the work counted is that chunk's (the last kern_chunk queries).
+        P_last = P_main[P_main.shape[0] - kern_chunk:]
+        flops = pair_rows(P_last) * 2 * d / kern_per_search
         distinct = 0
-        for j0, j1 in ((0, 1), (1, P_main.shape[1])):
-            cols = P_main[:, j0:j1]
+        for j0, j1 in ((0, 1), (1, P_last.shape[1])):
+            cols = P_last[:, j0:j1]
             used = np.unique(cols[cols >= 0])
             distinct += int(sizes[used].sum())
         lbytes = distinct * d * (1 if base == "fp8" else 2) / kern_per_search

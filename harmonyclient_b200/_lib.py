@@ -37,7 +37,8 @@ class SearchStats(C.Structure):
                 ("merge_ms", C.c_double), ("launches", C.c_uint64), ("fallback_queries", C.c_uint64),
                 ("mean_nprobe", C.c_double), ("judge_recall", C.c_double), ("learned_fallback", C.c_uint64),
                 ("kernel_ms", C.c_double), ("kernel_launches", C.c_uint64), ("graph_replayed", C.c_uint64),
-                ("seg_sums", C.c_uint64), ("seg_sums_max", C.c_uint64), ("list_major", C.c_uint64)]
+                ("seg_sums", C.c_uint64), ("seg_sums_max", C.c_uint64), ("list_major", C.c_uint64),
+                ("chunk_queries", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

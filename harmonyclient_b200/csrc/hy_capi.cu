@@ -737,6 +737,7 @@ int search_device_impl(hy_index* h, size_t n, const float* dq, size_t k, float* 
     }
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
+        h->stats.chunk_queries = m;  // the last chunk's count remains
         const float* qq = dq + q0 * h->d;
         if (timed && q0 == 0) HY_CUDA(ev_record(h->ev[0], s));
         // The list-major scan's counters restart at the last query chunk, the
@@ -1054,6 +1055,7 @@ int search_bf16_impl(hy_index* h, size_t n, const float* dq, size_t k, float* dD
     w.rest = w.big2 + (qc + 1);
     for (size_t q0 = 0; q0 < n; q0 += qc) {
         const size_t m = std::min(qc, n - q0);
+        h->stats.chunk_queries = m;  // the last chunk's count remains
         const float* qq = dq + q0 * h->d;
         w.overflow = h->b_ovf.as<int32_t>();  // [0] = count, then chunk-local query ids
         HY_CUDA(cudaMemsetAsync(w.overflow, 0, sizeof(int32_t), s));

@@ -113,6 +113,8 @@ typedef struct {
                                  with the tile counts, they cover the last query chunk */
     uint64_t seg_sums_max;    /* list-major plain scan: the segment sums a scan without pruning computes */
     uint64_t list_major;      /* plain form: 1 when the search ran the list-major scan */
+    uint64_t chunk_queries;   /* device search: queries of its last query chunk, the chunk whose launches
+                                 kernel_ms and the scan counters cover */
 } hy_search_stats_t;
 
 HY_API const char* hy_last_error(void);
